@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""MPD-RDME throughput on the rod-cell oscillator workload (B200).
+
+One bench step = TIMESTEPS_PER_STEP MPD timesteps (x, y, z sweeps, reaction,
+overflow handling) of the 64x64x128 rod-cell model (16 nm, 3 site types,
+5 species, 8 reactions, 4000 D + 1400 E, ByteLattice 8 slots, tau = 25 us),
+a segment of that model's 50,000-timestep trajectory.  Inputs are seeded and
+synthetic (lattice_microbes_b200.configs.config1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 is launched through torch.distributed.run: every rank runs its own
+replicate (its own seed) on its own GPU with no data exchange (replicas only);
+the value is all ranks' site-steps over the slowest rank's device time.
+
+--impl reference times the reference's own MPD code on the host cores: the
+reference device functions compiled for the CPU from the reference sources
+(oracle/_ref), one replicate per host core as ReplicateRunner runs replicates,
+each bench step a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TIMESTEPS_PER_STEP = 500
+WORKLOAD = "rod-cell 64x64x128 ByteLattice-8, 3 site types, 5 species, 8 reactions, 5400 particles"
+METRIC = "site-steps/s"
+B_SWEEP = 2 * 8 * 1 + 1       # bytes per site per sweep, Byte-8 (read + write 8 slots, read site type)
+B_STEP = 7 * 8 * 1 + 4        # bytes per site-step on the reference schedule
+L2_FLUSH_BYTES = 256 << 20    # larger than the 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--timesteps-per-step", type=int, default=TIMESTEPS_PER_STEP)
+    ap.add_argument("--cpu-sample-timesteps", type=int, default=0,
+                    help="timesteps per core in the CPU baseline sample (0 = auto)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+# CPU side: the reference's code on the host cores
+# --------------------------------------------------------------------------
+
+def _cpu_worker(args):
+    """One replicate of the reference MPD code on one core (spawned)."""
+    seed, timesteps = args
+    sys.path.insert(0, ROOT)
+    from lattice_microbes_b200 import configs
+    from tests.cases import oracle_tables
+    from tests.oracle_lib import reference_run
+    spec = configs.config1(seed=seed)
+    t = oracle_tables(spec)
+    t0 = time.perf_counter()
+    r = reference_run(t, spec.lattice, spec.sites, 1000 + seed, 0, timesteps)
+    dt = time.perf_counter() - t0
+    if r is None:
+        return None
+    return dt, int(r[1])
+
+
+def cpu_reference_sample(timesteps, cores):
+    """Runs `cores` replicates in parallel; returns (site-steps/s, sample)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_cpu_worker, [(s, timesteps) for s in range(cores)])
+    if any(r is None for r in res):
+        return None, "reference checker not built (oracle/_ref)"
+    wall = max(r[0] for r in res)
+    nsites = 64 * 64 * 128
+    value = nsites * timesteps * cores / wall
+    sample = ("%d replicates x %d timesteps of the rod-cell workload, one per core, reference device "
+              "functions compiled for the host; %.1f s wall" % (cores, timesteps, wall))
+    return value, sample
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------
+# Clocks during the timed region
+# --------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+            os.unlink(self.path)
+        except Exception:
+            return out
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].strip() == "Active":
+                    reasons.add(nm)
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+        if mx:
+            out["sm_max_mhz"] = max(mx)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(sm)
+        return out
+
+
+def measured_peak_hbm():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_sweep():
+    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        return d.get("sweep_dram_bytes_per_launch")
+    except Exception:
+        return None
+
+
+# --------------------------------------------------------------------------
+# Our arm
+# --------------------------------------------------------------------------
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+
+    # CPU baseline first (spawned workers, before any GPU work on this rank).
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cores = host_cores()
+        ts = a.cpu_sample_timesteps or 60
+        val, sample = cpu_reference_sample(ts, cores)
+        if val is not None:
+            cpu = {"value": val, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample}
+
+    from lattice_microbes_b200 import configs
+    from lattice_microbes_b200.solver import Context, Lattice, Model, compose_seed, kernel_launches
+
+    T = a.timesteps_per_step
+    spec = configs.config1(seed=1 + rank)
+    N = spec.nsites
+    ctx = Context(device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
+    model = Model.from_spec(ctx, spec)
+    lat = Lattice(ctx, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+    lat.set_native(spec.lattice, spec.sites)
+    seed = compose_seed(2024, rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    step = 0
+    for _ in range(a.warmup):
+        lat.run(model, seed, step, T)
+        step += T
+
+    # ---- device-timed throughput (inputs resident in HBM) ----
+    clocks = ClockSampler(device)
+    times = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    launches0 = kernel_launches()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for _ in range(a.steps):
+            flush.fill_(1.0)  # L2 flush between timed steps, outside the events
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lat.run_async(model, seed, step, T)
+            e1.record(stream)
+            lat.wait()
+            times.append(e0.elapsed_time(e1))
+            step += T
+    torch.cuda.synchronize(device)
+    clock_info = clocks.stop()
+    launches = kernel_launches() - launches0 - 0
+    if world > 1:
+        dist.barrier()
+    my_ms = sum(times)
+    ms_total = my_ms
+    if world > 1:
+        t = torch.tensor([my_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    value = N * T * a.steps * world / (ms_total / 1e3)
+
+    # ---- per-phase kernel times (roofline of the dominant kernel) ----
+    st, phase_ms, phase_n = lat.run_profiled(model, seed, step, T)
+    step += T
+    sweep_ms = float(phase_ms[:3].sum()) / max(1, int(phase_n[:3].sum()))
+    achieved = N * B_SWEEP / (sweep_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    phases = {name: {"ms_per_launch": float(phase_ms[k]) / max(1, int(phase_n[k])),
+                     "share": float(phase_ms[k]) / float(phase_ms.sum())}
+              for k, name in enumerate(["sweep_x", "sweep_y", "sweep_z", "reaction", "overflow"])}
+
+    # ---- end to end through the public API with host buffers ----
+    words = spec.words * N
+    h_lat = torch.from_numpy(spec.lattice.copy()).pin_memory()
+    h_sites = torch.from_numpy(spec.sites.copy()).pin_memory()
+    h_out = torch.empty(words, dtype=torch.int32).pin_memory()
+    import ctypes as C
+    from lattice_microbes_b200 import _lib as L
+    e2e_ms = []
+    if world > 1:
+        dist.barrier()
+    for _ in range(a.steps):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        L.check(L.lib().lmb_lattice_set_native(lat.handle, C.cast(h_lat.data_ptr(), L.u32p),
+                                               C.cast(h_sites.data_ptr(), L.u8p)))
+        lat.run(model, seed, 0, T)
+        L.check(L.lib().lmb_lattice_get_native(lat.handle, C.cast(h_out.data_ptr(), L.u32p), None))
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = N * T * a.steps * world / (e2e_total / 1e3)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": METRIC,
+            "n_gpus": world,
+            "steps": a.steps,
+            "warmup": a.warmup,
+            "ms_per_step": ms_total / a.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u8",
+            "data": "synthetic (seeded rod-cell model, lattice_microbes_b200.configs.config1)",
+            "config": {
+                "workload": WORKLOAD,
+                "timesteps_per_step": T,
+                "sites": N,
+                "parallelism": "replicas" if world > 1 else "single",
+                "l2": "flushed between timed steps (256 MB write); working set 9 MB is L2-resident within a step",
+            },
+            "roofline": {
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": ncu_traffic_per_sweep(),
+                "kernel": "sweep_kernel (x/y/z hop sweeps)",
+                "algorithmic_bytes_per_launch": N * B_SWEEP,
+                "peak_kind": peak_kind,
+                "phases": phases,
+                "step_fraction_reference_schedule": value * B_STEP / (peak * 1e9),
+            },
+            "e2e": {
+                "value": e2e_value,
+                "unit": METRIC,
+                "h2d_bytes_per_step": int(words * 4 + N),
+                "d2h_bytes_per_step": int(words * 4),
+            },
+            "gpu_launches": int(launches),
+            "clocks": clock_info,
+            "cpu_baseline": cpu,
+            "run_stats": {"overflows": int(st.overflows), "reactions_per_step": int(st.reactions)},
+        }
+        print(json.dumps(line), flush=True)
+    lat.close()
+    model.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = host_cores()
+    ts = a.cpu_sample_timesteps or 20
+    vals, samples = [], []
+    for _ in range(a.warmup if a.warmup < 1 else 1):
+        cpu_reference_sample(max(2, ts // 4), cores)
+    for _ in range(a.steps):
+        v, s = cpu_reference_sample(ts, cores)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": s}))
+            return
+        vals.append(v)
+        samples.append(s)
+    value = statistics.mean(vals)
+    nsites = 64 * 64 * 128
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": METRIC,
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": nsites * a.timesteps_per_step / value * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (seeded rod-cell model)",
+        "config": {"workload": WORKLOAD, "timesteps_per_step": a.timesteps_per_step, "sites": nsites,
+                   "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
+                         "sample": samples[-1]},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)

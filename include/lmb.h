@@ -1,0 +1,195 @@
+/*
+ * lmb.h -- C ABI of the B200-native MPD-RDME solver (liblmb200.so).
+ *
+ * The ABI carries plain pointers, sizes and status codes only.  Every entry
+ * returns an int status (LMB_OK = 0, negative = error) and never throws.
+ * Host pointers are host memory unless a name says "device".  All work of a
+ * lattice is ordered on the stream of the context that created it.
+ *
+ * Each declaration names the reference interface it stands in for (paths
+ * relative to the Lattice Microbes source tree).
+ */
+#ifndef LMB_H
+#define LMB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LMB_ABI_VERSION 1
+
+/* Status codes.  The reference throws lm::Exception / InvalidArgException /
+ * CUDAException (core/Exceptions.h, cuda/lm_cuda.h:89-92); here the same
+ * failures come back as codes and the C++ layer re-raises them. */
+#define LMB_OK 0
+#define LMB_E_ARG (-1)                 /* InvalidArgException */
+#define LMB_E_CUDA (-2)                /* CUDAException */
+#define LMB_E_NOMEM (-3)               /* device allocation failed */
+#define LMB_E_MODEL (-4)               /* model rejected (e.g. q > 0.5, MpdRdmeSolver.cu:415-421) */
+#define LMB_E_STATE (-5)               /* call out of order (no model, wrong lattice kind) */
+#define LMB_E_OVERFLOW_EXHAUSTED (-6)  /* "Too many particle overflows" (MpdRdmeSolver.cu:1122-1124) */
+#define LMB_E_OVERFLOW_UNRESOLVED (-7) /* "Unable to find an available site" (MpdRdmeSolver.cu:1155-1156) */
+#define LMB_E_TIMEOUT (-8)             /* a bounded device wait gave up */
+#define LMB_E_UNSUPPORTED (-9)         /* size or layout outside the compiled variants */
+
+/* Overflow handlers: parameter "rdme.mpd.overflowhandler" (MpdRdmeSolver.cu:126-146). */
+#define LMB_OVERFLOW_CLASSIC 0
+#define LMB_OVERFLOW_RELAXED 1
+
+/* Reaction types (CMESolver.h:79-112). */
+#define LMB_REACTION_ZEROTH 0
+#define LMB_REACTION_FIRST 1
+#define LMB_REACTION_SECOND 2
+#define LMB_REACTION_SECOND_SELF 3
+
+typedef struct lmb_ctx lmb_ctx;
+typedef struct lmb_model lmb_model;
+typedef struct lmb_lattice lmb_lattice;
+
+/* The reaction and diffusion model as the reference solver receives it:
+ * CMESolver::buildModel (cme/CMESolver.h:200-201) and
+ * RDMESolver::buildDiffusionModel (rdme/RDMESolver.h:57-67), plus the
+ * "timestep" parameter and the lattice spacing. */
+typedef struct {
+    uint32_t number_species;
+    uint32_t number_reactions;
+    uint32_t number_site_types;
+    const uint32_t *reaction_types; /* [R], LMB_REACTION_* */
+    const double *K;                /* [R * k_cols], rate constant in column 0 */
+    uint32_t k_cols;
+    const int32_t *S;               /* [NS * R] stoichiometry, species-major */
+    const uint32_t *D;              /* [NS * R] dependency (1 = reactant) */
+    const double *DF;               /* [NST * NST * NS] diffusion, m^2/s */
+    const uint32_t *RL;             /* [R * NST] reaction locations */
+    double timestep;                /* tau, s */
+    double lattice_spacing;         /* lambda, m */
+} lmb_model_desc;
+
+/* The FP32 per-timestep tables the kernels read (MpdRdmeSolver.cu:232-483,
+ * 697-787): T[src][dst][sp], qp0[st], qp1[st][sp], qp2[st][sp][sp], per-reaction
+ * order (1..4), 1-based reactants D1/D2, scaled rate, transposed S[rx][sp],
+ * RL[rx][st]. */
+typedef struct {
+    uint32_t number_species;
+    uint32_t number_reactions;
+    uint32_t number_site_types;
+    const float *T;
+    const float *qp0;
+    const float *qp1;
+    const float *qp2;
+    const uint32_t *order;
+    const uint32_t *D1;
+    const uint32_t *D2;
+    const float *rate;
+    const int8_t *S;
+    const uint8_t *RL;
+} lmb_tables;
+
+typedef struct {
+    int32_t status;         /* LMB_OK or the error that stopped the run */
+    uint32_t steps_done;    /* timesteps completed */
+    uint32_t failed_step;   /* timestep index that failed (if status != OK) */
+    uint32_t unresolved;    /* relaxed handler: particles still queued */
+    uint64_t overflows;     /* particles that left a full site */
+    uint64_t reactions;     /* reaction events */
+} lmb_run_stats;
+
+/* ---- library ------------------------------------------------------------ */
+int lmb_abi_version(void);
+const char *lmb_status_string(int status);
+
+/* MpdRdmeSolver::initialize seed composition (MpdRdmeSolver.cu:112-123). */
+uint32_t lmb_compose_seed(uint32_t seed_top, uint32_t replicate);
+/* MpdRdmeSolver::getTimestepSeed (MpdRdmeSolver.cu:987-994). */
+uint64_t lmb_timestep_hash(uint32_t seed, uint32_t timestep, uint32_t substep);
+
+/* ---- context: one device, one stream ------------------------------------
+ * Replaces the per-solver cudaSetDevice + cudaStreamCreate of
+ * ReplicateRunner::run / MpdRdmeSolver::initialize (MpdRdmeSolver.cu:161). */
+int lmb_ctx_create(int device, lmb_ctx **out);
+/* Uses an existing cudaStream_t (passed as void*) instead of creating one. */
+int lmb_ctx_create_on_stream(int device, void *cuda_stream, lmb_ctx **out);
+int lmb_ctx_destroy(lmb_ctx *ctx);
+void *lmb_ctx_stream(lmb_ctx *ctx);
+int lmb_ctx_synchronize(lmb_ctx *ctx);
+
+/* ---- model ---------------------------------------------------------------
+ * MpdRdmeSolver::buildModel + buildDiffusionModel + computePropensities +
+ * copyModelsToDevice (MpdRdmeSolver.cu:232-483, 697-787) for a lattice of
+ * X*Y*Z sites (the rates scale with the site count). */
+int lmb_model_create(lmb_ctx *ctx, const lmb_model_desc *desc, uint32_t X, uint32_t Y, uint32_t Z,
+                     lmb_model **out);
+/* The host half of lmb_model_create alone: fills caller arrays with the
+ * tables it would upload (sizes as in lmb_tables).  Needs no device. */
+int lmb_tables_build(const lmb_model_desc *desc, uint32_t X, uint32_t Y, uint32_t Z, float *T, float *qp0,
+                     float *qp1, float *qp2, uint32_t *order, uint32_t *D1, uint32_t *D2, float *rate,
+                     int8_t *S, uint8_t *RL);
+/* Same from ready FP32 tables (test and batch use). */
+int lmb_model_create_from_tables(lmb_ctx *ctx, const lmb_tables *tables, lmb_model **out);
+/* Copies the host copy of the tables out; NULL arrays are skipped. */
+int lmb_model_get_tables(const lmb_model *model, float *T, float *qp0, float *qp1, float *qp2,
+                         uint32_t *order, uint32_t *D1, uint32_t *D2, float *rate, int8_t *S,
+                         uint8_t *RL);
+/* MpdRdmeSolver::setReactionRate (MpdRdmeSolver.h:85, .cu:670-695): new
+ * rate constant (LM units) for one reaction; tables are rebuilt and uploaded
+ * before the next run. */
+int lmb_model_set_reaction_rate(lmb_model *model, uint32_t reaction, double rate);
+int lmb_model_destroy(lmb_model *model);
+
+/* ---- lattice -------------------------------------------------------------
+ * CudaByteLattice / CudaIntLattice (rdme/CudaByteLattice.cu:75-220,
+ * CudaIntLattice.cu:78-189): two device particle buffers and the site types.
+ * bytes_per_particle 1 = ByteLattice (4 slots per uint32 word), 4 = IntLattice.
+ * Native layout: word w of site i = x + y*X + z*X*Y at particles[w*N + i]. */
+int lmb_lattice_create(lmb_ctx *ctx, uint32_t X, uint32_t Y, uint32_t Z, uint32_t particles_per_site,
+                       uint32_t bytes_per_particle, lmb_lattice **out);
+int lmb_lattice_destroy(lmb_lattice *lattice);
+/* CudaByteLattice::copyToGPU / copyFromGPU with native host buffers
+ * (W*N uint32 words; N site types).  Either pointer may be NULL. */
+int lmb_lattice_set_native(lmb_lattice *lattice, const uint32_t *particles, const uint8_t *sites);
+int lmb_lattice_get_native(lmb_lattice *lattice, uint32_t *particles, uint8_t *sites);
+/* RDMESolver::setLatticeData / setLatticeSitesData (RDMESolver.cpp:144-189):
+ * row-major [x][y][z][p] particles (uint8 for byte lattices, uint32 for int
+ * lattices) and [x][y][z] site types; each particle is added to the first
+ * free slot; ids above number_species or site types >= number_site_types are
+ * rejected.  get_row_major is ByteLattice::copyNativeToRowMajorByte
+ * (ByteLattice.cpp:371-402). */
+int lmb_lattice_set_row_major(lmb_lattice *lattice, const void *particles, const uint8_t *sites,
+                              uint32_t number_species, uint32_t number_site_types);
+int lmb_lattice_get_row_major(lmb_lattice *lattice, void *particles, uint8_t *sites);
+/* Device pointers of the current particle buffer and of the site types. */
+int lmb_lattice_device_buffers(lmb_lattice *lattice, void **particles, void **sites);
+/* ByteLattice::getParticleCounts (ByteLattice.cpp:495-520), computed on the
+ * device: counts[s] for s = 0..number_species (counts[0] is 0). */
+int lmb_lattice_species_counts(lmb_lattice *lattice, uint32_t number_species, uint64_t *counts);
+
+/* ---- timesteps -----------------------------------------------------------
+ * number_timesteps calls of MpdRdmeSolver::runTimestep (MpdRdmeSolver.cu:
+ * 996-1193), timestep indices first_timestep.., with `seed` the composed
+ * 32-bit solver seed.  Overflow handling runs on the device; the classic
+ * handler gives the reference's result for the reinsertion order sorted by
+ * (sweep, site, slot).  Blocks until done; stats may be NULL. */
+int lmb_run(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
+            uint32_t number_timesteps, int overflow_mode, lmb_run_stats *stats);
+/* Enqueues the same work and returns; lmb_run_wait blocks and reports. */
+int lmb_run_async(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
+                  uint32_t number_timesteps, int overflow_mode);
+int lmb_run_wait(lmb_lattice *lattice, lmb_run_stats *stats);
+
+/* lmb_run with a CUDA event pair around every kernel on the lattice's
+ * stream; phase_ms[5] / phase_launches[5] receive the summed device time and
+ * launch count of the x, y, z sweeps, the reaction and the overflow kernel. */
+int lmb_run_profiled(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
+                     uint32_t number_timesteps, int overflow_mode, float *phase_ms, uint32_t *phase_launches,
+                     lmb_run_stats *stats);
+
+/* Launch counters for the bench's kernel accounting. */
+uint64_t lmb_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,8 @@
+"""B200-native MPD-RDME solver for Lattice Microbes models.
+
+The solver runs in liblmb200.so (CUDA for sm_100a behind the C ABI in
+include/lmb.h).  ``solver`` is the Python face of that ABI; ``configs``
+generates seeded synthetic problems.  Importing ``solver`` fails when the
+library has not been built: there is no CPU fallback.
+"""
+__all__ = ["configs", "solver"]

@@ -1,0 +1,845 @@
+// lmb_capi.cu -- the C ABI declared in include/lmb.h.
+//
+// Host side of the solver: model building (the reference's
+// MpdRdmeSolver::buildModel / buildDiffusionModel / computePropensities,
+// restated), device buffers, and the timestep loop that queues the per-phase
+// kernels of lmb_kernels.cu on the context stream.  Nothing here throws; every
+// entry returns a status code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "lmb.h"
+#include "lmb_device.cuh"
+#include "lmb_internal.h"
+
+using namespace lmb;
+
+namespace lmb {
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(uint64_t n) { g_launches += n; }
+}  // namespace lmb
+
+struct lmb_ctx {
+    int device;
+    cudaStream_t stream;
+    bool own_stream;
+};
+
+struct lmb_model {
+    lmb_ctx *ctx;
+    uint32_t ns, nst, nr;
+    uint32_t X, Y, Z;
+    bool has_desc;
+    // Reference-side inputs kept for setReactionRate.
+    std::vector<uint32_t> rtype, s1, s2;
+    std::vector<double> K;
+    std::vector<uint32_t> RLin;
+    double tau;
+    // Host copy of the FP32 tables.
+    std::vector<float> T, qp0, qp1, qp2, rate;
+    std::vector<uint32_t> order, D1, D2;
+    std::vector<int8_t> S;
+    std::vector<uint8_t> RL;
+    std::vector<uint32_t> st_off, st_sp;
+    std::vector<int32_t> st_d;
+    // Device copy.
+    void *dev_block;
+    size_t dev_bytes;
+    DevTables dev;
+    bool dirty;
+};
+
+struct lmb_lattice {
+    lmb_ctx *ctx;
+    Geometry g;
+    uint32_t bps, slots, words;
+    uint32_t *buf[2];
+    int cur;
+    uint8_t *sites;
+    RunState *rs;
+    RunState *rs_host;  // pinned
+    OverflowEntry *list;
+    uint32_t cap;
+    unsigned long long *counts_dev;
+    uint32_t counts_len;
+    bool validated;
+    uint32_t max_species, max_site_type;
+    // Pending async run.
+    bool pending;
+    int pending_cur0;
+    uint32_t pending_first, pending_n;
+};
+
+#define CK(call)                                      \
+    do {                                              \
+        cudaError_t e_ = (call);                      \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+static int cuda_status(cudaError_t e)
+{
+    if (e == cudaErrorMemoryAllocation) return LMB_E_NOMEM;
+    return LMB_E_CUDA;
+}
+
+extern "C" int lmb_abi_version(void) { return LMB_ABI_VERSION; }
+
+extern "C" const char *lmb_status_string(int s)
+{
+    switch (s) {
+    case LMB_OK: return "ok";
+    case LMB_E_ARG: return "invalid argument";
+    case LMB_E_CUDA: return "CUDA error";
+    case LMB_E_NOMEM: return "device out of memory";
+    case LMB_E_MODEL: return "model rejected";
+    case LMB_E_STATE: return "invalid call order or state";
+    case LMB_E_OVERFLOW_EXHAUSTED: return "Too many particle overflows for the available buffer";
+    case LMB_E_OVERFLOW_UNRESOLVED: return "Unable to find an available site to handle a particle overflow";
+    case LMB_E_TIMEOUT: return "device wait timed out";
+    case LMB_E_UNSUPPORTED: return "unsupported lattice layout or size";
+    default: return "unknown status";
+    }
+}
+
+extern "C" uint32_t lmb_compose_seed(uint32_t seed_top, uint32_t replicate)
+{
+    return (uint32_t)((seed_top << 16) | (replicate & 0xFFFFu));
+}
+
+extern "C" uint64_t lmb_timestep_hash(uint32_t seed, uint32_t timestep, uint32_t substep)
+{
+    return timestep_hash(seed, timestep, substep);
+}
+
+extern "C" uint64_t lmb_kernel_launches(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+
+extern "C" int lmb_ctx_create_on_stream(int device, void *stream, lmb_ctx **out)
+{
+    if (!out) return LMB_E_ARG;
+    *out = nullptr;
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return LMB_E_ARG;
+    CK(cudaSetDevice(device));
+    lmb_ctx *c = new (std::nothrow) lmb_ctx;
+    if (!c) return LMB_E_NOMEM;
+    c->device = device;
+    c->own_stream = stream == nullptr;
+    if (stream) c->stream = (cudaStream_t)stream;
+    else {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete c;
+            return cuda_status(e);
+        }
+    }
+    *out = c;
+    return LMB_OK;
+}
+
+extern "C" int lmb_ctx_create(int device, lmb_ctx **out) { return lmb_ctx_create_on_stream(device, nullptr, out); }
+
+extern "C" int lmb_ctx_destroy(lmb_ctx *c)
+{
+    if (!c) return LMB_E_ARG;
+    cudaSetDevice(c->device);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return LMB_OK;
+}
+
+extern "C" void *lmb_ctx_stream(lmb_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+extern "C" int lmb_ctx_synchronize(lmb_ctx *c)
+{
+    if (!c) return LMB_E_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    return LMB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Model
+// ---------------------------------------------------------------------------
+
+// computePropensities (MpdRdmeSolver.cu:697-774): per-reaction scaled rates
+// and the per-site-type qp0/qp1/qp2 tables.  "float += double" expressions of
+// the reference round once after a double add, and are evaluated that way.
+static void compute_propensities(lmb_model *m)
+{
+    const uint32_t X = m->X, Y = m->Y, Z = m->Z, ns = m->ns, nst = m->nst, nr = m->nr;
+    const double tau = m->tau;
+    const uint32_t nsites_u = X * Y * Z;
+    for (uint32_t r = 0; r < nr; r++) {
+        const double k = m->K[r];
+        switch (m->rtype[r]) {
+        case LMB_REACTION_ZEROTH: m->rate[r] = (float)(k * tau / (double)nsites_u); break;
+        case LMB_REACTION_FIRST: m->rate[r] = (float)(k * tau); break;
+        default: m->rate[r] = (float)(k * tau * X * Y * Z); break;
+        }
+    }
+    const float scale = (float)nsites_u;
+    for (uint32_t st = 0; st < nst; st++) {
+        const size_t o1 = (size_t)st * ns, o2 = (size_t)st * ns * ns;
+        m->qp0[st] = 0.0f;
+        std::fill(m->qp1.begin() + o1, m->qp1.begin() + o1 + ns, 0.0f);
+        std::fill(m->qp2.begin() + o2, m->qp2.begin() + o2 + (size_t)ns * ns, 0.0f);
+        for (uint32_t r = 0; r < nr; r++) {
+            if (!m->RLin[(size_t)r * nst + st]) continue;
+            const double k = m->K[r];
+            const uint32_t a = m->s1[r], b = m->s2[r];
+            switch (m->rtype[r]) {
+            case LMB_REACTION_ZEROTH: m->qp0[st] = (float)((double)m->qp0[st] + k * tau / (double)scale); break;
+            case LMB_REACTION_FIRST: m->qp1[o1 + a] = (float)((double)m->qp1[o1 + a] + k * tau); break;
+            case LMB_REACTION_SECOND:
+                // Assignment, not accumulation (MpdRdmeSolver.cu:760-764).
+                m->qp2[o2 + (size_t)a * ns + b] = (float)(k * tau * (double)scale);
+                m->qp2[o2 + (size_t)b * ns + a] = (float)(k * tau * (double)scale);
+                break;
+            case LMB_REACTION_SECOND_SELF: {
+                const size_t e = o2 + (size_t)a * ns + a;
+                m->qp2[e] = (float)((double)m->qp2[e] + k * tau * (double)scale * 2);
+                break;
+            }
+            }
+        }
+    }
+}
+
+static int upload_model(lmb_model *m)
+{
+    lmb_ctx *c = m->ctx;
+    CK(cudaSetDevice(c->device));
+    // One device block holding every table, 256-byte aligned pieces.
+    std::vector<std::pair<const void *, size_t>> parts = {
+        {m->T.data(), m->T.size() * 4},          {m->qp0.data(), m->qp0.size() * 4},
+        {m->qp1.data(), m->qp1.size() * 4},      {m->qp2.data(), m->qp2.size() * 4},
+        {m->order.data(), m->order.size() * 4},  {m->D1.data(), m->D1.size() * 4},
+        {m->D2.data(), m->D2.size() * 4},        {m->rate.data(), m->rate.size() * 4},
+        {m->RL.data(), m->RL.size()},            {m->st_off.data(), m->st_off.size() * 4},
+        {m->st_sp.data(), m->st_sp.size() * 4},  {m->st_d.data(), m->st_d.size() * 4}};
+    std::vector<size_t> off(parts.size());
+    size_t total = 0;
+    for (size_t i = 0; i < parts.size(); i++) {
+        off[i] = total;
+        total += (parts[i].second + 255) & ~(size_t)255;
+        if (parts[i].second == 0) total += 256;
+    }
+    if (!m->dev_block || m->dev_bytes < total) {
+        if (m->dev_block) cudaFree(m->dev_block);
+        m->dev_block = nullptr;
+        CK(cudaMalloc(&m->dev_block, total));
+        m->dev_bytes = total;
+    }
+    std::vector<uint8_t> staging(total, 0);
+    for (size_t i = 0; i < parts.size(); i++)
+        if (parts[i].second) memcpy(staging.data() + off[i], parts[i].first, parts[i].second);
+    CK(cudaMemcpyAsync(m->dev_block, staging.data(), total, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    uint8_t *b = (uint8_t *)m->dev_block;
+    m->dev.ns = m->ns;
+    m->dev.nst = m->nst;
+    m->dev.nr = m->nr;
+    m->dev.T = (const float *)(b + off[0]);
+    m->dev.qp0 = (const float *)(b + off[1]);
+    m->dev.qp1 = (const float *)(b + off[2]);
+    m->dev.qp2 = (const float *)(b + off[3]);
+    m->dev.order = (const uint32_t *)(b + off[4]);
+    m->dev.D1 = (const uint32_t *)(b + off[5]);
+    m->dev.D2 = (const uint32_t *)(b + off[6]);
+    m->dev.rate = (const float *)(b + off[7]);
+    m->dev.RL = (const uint8_t *)(b + off[8]);
+    m->dev.stoich_off = (const uint32_t *)(b + off[9]);
+    m->dev.stoich_sp = (const uint32_t *)(b + off[10]);
+    m->dev.stoich_d = (const int32_t *)(b + off[11]);
+    m->dirty = false;
+    return LMB_OK;
+}
+
+// Sparse per-reaction stoichiometry from the transposed S (ascending species).
+static int build_stoich(lmb_model *m)
+{
+    m->st_off.assign(m->nr + 1, 0);
+    m->st_sp.clear();
+    m->st_d.clear();
+    for (uint32_t r = 0; r < m->nr; r++) {
+        m->st_off[r] = (uint32_t)m->st_sp.size();
+        uint32_t cnt = 0;
+        for (uint32_t s = 0; s < m->ns; s++) {
+            const int8_t v = m->S[(size_t)r * m->ns + s];
+            if (v != 0) {
+                m->st_sp.push_back(s);
+                m->st_d.push_back(v);
+                cnt++;
+            }
+        }
+        if (cnt > 32) return LMB_E_UNSUPPORTED;
+    }
+    m->st_off[m->nr] = (uint32_t)m->st_sp.size();
+    return LMB_OK;
+}
+
+extern "C" int lmb_model_get_tables(const lmb_model *m, float *T, float *qp0, float *qp1, float *qp2,
+                                    uint32_t *order, uint32_t *D1, uint32_t *D2, float *rate, int8_t *S,
+                                    uint8_t *RL);
+
+static lmb_model *new_model(lmb_ctx *c, uint32_t ns, uint32_t nst, uint32_t nr)
+{
+    lmb_model *m = new (std::nothrow) lmb_model;
+    if (!m) return nullptr;
+    m->ctx = c;
+    m->ns = ns;
+    m->nst = nst;
+    m->nr = nr;
+    m->X = m->Y = m->Z = 0;
+    m->has_desc = false;
+    m->tau = 0;
+    m->dev_block = nullptr;
+    m->dev_bytes = 0;
+    m->dirty = true;
+    m->T.assign((size_t)nst * nst * ns, 0.0f);
+    m->qp0.assign(nst, 0.0f);
+    m->qp1.assign((size_t)nst * ns, 0.0f);
+    m->qp2.assign((size_t)nst * ns * ns, 0.0f);
+    m->rate.assign(nr, 0.0f);
+    m->order.assign(nr, 0);
+    m->D1.assign(nr, 0);
+    m->D2.assign(nr, 0);
+    m->S.assign((size_t)nr * ns, 0);
+    m->RL.assign((size_t)nr * nst, 0);
+    return m;
+}
+
+// Fills a model's host tables from reference-style inputs; no device work.
+static int build_model_host(const lmb_model_desc *d, uint32_t X, uint32_t Y, uint32_t Z, lmb_model *m)
+{
+    const uint32_t ns = d->number_species, nr = d->number_reactions, nst = d->number_site_types;
+    m->X = X;
+    m->Y = Y;
+    m->Z = Z;
+    m->has_desc = true;
+    m->tau = d->timestep;
+    m->rtype.assign(d->reaction_types, d->reaction_types + nr);
+    m->K.resize(nr);
+    for (uint32_t r = 0; r < nr; r++) m->K[r] = d->K[(size_t)r * d->k_cols];
+    m->RLin.assign(d->RL, d->RL + (size_t)nr * nst);
+    m->s1.assign(nr, 0);
+    m->s2.assign(nr, 0);
+    // Reactants from the dependency columns (CMESolver.cpp:340-430) and the
+    // device order / 1-based ids (MpdRdmeSolver.cu:265-302).
+    for (uint32_t r = 0; r < nr; r++) {
+        uint32_t deps[3], nd = 0;
+        for (uint32_t s = 0; s < ns; s++)
+            if (d->D[(size_t)s * nr + r] == 1) {
+                if (nd < 3) deps[nd] = s;
+                nd++;
+            }
+        const uint32_t t = m->rtype[r];
+        bool ok = (t == LMB_REACTION_ZEROTH && nd == 0) || (t == LMB_REACTION_FIRST && nd == 1) ||
+                  (t == LMB_REACTION_SECOND && nd == 2) || (t == LMB_REACTION_SECOND_SELF && nd == 1);
+        if (!ok) return LMB_E_MODEL;
+        m->order[r] = t + 1;
+        if (nd >= 1) m->s1[r] = deps[0];
+        if (nd >= 2) m->s2[r] = deps[1];
+        m->D1[r] = t == LMB_REACTION_ZEROTH ? 0 : m->s1[r] + 1;
+        m->D2[r] = t == LMB_REACTION_SECOND ? m->s2[r] + 1 : 0;
+    }
+    // T[src][dst][sp] = (float)(DF * tau / spacing^2), q > 0.5 rejected
+    // (MpdRdmeSolver.cu:407-421).
+    for (size_t i = 0; i < m->T.size(); i++) {
+        const float q = (float)(d->DF[i] * d->timestep / pow(d->lattice_spacing, 2));
+        if (q > 0.50f) return LMB_E_MODEL;
+        m->T[i] = q;
+    }
+    // SG[rx][sp] = S[sp][rx] (MpdRdmeSolver.cu:312-321); RL as bytes.
+    for (uint32_t r = 0; r < nr; r++)
+        for (uint32_t s = 0; s < ns; s++) m->S[(size_t)r * ns + s] = (int8_t)d->S[(size_t)s * nr + r];
+    for (size_t i = 0; i < m->RL.size(); i++) m->RL[i] = (uint8_t)m->RLin[i];
+    int rc = build_stoich(m);
+    if (rc != LMB_OK) return rc;
+    compute_propensities(m);
+    return LMB_OK;
+}
+
+static int check_desc(const lmb_model_desc *d, uint32_t X, uint32_t Y, uint32_t Z)
+{
+    if (!d || X == 0 || Y == 0 || Z == 0) return LMB_E_ARG;
+    const uint32_t ns = d->number_species, nr = d->number_reactions, nst = d->number_site_types;
+    if (ns == 0 || nst == 0 || nst > 256) return LMB_E_ARG;
+    if (nr > 0 && (!d->reaction_types || !d->K || d->k_cols == 0 || !d->S || !d->D || !d->RL)) return LMB_E_ARG;
+    if (!d->DF || !(d->timestep > 0.0) || !(d->lattice_spacing > 0.0)) return LMB_E_ARG;
+    return LMB_OK;
+}
+
+extern "C" int lmb_model_create(lmb_ctx *c, const lmb_model_desc *d, uint32_t X, uint32_t Y, uint32_t Z,
+                                lmb_model **out)
+{
+    if (!c || !out) return LMB_E_ARG;
+    *out = nullptr;
+    int rc = check_desc(d, X, Y, Z);
+    if (rc) return rc;
+    lmb_model *m = new_model(c, d->number_species, d->number_site_types, d->number_reactions);
+    if (!m) return LMB_E_NOMEM;
+    rc = build_model_host(d, X, Y, Z, m);
+    if (rc == LMB_OK) rc = upload_model(m);
+    if (rc != LMB_OK) {
+        if (m->dev_block) cudaFree(m->dev_block);
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return LMB_OK;
+}
+
+extern "C" int lmb_tables_build(const lmb_model_desc *d, uint32_t X, uint32_t Y, uint32_t Z, float *T, float *qp0,
+                                float *qp1, float *qp2, uint32_t *order, uint32_t *D1, uint32_t *D2, float *rate,
+                                int8_t *S, uint8_t *RL)
+{
+    int rc = check_desc(d, X, Y, Z);
+    if (rc) return rc;
+    lmb_model *m = new_model(nullptr, d->number_species, d->number_site_types, d->number_reactions);
+    if (!m) return LMB_E_NOMEM;
+    rc = build_model_host(d, X, Y, Z, m);
+    if (rc == LMB_OK) rc = lmb_model_get_tables(m, T, qp0, qp1, qp2, order, D1, D2, rate, S, RL);
+    delete m;
+    return rc;
+}
+
+extern "C" int lmb_model_create_from_tables(lmb_ctx *c, const lmb_tables *t, lmb_model **out)
+{
+    if (!c || !t || !out || t->number_species == 0 || t->number_site_types == 0 || t->number_site_types > 256)
+        return LMB_E_ARG;
+    *out = nullptr;
+    const uint32_t ns = t->number_species, nst = t->number_site_types, nr = t->number_reactions;
+    if (!t->T || !t->qp0 || !t->qp1 || !t->qp2) return LMB_E_ARG;
+    if (nr && (!t->order || !t->D1 || !t->D2 || !t->rate || !t->S || !t->RL)) return LMB_E_ARG;
+    lmb_model *m = new_model(c, ns, nst, nr);
+    if (!m) return LMB_E_NOMEM;
+    std::copy(t->T, t->T + m->T.size(), m->T.begin());
+    std::copy(t->qp0, t->qp0 + m->qp0.size(), m->qp0.begin());
+    std::copy(t->qp1, t->qp1 + m->qp1.size(), m->qp1.begin());
+    std::copy(t->qp2, t->qp2 + m->qp2.size(), m->qp2.begin());
+    if (nr) {
+        std::copy(t->order, t->order + nr, m->order.begin());
+        std::copy(t->D1, t->D1 + nr, m->D1.begin());
+        std::copy(t->D2, t->D2 + nr, m->D2.begin());
+        std::copy(t->rate, t->rate + nr, m->rate.begin());
+        std::copy(t->S, t->S + m->S.size(), m->S.begin());
+        std::copy(t->RL, t->RL + m->RL.size(), m->RL.begin());
+    }
+    for (float q : m->T)
+        if (q > 0.50f) {
+            delete m;
+            return LMB_E_MODEL;
+        }
+    int rc = build_stoich(m);
+    if (rc == LMB_OK) rc = upload_model(m);
+    if (rc != LMB_OK) {
+        if (m->dev_block) cudaFree(m->dev_block);
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return LMB_OK;
+}
+
+extern "C" int lmb_model_get_tables(const lmb_model *m, float *T, float *qp0, float *qp1, float *qp2,
+                                    uint32_t *order, uint32_t *D1, uint32_t *D2, float *rate, int8_t *S,
+                                    uint8_t *RL)
+{
+    if (!m) return LMB_E_ARG;
+    if (T) std::copy(m->T.begin(), m->T.end(), T);
+    if (qp0) std::copy(m->qp0.begin(), m->qp0.end(), qp0);
+    if (qp1) std::copy(m->qp1.begin(), m->qp1.end(), qp1);
+    if (qp2) std::copy(m->qp2.begin(), m->qp2.end(), qp2);
+    if (order) std::copy(m->order.begin(), m->order.end(), order);
+    if (D1) std::copy(m->D1.begin(), m->D1.end(), D1);
+    if (D2) std::copy(m->D2.begin(), m->D2.end(), D2);
+    if (rate) std::copy(m->rate.begin(), m->rate.end(), rate);
+    if (S) std::copy(m->S.begin(), m->S.end(), S);
+    if (RL) std::copy(m->RL.begin(), m->RL.end(), RL);
+    return LMB_OK;
+}
+
+extern "C" int lmb_model_set_reaction_rate(lmb_model *m, uint32_t reaction, double rate)
+{
+    if (!m || reaction >= m->nr) return LMB_E_ARG;
+    if (!m->has_desc) return LMB_E_STATE;
+    m->K[reaction] = rate;
+    compute_propensities(m);
+    m->dirty = true;
+    return LMB_OK;
+}
+
+extern "C" int lmb_model_destroy(lmb_model *m)
+{
+    if (!m) return LMB_E_ARG;
+    if (m->dev_block) {
+        cudaSetDevice(m->ctx->device);
+        cudaStreamSynchronize(m->ctx->stream);
+        cudaFree(m->dev_block);
+    }
+    delete m;
+    return LMB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Lattice
+// ---------------------------------------------------------------------------
+
+static const uint32_t DEFAULT_OVERFLOW_CAPACITY = 2048;  // TUNE_MPD_MAX_PARTICLE_OVERFLOWS
+
+extern "C" int lmb_lattice_create(lmb_ctx *c, uint32_t X, uint32_t Y, uint32_t Z, uint32_t slots, uint32_t bps,
+                                  lmb_lattice **out)
+{
+    if (!c || !out || X == 0 || Y == 0 || Z == 0) return LMB_E_ARG;
+    *out = nullptr;
+    if (!slots_supported((int)bps, (int)slots)) return LMB_E_UNSUPPORTED;
+    const uint64_t N = (uint64_t)X * Y * Z;
+    if (N > 0xFFFFFFFFull) return LMB_E_UNSUPPORTED;  // site indices are 32-bit
+    CK(cudaSetDevice(c->device));
+    lmb_lattice *l = new (std::nothrow) lmb_lattice;
+    if (!l) return LMB_E_NOMEM;
+    memset(l, 0, sizeof(*l));
+    l->ctx = c;
+    l->g.X = X;
+    l->g.Y = Y;
+    l->g.Z = Z;
+    l->g.XY = X * Y;
+    l->g.N = (uint32_t)N;
+    l->bps = bps;
+    l->slots = slots;
+    l->words = bps == 1 ? slots / 4 : slots;
+    l->cap = DEFAULT_OVERFLOW_CAPACITY;
+    const size_t wbytes = (size_t)l->words * N * sizeof(uint32_t);
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc(&l->buf[0], wbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&l->buf[1], wbytes);
+    if (e == cudaSuccess) e = cudaMalloc(&l->sites, N);
+    if (e == cudaSuccess) e = cudaMalloc(&l->rs, sizeof(RunState));
+    if (e == cudaSuccess) e = cudaMalloc(&l->list, sizeof(OverflowEntry) * l->cap);
+    if (e == cudaSuccess) e = cudaMallocHost(&l->rs_host, sizeof(RunState));
+    if (e == cudaSuccess) e = cudaMemsetAsync(l->buf[0], 0, wbytes, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l->buf[1], 0, wbytes, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l->sites, 0, N, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(l->rs, 0, sizeof(RunState), c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        lmb_lattice_destroy(l);
+        return cuda_status(e);
+    }
+    l->validated = false;
+    *out = l;
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_destroy(lmb_lattice *l)
+{
+    if (!l) return LMB_E_ARG;
+    cudaSetDevice(l->ctx->device);
+    cudaStreamSynchronize(l->ctx->stream);
+    if (l->buf[0]) cudaFree(l->buf[0]);
+    if (l->buf[1]) cudaFree(l->buf[1]);
+    if (l->sites) cudaFree(l->sites);
+    if (l->rs) cudaFree(l->rs);
+    if (l->list) cudaFree(l->list);
+    if (l->counts_dev) cudaFree(l->counts_dev);
+    if (l->rs_host) cudaFreeHost(l->rs_host);
+    delete l;
+    return LMB_OK;
+}
+
+static void reset_overflow_queue(lmb_lattice *l)
+{
+    // A new lattice state drops whatever the relaxed handler had queued.
+    RunState z;
+    memset(&z, 0, sizeof(z));
+    *l->rs_host = z;
+}
+
+extern "C" int lmb_lattice_set_native(lmb_lattice *l, const uint32_t *particles, const uint8_t *sites)
+{
+    if (!l || l->pending) return l ? LMB_E_STATE : LMB_E_ARG;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    if (particles)
+        CK(cudaMemcpyAsync(l->buf[l->cur], particles, (size_t)l->words * l->g.N * 4, cudaMemcpyHostToDevice, c->stream));
+    if (sites) CK(cudaMemcpyAsync(l->sites, sites, l->g.N, cudaMemcpyHostToDevice, c->stream));
+    reset_overflow_queue(l);
+    CK(cudaMemcpyAsync(l->rs, l->rs_host, sizeof(RunState), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    l->validated = false;
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_get_native(lmb_lattice *l, uint32_t *particles, uint8_t *sites)
+{
+    if (!l || l->pending) return l ? LMB_E_STATE : LMB_E_ARG;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    if (particles)
+        CK(cudaMemcpyAsync(particles, l->buf[l->cur], (size_t)l->words * l->g.N * 4, cudaMemcpyDeviceToHost, c->stream));
+    if (sites) CK(cudaMemcpyAsync(sites, l->sites, l->g.N, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_set_row_major(lmb_lattice *l, const void *particles, const uint8_t *sites,
+                                         uint32_t number_species, uint32_t number_site_types)
+{
+    if (!l || !particles || !sites) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    const size_t pbytes = (size_t)l->g.N * l->slots * l->bps;
+    void *tmp = nullptr;
+    uint8_t *tmp_sites = nullptr;
+    CK(cudaMalloc(&tmp, pbytes));
+    cudaError_t e = cudaMalloc(&tmp_sites, l->g.N);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, particles, pbytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp_sites, sites, l->g.N, cudaMemcpyHostToDevice, c->stream);
+    reset_overflow_queue(l);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(l->rs, l->rs_host, sizeof(RunState), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = launch_row_major_to_native((int)l->bps, (int)l->slots, tmp, tmp_sites, l->buf[l->cur], l->sites, l->g,
+                                       l->rs, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (tmp_sites) cudaFree(tmp_sites);
+    if (e != cudaSuccess) return cuda_status(e);
+    // RDMESolver.cpp:160-185 rejects invalid species ids and site types.
+    if (l->rs_host->max_species > number_species || l->rs_host->max_site_type >= number_site_types) {
+        return LMB_E_ARG;
+    }
+    l->validated = false;
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_get_row_major(lmb_lattice *l, void *particles, uint8_t *sites)
+{
+    if (!l || !particles) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    const size_t pbytes = (size_t)l->g.N * l->slots * l->bps;
+    void *tmp = nullptr;
+    uint8_t *tmp_sites = nullptr;
+    CK(cudaMalloc(&tmp, pbytes));
+    cudaError_t e = sites ? cudaMalloc(&tmp_sites, l->g.N) : cudaSuccess;
+    if (e == cudaSuccess)
+        e = launch_native_to_row_major((int)l->bps, (int)l->slots, l->buf[l->cur], l->sites, tmp, tmp_sites, l->g,
+                                       c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(particles, tmp, pbytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && sites) e = cudaMemcpyAsync(sites, tmp_sites, l->g.N, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (tmp_sites) cudaFree(tmp_sites);
+    if (e != cudaSuccess) return cuda_status(e);
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_device_buffers(lmb_lattice *l, void **particles, void **sites)
+{
+    if (!l) return LMB_E_ARG;
+    if (particles) *particles = l->buf[l->cur];
+    if (sites) *sites = l->sites;
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_species_counts(lmb_lattice *l, uint32_t ns, uint64_t *counts)
+{
+    if (!l || !counts) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    if (!l->counts_dev || l->counts_len < ns + 1) {
+        if (l->counts_dev) cudaFree(l->counts_dev);
+        l->counts_dev = nullptr;
+        CK(cudaMalloc(&l->counts_dev, sizeof(unsigned long long) * (ns + 1)));
+        l->counts_len = ns + 1;
+    }
+    CK(cudaMemsetAsync(l->counts_dev, 0, sizeof(unsigned long long) * (ns + 1), c->stream));
+    CK(launch_counts((int)l->bps, (int)l->slots, l->buf[l->cur], l->g, ns, l->counts_dev, c->stream));
+    CK(cudaMemcpyAsync(counts, l->counts_dev, sizeof(uint64_t) * (ns + 1), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    counts[0] = 0;
+    return LMB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Timesteps
+// ---------------------------------------------------------------------------
+
+static int validate_for_model(lmb_lattice *l, const lmb_model *m)
+{
+    if (!l->validated) {
+        lmb_ctx *c = l->ctx;
+        CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        l->rs_host->max_species = 0;
+        l->rs_host->max_site_type = 0;
+        CK(cudaMemcpyAsync(l->rs, l->rs_host, sizeof(RunState), cudaMemcpyHostToDevice, c->stream));
+        CK(launch_validate((int)l->bps, (int)l->slots, l->buf[l->cur], l->sites, l->g, l->rs, c->stream));
+        CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        l->max_species = l->rs_host->max_species;
+        l->max_site_type = l->rs_host->max_site_type;
+        l->validated = true;
+    }
+    // Species ids index the qp tables unchecked on the device
+    // (MpdRdmeSolver.cu:1617-1636), as the reference assumes after
+    // RDMESolver::setLatticeData validated them.
+    if (l->max_species > m->ns || l->max_site_type >= m->nst) return LMB_E_ARG;
+    return LMB_OK;
+}
+
+extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_t first, uint32_t n, int mode)
+{
+    if (!l || !mc) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    if (mode != LMB_OVERFLOW_CLASSIC && mode != LMB_OVERFLOW_RELAXED) return LMB_E_ARG;
+    lmb_model *m = const_cast<lmb_model *>(mc);
+    if (m->ctx->device != l->ctx->device) return LMB_E_ARG;
+    if (m->has_desc && (m->X != l->g.X || m->Y != l->g.Y || m->Z != l->g.Z)) return LMB_E_ARG;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    if (m->dirty) {
+        int rc = upload_model(m);
+        if (rc) return rc;
+    }
+    int rc = validate_for_model(l, m);
+    if (rc) return rc;
+    CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream));
+    const int bps = (int)l->bps, S = (int)l->slots;
+    l->pending_cur0 = l->cur;
+    for (uint32_t s = 0; s < n; s++) {
+        uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
+        CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        l->cur ^= 1;
+        if (m->nr > 0)
+            CK(launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, c->stream));
+    }
+    CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));
+    l->pending = true;
+    l->pending_first = first;
+    l->pending_n = n;
+    return LMB_OK;
+}
+
+extern "C" int lmb_run_wait(lmb_lattice *l, lmb_run_stats *st)
+{
+    if (!l) return LMB_E_ARG;
+    if (!l->pending) return LMB_E_STATE;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    l->pending = false;
+    CK(cudaStreamSynchronize(c->stream));
+    const RunState &h = *l->rs_host;
+    uint32_t done = h.status == LMB_OK ? l->pending_n : h.failed_step - l->pending_first;
+    if (h.status != LMB_OK) {
+        // Kernels after the failing step did nothing: the lattice sits in the
+        // buffer reached after done + 1 steps (each step flips once).
+        l->cur = l->pending_cur0 ^ (int)((done + 1) & 1u);
+    }
+    if (st) {
+        st->status = h.status;
+        st->steps_done = done;
+        st->failed_step = h.status == LMB_OK ? 0 : h.failed_step;
+        st->unresolved = h.mode == LMB_OVERFLOW_RELAXED ? h.ovf_count : 0;
+        st->overflows = h.overflows;
+        st->reactions = h.reactions;
+    }
+    return h.status;
+}
+
+extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_t first, uint32_t n,
+                                int mode, float *phase_ms, uint32_t *phase_launches, lmb_run_stats *st)
+{
+    // Same work as lmb_run with a CUDA event pair around every kernel, on the
+    // lattice's stream.  phase order: x, y, z sweeps, reaction, overflow.
+    if (!l || !mc || !phase_ms || !phase_launches) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    lmb_model *m = const_cast<lmb_model *>(mc);
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    if (m->dirty) {
+        int rc = upload_model(m);
+        if (rc) return rc;
+    }
+    int rc = validate_for_model(l, m);
+    if (rc) return rc;
+    CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream));
+    std::vector<cudaEvent_t> ev((size_t)n * 10);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    const int bps = (int)l->bps, S = (int)l->slots;
+    const int cur0 = l->cur;
+    for (uint32_t s = 0; s < n; s++) {
+        uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
+        cudaEvent_t *E = &ev[(size_t)s * 10];
+        CK(cudaEventRecord(E[0], c->stream));
+        CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(cudaEventRecord(E[1], c->stream));
+        CK(cudaEventRecord(E[2], c->stream));
+        CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(cudaEventRecord(E[3], c->stream));
+        CK(cudaEventRecord(E[4], c->stream));
+        CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(cudaEventRecord(E[5], c->stream));
+        l->cur ^= 1;
+        CK(cudaEventRecord(E[6], c->stream));
+        if (m->nr > 0)
+            CK(launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(cudaEventRecord(E[7], c->stream));
+        CK(cudaEventRecord(E[8], c->stream));
+        CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, c->stream));
+        CK(cudaEventRecord(E[9], c->stream));
+    }
+    CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int p = 0; p < 5; p++) {
+        phase_ms[p] = 0.0f;
+        phase_launches[p] = 0;
+    }
+    for (uint32_t s = 0; s < n; s++)
+        for (int p = 0; p < 5; p++) {
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, ev[(size_t)s * 10 + 2 * p], ev[(size_t)s * 10 + 2 * p + 1]));
+            phase_ms[p] += ms;
+            if (p != 3 || m->nr > 0) phase_launches[p] += 1;
+        }
+    for (auto &e : ev) cudaEventDestroy(e);
+    const RunState &h = *l->rs_host;
+    const uint32_t done = h.status == LMB_OK ? n : h.failed_step - first;
+    if (h.status != LMB_OK) l->cur = cur0 ^ (int)((done + 1) & 1u);
+    if (st) {
+        st->status = h.status;
+        st->steps_done = done;
+        st->failed_step = h.status == LMB_OK ? 0 : h.failed_step;
+        st->unresolved = h.mode == LMB_OVERFLOW_RELAXED ? h.ovf_count : 0;
+        st->overflows = h.overflows;
+        st->reactions = h.reactions;
+    }
+    return h.status;
+}
+
+extern "C" int lmb_run(lmb_lattice *l, const lmb_model *m, uint32_t seed, uint32_t first, uint32_t n, int mode,
+                       lmb_run_stats *st)
+{
+    int rc = lmb_run_async(l, m, seed, first, n, mode);
+    if (rc != LMB_OK) return rc;
+    return lmb_run_wait(l, st);
+}

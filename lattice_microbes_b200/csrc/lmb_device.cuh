@@ -1,0 +1,131 @@
+// lmb_device.cuh -- device building blocks of the MPD-RDME timestep.
+//
+// Arithmetic that decides a particle's fate is written so that the compiler
+// cannot fuse a multiply into a following add (__fmul_rn / __fsub_rn): every
+// product and sum is rounded on its own, as the restatement of the
+// reference's rules requires.
+#pragma once
+
+#include <stdint.h>
+
+#include "lmb_internal.h"
+
+namespace lmb {
+
+// Counter hash of (key ^ timestep hash), upper 32 bits
+// (rdme/dev/xor_random_dev.cu:46-53).
+__device__ __forceinline__ uint32_t mix_hash(unsigned long long v, unsigned long long th)
+{
+    v ^= th;
+    v = v * 3935559000370003845ULL + 2691343689449507681ULL;
+    v ^= v >> 21;
+    v ^= v << 37;
+    v ^= v >> 4;
+    v *= 2685821657736338717ULL;
+    return (uint32_t)(v >> 32);
+}
+
+// [0,1) float: (float)r rounded to nearest, times 2^-32 (xor_random_dev.cu:44,66-70).
+__device__ __forceinline__ float hash_float(unsigned long long key, unsigned long long th)
+{
+    return __fmul_rn(__uint2float_rn(mix_hash(key, th)), 2.32830643654e-10f);
+}
+
+// Per-launch seed mixing (MpdRdmeSolver.cu:987-994), evaluated on the device
+// from the run state so that captured launches replay with the right step.
+__host__ __device__ __forceinline__ unsigned long long timestep_hash(uint32_t seed, uint32_t step,
+                                                                     uint32_t substep)
+{
+    unsigned long long h = ((((unsigned long long)seed << 30) + step) << 2) + substep;
+    h = h * 3202034522624059733ULL + 4354685564936845319ULL;
+    h ^= h >> 20;
+    h ^= h << 41;
+    h ^= h >> 5;
+    h *= 7664345821815920749ULL;
+    return h;
+}
+
+// Hash-key slot bits (byte_diffusion_1d_dev.cu:51-60).
+template <int S>
+struct CountBits {
+    static constexpr int value = S <= 4 ? 2 : (S <= 8 ? 3 : 4);
+};
+
+// A site's S slots held in W registers (4 uint8 slots per word for byte
+// lattices, one uint32 slot per word for int lattices).
+template <int BPS, int S>
+struct SiteWords {
+    static constexpr int W = (BPS == 1) ? S / 4 : S;
+    uint32_t w[W];
+
+    __device__ __forceinline__ void load(const uint32_t *__restrict__ lat, uint32_t N, uint32_t i)
+    {
+#pragma unroll
+        for (int k = 0; k < W; k++) w[k] = __ldg(lat + (size_t)k * N + i);
+    }
+    __device__ __forceinline__ void load_plain(const uint32_t *lat, uint32_t N, uint32_t i)
+    {
+#pragma unroll
+        for (int k = 0; k < W; k++) w[k] = lat[(size_t)k * N + i];
+    }
+    __device__ __forceinline__ void store(uint32_t *lat, uint32_t N, uint32_t i) const
+    {
+#pragma unroll
+        for (int k = 0; k < W; k++) lat[(size_t)k * N + i] = w[k];
+    }
+    __device__ __forceinline__ uint32_t slot(int k) const
+    {
+        if (BPS == 1) return (w[k >> 2] >> (8 * (k & 3))) & 0xFFu;
+        return w[k];
+    }
+    __device__ __forceinline__ bool empty() const
+    {
+        uint32_t o = 0;
+#pragma unroll
+        for (int k = 0; k < W; k++) o |= w[k];
+        return o == 0;
+    }
+    __device__ __forceinline__ void clear()
+    {
+#pragma unroll
+        for (int k = 0; k < W; k++) w[k] = 0;
+    }
+    // Writes slot n (n < S) without dynamic register indexing.
+    __device__ __forceinline__ void put(int n, uint32_t p)
+    {
+        if (BPS == 1) {
+#pragma unroll
+            for (int k = 0; k < W; k++)
+                if ((n >> 2) == k) w[k] |= (p & 0xFFu) << (8 * (n & 3));
+        } else {
+#pragma unroll
+            for (int k = 0; k < W; k++)
+                if (n == k) w[k] = p;
+        }
+    }
+};
+
+// T[src][dst][species], 0 for out-of-range ids (byte_diffusion_1d_dev.cu:70-78).
+__device__ __forceinline__ float lookup_T(const DevTables &m, uint32_t p, uint32_t src, uint32_t dst)
+{
+    if ((uint32_t)(p - 1u) >= m.ns || dst >= m.nst || src >= m.nst) return 0.0f;
+    return __ldg(m.T + ((size_t)src * m.nst + dst) * m.ns + (p - 1u));
+}
+
+// Queues one overflowed particle; the list index comes from an atomic, the
+// sort key restores a deterministic order later.
+__device__ __forceinline__ void push_overflow(RunState *rs, OverflowEntry *list, uint32_t cap,
+                                              uint32_t phase, uint32_t site, uint32_t seq, uint32_t particle)
+{
+    uint32_t idx = atomicAdd(&rs->ovf_count, 1u);
+    if (idx < cap) {
+        OverflowEntry e;
+        e.key = ((unsigned long long)phase << KEY_PHASE_SHIFT) |
+                ((unsigned long long)site << KEY_SITE_SHIFT) | (unsigned long long)seq;
+        e.site = site;
+        e.particle = particle;
+        list[idx] = e;
+    }
+}
+
+}  // namespace lmb

@@ -1,0 +1,85 @@
+// lmb_internal.h -- structures shared by the C ABI and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lmb {
+
+// Lattice geometry; site i = x + y*X + z*X*Y.
+struct Geometry {
+    uint32_t X, Y, Z;
+    uint32_t XY;
+    uint32_t N;
+};
+
+// Device-resident model tables (FP32 per-timestep values).  The sparse
+// stoichiometry (stoich_*) lists each reaction's nonzero S entries in
+// ascending species order; it replaces the dense column the reference copies
+// per reaction event (byte_reaction_dev.cu:182-199).
+struct DevTables {
+    uint32_t ns, nst, nr;
+    const float *T;
+    const float *qp0, *qp1, *qp2;
+    const uint32_t *order, *D1, *D2;
+    const float *rate;
+    const uint8_t *RL;
+    const uint32_t *stoich_off;  // [nr+1]
+    const uint32_t *stoich_sp;   // 0-based species
+    const int32_t *stoich_d;     // stoichiometric change
+};
+
+// One queued overflow: the sort key orders entries by (phase, site, seq);
+// phase 0 marks entries carried over by the relaxed handler.
+struct OverflowEntry {
+    unsigned long long key;
+    uint32_t site;
+    uint32_t particle;
+};
+
+constexpr int KEY_PHASE_SHIFT = 60;
+constexpr int KEY_SITE_SHIFT = 20;
+
+// Per-lattice run state in device memory, read by every kernel.
+struct RunState {
+    uint32_t seed;
+    uint32_t step;        // timestep index the next kernels work on
+    uint32_t end_step;    // exclusive end of the current run
+    int32_t status;       // LMB_OK or the error that stopped the run
+    uint32_t failed_step;
+    uint32_t ovf_count;   // entries in the list, carried ones first
+    uint32_t carried;     // relaxed handler: entries kept from earlier steps
+    uint32_t mode;        // LMB_OVERFLOW_*
+    unsigned long long overflows;
+    unsigned long long reactions;
+    uint32_t max_species; // validation scratch
+    uint32_t max_site_type;
+};
+
+// Kernel launchers (lmb_kernels.cu).  Each returns a cudaError_t.
+cudaError_t launch_sweep(int bytes_per_slot, int slots, int dim, const uint32_t *src, uint32_t *dst,
+                         const uint8_t *sites, const Geometry &g, const DevTables &m, RunState *rs,
+                         OverflowEntry *list, uint32_t cap, cudaStream_t stream);
+cudaError_t launch_reaction(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
+                            const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list,
+                            uint32_t cap, cudaStream_t stream);
+cudaError_t launch_resolve(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
+                           const Geometry &g, RunState *rs, OverflowEntry *list, uint32_t cap,
+                           cudaStream_t stream);
+cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
+                             cudaStream_t stream);
+cudaError_t launch_counts(int bytes_per_slot, int slots, const uint32_t *lat, const Geometry &g,
+                          uint32_t ns, unsigned long long *counts, cudaStream_t stream);
+cudaError_t launch_validate(int bytes_per_slot, int slots, const uint32_t *lat, const uint8_t *sites,
+                            const Geometry &g, RunState *rs, cudaStream_t stream);
+cudaError_t launch_row_major_to_native(int bytes_per_slot, int slots, const void *rm_particles,
+                                       const uint8_t *rm_sites, uint32_t *native, uint8_t *sites,
+                                       const Geometry &g, RunState *rs, cudaStream_t stream);
+cudaError_t launch_native_to_row_major(int bytes_per_slot, int slots, const uint32_t *native,
+                                       const uint8_t *sites, void *rm_particles, uint8_t *rm_sites,
+                                       const Geometry &g, cudaStream_t stream);
+
+bool slots_supported(int bytes_per_slot, int slots);
+void count_launch(uint64_t n = 1);
+
+}  // namespace lmb

@@ -1,0 +1,238 @@
+"""Python face of the C ABI: contexts, models, lattices and timestep runs.
+
+This mirrors the pieces of the reference's ``lm`` module the MPD-RDME path
+uses (a solver's model upload, its CUDA lattice and ``runTimestep`` loop); the
+work happens in liblmb200.so.
+"""
+import ctypes as C
+
+import numpy as np
+
+from lattice_microbes_b200 import _lib as L
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+class Context:
+    """One device and one CUDA stream (lmb_ctx)."""
+
+    def __init__(self, device=0, stream=None):
+        h = L.vp()
+        if stream is None:
+            L.check(L.lib().lmb_ctx_create(device, C.byref(h)), "lmb_ctx_create")
+        else:
+            L.check(L.lib().lmb_ctx_create_on_stream(device, C.c_void_p(stream), C.byref(h)),
+                    "lmb_ctx_create_on_stream")
+        self.handle = h
+        self.device = device
+
+    @property
+    def stream(self):
+        return L.lib().lmb_ctx_stream(self.handle)
+
+    def synchronize(self):
+        L.check(L.lib().lmb_ctx_synchronize(self.handle))
+
+    def close(self):
+        if self.handle:
+            L.lib().lmb_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Model:
+    """Device model tables (lmb_model)."""
+
+    def __init__(self, ctx, handle, ns, nst, nr):
+        self.ctx, self.handle = ctx, handle
+        self.ns, self.nst, self.nr = ns, nst, nr
+
+    @classmethod
+    def from_spec(cls, ctx, spec):
+        """Builds from reference-style inputs (a configs.ModelSpec or any
+        object with the same fields)."""
+        ns, nst, nr = spec.ns, spec.nst, spec.nr
+        keep = dict(
+            rtype=np.ascontiguousarray(spec.rtype, dtype=np.uint32) if nr else np.zeros(1, np.uint32),
+            K=np.ascontiguousarray(spec.K, dtype=np.float64) if nr else np.zeros(1),
+            S=np.ascontiguousarray(spec.S, dtype=np.int32).reshape(-1) if nr else np.zeros(1, np.int32),
+            D=np.ascontiguousarray(spec.D, dtype=np.uint32).reshape(-1) if nr else np.zeros(1, np.uint32),
+            DF=np.ascontiguousarray(spec.DF, dtype=np.float64).reshape(-1),
+            RL=np.ascontiguousarray(spec.RL, dtype=np.uint32).reshape(-1) if nr else np.zeros(1, np.uint32),
+        )
+        d = L.ModelDesc()
+        d.number_species, d.number_reactions, d.number_site_types = ns, nr, nst
+        d.reaction_types = _p(keep["rtype"], L.u32p)
+        d.K = _p(keep["K"], L.f64p)
+        d.k_cols = 1
+        d.S = _p(keep["S"], L.i32p)
+        d.D = _p(keep["D"], L.u32p)
+        d.DF = _p(keep["DF"], L.f64p)
+        d.RL = _p(keep["RL"], L.u32p)
+        d.timestep = spec.tau
+        d.lattice_spacing = spec.spacing
+        h = L.vp()
+        L.check(L.lib().lmb_model_create(ctx.handle, C.byref(d), spec.X, spec.Y, spec.Z, C.byref(h)),
+                "lmb_model_create")
+        return cls(ctx, h, ns, nst, nr)
+
+    @classmethod
+    def from_tables(cls, ctx, t):
+        """From ready FP32 tables (an object with T, qp0.. RL arrays)."""
+        arrs = dict(T=np.ascontiguousarray(t.T, np.float32), qp0=np.ascontiguousarray(t.qp0, np.float32),
+                    qp1=np.ascontiguousarray(t.qp1, np.float32), qp2=np.ascontiguousarray(t.qp2, np.float32),
+                    order=np.ascontiguousarray(t.order, np.uint32), D1=np.ascontiguousarray(t.D1, np.uint32),
+                    D2=np.ascontiguousarray(t.D2, np.uint32), rate=np.ascontiguousarray(t.rate, np.float32),
+                    S=np.ascontiguousarray(t.S, np.int8), RL=np.ascontiguousarray(t.RL, np.uint8))
+        tb = L.Tables()
+        tb.number_species, tb.number_reactions, tb.number_site_types = t.ns, t.nr, t.nst
+        tb.T, tb.qp0, tb.qp1, tb.qp2 = (_p(arrs["T"], L.f32p), _p(arrs["qp0"], L.f32p),
+                                        _p(arrs["qp1"], L.f32p), _p(arrs["qp2"], L.f32p))
+        tb.order, tb.D1, tb.D2 = _p(arrs["order"], L.u32p), _p(arrs["D1"], L.u32p), _p(arrs["D2"], L.u32p)
+        tb.rate, tb.S, tb.RL = _p(arrs["rate"], L.f32p), _p(arrs["S"], L.i8p), _p(arrs["RL"], L.u8p)
+        h = L.vp()
+        L.check(L.lib().lmb_model_create_from_tables(ctx.handle, C.byref(tb), C.byref(h)),
+                "lmb_model_create_from_tables")
+        return cls(ctx, h, t.ns, t.nst, t.nr)
+
+    def tables(self):
+        ns, nst, nr = self.ns, self.nst, self.nr
+        out = dict(T=np.zeros(nst * nst * ns, np.float32), qp0=np.zeros(nst, np.float32),
+                   qp1=np.zeros(nst * ns, np.float32), qp2=np.zeros(nst * ns * ns, np.float32),
+                   order=np.zeros(max(nr, 1), np.uint32), D1=np.zeros(max(nr, 1), np.uint32),
+                   D2=np.zeros(max(nr, 1), np.uint32), rate=np.zeros(max(nr, 1), np.float32),
+                   S=np.zeros(max(nr * ns, 1), np.int8), RL=np.zeros(max(nr * nst, 1), np.uint8))
+        L.check(L.lib().lmb_model_get_tables(
+            self.handle, _p(out["T"], L.f32p), _p(out["qp0"], L.f32p), _p(out["qp1"], L.f32p),
+            _p(out["qp2"], L.f32p), _p(out["order"], L.u32p), _p(out["D1"], L.u32p), _p(out["D2"], L.u32p),
+            _p(out["rate"], L.f32p), _p(out["S"], L.i8p), _p(out["RL"], L.u8p)))
+        for k in ("order", "D1", "D2", "rate"):
+            out[k] = out[k][:nr]
+        out["S"] = out["S"][: nr * ns]
+        out["RL"] = out["RL"][: nr * nst]
+        return out
+
+    def set_reaction_rate(self, reaction, rate):
+        L.check(L.lib().lmb_model_set_reaction_rate(self.handle, reaction, rate))
+
+    def close(self):
+        if self.handle:
+            L.lib().lmb_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """Device lattice (lmb_lattice): two particle buffers + site types."""
+
+    def __init__(self, ctx, X, Y, Z, slots, bytes_per_slot):
+        h = L.vp()
+        L.check(L.lib().lmb_lattice_create(ctx.handle, X, Y, Z, slots, bytes_per_slot, C.byref(h)),
+                "lmb_lattice_create")
+        self.ctx, self.handle = ctx, h
+        self.X, self.Y, self.Z = X, Y, Z
+        self.slots, self.bytes_per_slot = slots, bytes_per_slot
+        self.words = slots // 4 if bytes_per_slot == 1 else slots
+
+    @property
+    def nsites(self):
+        return self.X * self.Y * self.Z
+
+    def set_native(self, particles=None, sites=None):
+        p = None if particles is None else np.ascontiguousarray(particles, dtype=np.uint32)
+        s = None if sites is None else np.ascontiguousarray(sites, dtype=np.uint8)
+        if p is not None and p.size != self.words * self.nsites:
+            raise ValueError("particle array size")
+        if s is not None and s.size != self.nsites:
+            raise ValueError("site array size")
+        L.check(L.lib().lmb_lattice_set_native(self.handle, None if p is None else _p(p, L.u32p),
+                                               None if s is None else _p(s, L.u8p)))
+
+    def get_native(self):
+        p = np.zeros(self.words * self.nsites, dtype=np.uint32)
+        s = np.zeros(self.nsites, dtype=np.uint8)
+        L.check(L.lib().lmb_lattice_get_native(self.handle, _p(p, L.u32p), _p(s, L.u8p)))
+        return p, s
+
+    def set_row_major(self, particles, sites, number_species, number_site_types):
+        dt = np.uint8 if self.bytes_per_slot == 1 else np.uint32
+        p = np.ascontiguousarray(particles, dtype=dt)
+        s = np.ascontiguousarray(sites, dtype=np.uint8)
+        L.check(L.lib().lmb_lattice_set_row_major(self.handle, p.ctypes.data_as(C.c_void_p), _p(s, L.u8p),
+                                                  number_species, number_site_types))
+
+    def get_row_major(self):
+        dt = np.uint8 if self.bytes_per_slot == 1 else np.uint32
+        p = np.zeros((self.X, self.Y, self.Z, self.slots), dtype=dt)
+        s = np.zeros((self.X, self.Y, self.Z), dtype=np.uint8)
+        L.check(L.lib().lmb_lattice_get_row_major(self.handle, p.ctypes.data_as(C.c_void_p), _p(s, L.u8p)))
+        return p, s
+
+    def device_buffers(self):
+        a, b = L.vp(), L.vp()
+        L.check(L.lib().lmb_lattice_device_buffers(self.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def species_counts(self, ns):
+        c = np.zeros(ns + 1, dtype=np.uint64)
+        L.check(L.lib().lmb_lattice_species_counts(self.handle, ns, _p(c, L.u64p)))
+        return c
+
+    def run(self, model, seed, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC, check=True):
+        st = L.RunStats()
+        rc = L.lib().lmb_run(self.handle, model.handle, seed, first_timestep, timesteps, overflow_mode,
+                             C.byref(st))
+        if check:
+            L.check(rc, "lmb_run")
+        return rc, st
+
+    def run_profiled(self, model, seed, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
+        """Runs with CUDA events around every kernel; returns (stats, phase
+        milliseconds [x, y, z, reaction, overflow], launches per phase)."""
+        st = L.RunStats()
+        ms = np.zeros(5, dtype=np.float32)
+        n = np.zeros(5, dtype=np.uint32)
+        L.check(L.lib().lmb_run_profiled(self.handle, model.handle, seed, first_timestep, timesteps, overflow_mode,
+                                         _p(ms, L.f32p), _p(n, L.u32p), C.byref(st)), "lmb_run_profiled")
+        return st, ms, n
+
+    def run_async(self, model, seed, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
+        L.check(L.lib().lmb_run_async(self.handle, model.handle, seed, first_timestep, timesteps, overflow_mode))
+
+    def wait(self, check=True):
+        st = L.RunStats()
+        rc = L.lib().lmb_run_wait(self.handle, C.byref(st))
+        if check:
+            L.check(rc, "lmb_run_wait")
+        return rc, st
+
+    def close(self):
+        if self.handle:
+            L.lib().lmb_lattice_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def compose_seed(seed_top, replicate):
+    return L.lib().lmb_compose_seed(seed_top, replicate)
+
+
+def kernel_launches():
+    return L.lib().lmb_kernel_launches()

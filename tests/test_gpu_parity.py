@@ -1,0 +1,211 @@
+"""CUDA path (through the C ABI) against the oracle and the golden fixtures.
+
+Integer lattice state must match bit for bit.  The classic overflow handler
+is compared for the canonical reinsertion order (sorted by sweep, site,
+slot); the oracle uses the same order and is itself pinned to the
+reference's device functions.
+"""
+import numpy as np
+import pytest
+
+from lattice_microbes_b200 import configs
+from tests.cases import oracle_tables
+from tests.golden_lib import case_names, load_case
+from tests.oracle_lib import oracle_counts, oracle_run
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(gpu):
+    from lattice_microbes_b200.solver import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def _gpu_run(ctx, tables_or_spec, lattice, sites, seed, step0, nsteps, mode=0, from_spec=False, chunks=None):
+    from lattice_microbes_b200.solver import Lattice, Model
+    t = tables_or_spec
+    model = Model.from_spec(ctx, t) if from_spec else Model.from_tables(ctx, t)
+    lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
+    lat.set_native(lattice, sites)
+    if chunks is None:
+        chunks = [nsteps]
+    step, stats, rc = step0, [], 0
+    for n in chunks:
+        rc, st = lat.run(model, seed, step, n, mode, check=False)
+        stats.append(st)
+        step += n
+        if rc:
+            break
+    out, _ = lat.get_native()
+    lat.close()
+    model.close()
+    return out, rc, stats
+
+
+@pytest.mark.parametrize("name", case_names())
+def test_golden_fixture(ctx, name):
+    t, g = load_case(name)
+    out, rc, st = _gpu_run(ctx, t, g["lattice_in"], g["sites"], int(g["seed"]), int(g["step0"]), int(g["nsteps"]))
+    assert rc == 0
+    assert st[0].overflows == int(g["overflows"])
+    assert st[0].reactions == int(g["reactions"])
+    assert np.array_equal(out, g["lattice_out"])
+
+
+VARIANTS = [(4, 1), (8, 1), (16, 1), (32, 1), (4, 4), (8, 4), (16, 4)]
+
+
+@pytest.mark.parametrize("slots,bps", VARIANTS)
+@pytest.mark.parametrize("seed", [0, 1])
+def test_random_problem_vs_oracle(ctx, seed, slots, bps):
+    dens = {4: 0.3, 8: 0.5, 16: 1.2, 32: 2.0}[slots]
+    spec = configs.random_problem(seed, X=32, Y=16, Z=16, slots=slots, bytes_per_slot=bps, density=dens)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 4321 + seed, 11, 12)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 4321 + seed, 11, 12)
+    assert rc == rc_ref == 0
+    assert (st[0].overflows, st[0].reactions) == (st_ref.overflows, st_ref.reactions)
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("shape", [(16, 24, 8), (24, 16, 40), (7, 5, 3), (48, 8, 16), (1, 8, 8)])
+def test_odd_shapes_vs_oracle(ctx, shape):
+    X, Y, Z = shape
+    spec = configs.random_problem(5, X=X, Y=Y, Z=Z, density=0.6)
+    t = oracle_tables(spec)
+    ref, rc_ref, _ = oracle_run(t, spec.lattice, spec.sites, 99, 0, 10)
+    out, rc, _ = _gpu_run(ctx, t, spec.lattice, spec.sites, 99, 0, 10)
+    assert rc == rc_ref
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("slots,bps,dens", [(8, 1, 5.0), (16, 4, 12.0), (8, 4, 6.0)])
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_overflow_storm_vs_oracle(ctx, seed, slots, bps, dens):
+    """Heavy overflow traffic; seeds 1-3 end in the reference's two errors
+    (list exhausted / no free site), which must stop at the same step with
+    the same partial lattice."""
+    spec = configs.random_problem(seed, X=32, Y=8, Z=8, slots=slots, bytes_per_slot=bps, density=dens, nst=2)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 99 + seed, 5, 8)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 99 + seed, 5, 8)
+    assert rc == rc_ref
+    if rc == 0:
+        assert st[0].overflows == st_ref.overflows
+    assert np.array_equal(out, ref)
+
+
+def test_relaxed_handler_vs_oracle(ctx):
+    spec = configs.random_problem(2, X=32, Y=8, Z=8, slots=8, bytes_per_slot=1, density=3.0, nst=2)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 7, 0, 6, mode=1)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 7, 0, 6, mode=1)
+    assert rc == rc_ref
+    assert st[-1].unresolved == st_ref.unresolved
+    assert np.array_equal(out, ref)
+
+
+def test_chunked_run_equals_single_run(ctx):
+    spec = configs.random_problem(8, X=32, Y=16, Z=8, density=0.7)
+    t = oracle_tables(spec)
+    a, rc1, _ = _gpu_run(ctx, t, spec.lattice, spec.sites, 3, 0, 20)
+    b, rc2, _ = _gpu_run(ctx, t, spec.lattice, spec.sites, 3, 0, 20, chunks=[1, 7, 5, 7])
+    assert rc1 == rc2 == 0
+    assert np.array_equal(a, b)
+
+
+def test_model_from_spec_equals_oracle(ctx):
+    spec = configs.config0(seed=4)
+    t = oracle_tables(spec)
+    ref, _, _ = oracle_run(t, spec.lattice, spec.sites, 55, 0, 100)
+    out, rc, _ = _gpu_run(ctx, spec, spec.lattice, spec.sites, 55, 0, 100, from_spec=True)
+    assert rc == 0
+    assert np.array_equal(out, ref)
+
+
+def test_config1_short_vs_oracle(ctx):
+    spec = configs.config1(seed=2)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 31, 0, 6)
+    out, rc, st = _gpu_run(ctx, spec, spec.lattice, spec.sites, 31, 0, 6, from_spec=True)
+    assert rc == rc_ref == 0
+    assert np.array_equal(out, ref)
+
+
+def test_set_reaction_rate(ctx):
+    from lattice_microbes_b200.solver import Model
+    spec = configs.config0(seed=5)
+    m = Model.from_spec(ctx, spec)
+    spec.K = spec.K.copy()
+    spec.K[1] *= 50.0
+    m.set_reaction_rate(1, float(spec.K[1]))
+    ref = oracle_tables(spec)
+    got = m.tables()
+    assert np.array_equal(got["rate"], ref.rate)
+    assert np.array_equal(got["qp1"], ref.qp1)
+    m.close()
+
+
+def test_species_counts_and_layouts(ctx):
+    from lattice_microbes_b200.solver import Lattice
+    spec = configs.random_problem(6, X=24, Y=16, Z=8, slots=16, bytes_per_slot=4, density=2.0, ns=9)
+    t = oracle_tables(spec)
+    lat = Lattice(ctx, spec.X, spec.Y, spec.Z, 16, 4)
+    lat.set_native(spec.lattice, spec.sites)
+    counts = lat.species_counts(spec.ns)
+    assert np.array_equal(counts, oracle_counts(t, spec.lattice))
+    rm, rs = lat.get_row_major()
+    slots = configs.native_to_slots(spec.lattice, spec.X, spec.Y, spec.Z, 16, 4)
+    expect = slots.reshape(spec.Z, spec.Y, spec.X, 16).transpose(2, 1, 0, 3)
+    assert np.array_equal(rm, expect)
+    assert np.array_equal(rs, spec.sites.reshape(spec.Z, spec.Y, spec.X).transpose(2, 1, 0))
+    # Row-major with holes packs each site (RDMESolver.cpp:144-167).
+    holes = rm.copy()
+    holes[..., 0] = 0
+    lat.set_row_major(holes, rs, spec.ns, spec.nst)
+    back, _ = lat.get_row_major()
+    for site in [(0, 0, 0), (5, 3, 2), (23, 15, 7)]:
+        v = holes[site]
+        nz = v[v != 0]
+        assert np.array_equal(back[site][: len(nz)], nz)
+        assert not back[site][len(nz):].any()
+    lat.close()
+
+
+def test_pure_diffusion_conserves_counts_large(ctx):
+    """Size-independent property at a larger lattice: no reactions, counts
+    are conserved exactly over many steps."""
+    from lattice_microbes_b200.solver import Lattice, Model
+    spec = configs.config1(seed=3, X=64, Y=64, Z=128)
+    spec.rtype = spec.rtype[:0]
+    spec.K = spec.K[:0]
+    spec.S = spec.S[:, :0]
+    spec.D = spec.D[:, :0]
+    spec.RL = spec.RL[:0]
+    m = Model.from_spec(ctx, spec)
+    lat = Lattice(ctx, spec.X, spec.Y, spec.Z, 8, 1)
+    lat.set_native(spec.lattice, spec.sites)
+    before = lat.species_counts(spec.ns)
+    rc, st = lat.run(m, 9, 0, 300)
+    assert rc == 0
+    assert np.array_equal(before, lat.species_counts(spec.ns))
+    lat.close()
+    m.close()
+
+
+def test_invalid_species_rejected(ctx):
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import Lattice, Model
+    spec = configs.config0(seed=1, edge=16)
+    m = Model.from_spec(ctx, spec)
+    lat = Lattice(ctx, 16, 16, 16, 8, 1)
+    bad = spec.lattice.copy()
+    bad[0] = 9  # species 9 > 3
+    lat.set_native(bad, spec.sites)
+    rc, _ = lat.run(m, 1, 0, 1, check=False)
+    assert rc == L.LMB_E_ARG
+    lat.close()
+    m.close()
