@@ -39,6 +39,14 @@ extern "C" {
 #define LMB_OVERFLOW_CLASSIC 0
 #define LMB_OVERFLOW_RELAXED 1
 
+/* Timestep schedules.  FUSED runs the x, y, z sweeps and the reaction of a
+ * tile of Ty x Tz full x-rows in shared memory, one launch per timestep;
+ * PHASES launches one kernel per sweep, the reaction and the overflow pass
+ * (the reference's schedule, MpdRdmeSolver.cu:1011-1090).  Both give the
+ * same lattice bit for bit. */
+#define LMB_SCHEDULE_FUSED 0
+#define LMB_SCHEDULE_PHASES 1
+
 /* Reaction types (CMESolver.h:79-112). */
 #define LMB_REACTION_ZEROTH 0
 #define LMB_REACTION_FIRST 1
@@ -160,6 +168,16 @@ int lmb_lattice_get_native(lmb_lattice *lattice, uint32_t *particles, uint8_t *s
 int lmb_lattice_set_row_major(lmb_lattice *lattice, const void *particles, const uint8_t *sites,
                               uint32_t number_species, uint32_t number_site_types);
 int lmb_lattice_get_row_major(lmb_lattice *lattice, void *particles, uint8_t *sites);
+/* Timestep schedule of this lattice: LMB_SCHEDULE_FUSED with tile Ty x Tz
+ * (0, 0 = default plan) or LMB_SCHEDULE_PHASES.  The reference has fixed
+ * block sizes instead (options.cmake:89-95). */
+int lmb_lattice_set_schedule(lmb_lattice *lattice, int schedule, uint32_t Ty, uint32_t Tz);
+int lmb_lattice_get_schedule(lmb_lattice *lattice, int *schedule, uint32_t *Ty, uint32_t *Tz);
+/* Autotuner: times every schedule and tile shape that fits for `timesteps`
+ * on a saved copy of the lattice state, restores the state and keeps the
+ * fastest. */
+int lmb_lattice_autotune(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
+                         uint32_t timesteps, int *schedule, uint32_t *Ty, uint32_t *Tz, float *best_ms);
 /* Device pointers of the current particle buffer and of the site types. */
 int lmb_lattice_device_buffers(lmb_lattice *lattice, void **particles, void **sites);
 /* ByteLattice::getParticleCounts (ByteLattice.cpp:495-520), computed on the
@@ -180,8 +198,9 @@ int lmb_run_async(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, u
 int lmb_run_wait(lmb_lattice *lattice, lmb_run_stats *stats);
 
 /* lmb_run with a CUDA event pair around every kernel on the lattice's
- * stream; phase_ms[5] / phase_launches[5] receive the summed device time and
- * launch count of the x, y, z sweeps, the reaction and the overflow kernel. */
+ * stream; phase_ms[6] / phase_launches[6] receive the summed device time and
+ * launch count of the x, y, z sweeps, the reaction, the overflow kernel and
+ * the fused timestep kernel. */
 int lmb_run_profiled(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
                      uint32_t number_timesteps, int overflow_mode, float *phase_ms, uint32_t *phase_launches,
                      lmb_run_stats *stats);

@@ -23,6 +23,9 @@ LMB_E_UNSUPPORTED = -9
 LMB_OVERFLOW_CLASSIC = 0
 LMB_OVERFLOW_RELAXED = 1
 
+LMB_SCHEDULE_FUSED = 0
+LMB_SCHEDULE_PHASES = 1
+
 u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
 f32p = C.POINTER(C.c_float)
@@ -84,6 +87,10 @@ PROTOTYPES = {
     "lmb_lattice_get_native": (C.c_int, [vp, u32p, u8p]),
     "lmb_lattice_set_row_major": (C.c_int, [vp, vp, u8p, C.c_uint32, C.c_uint32]),
     "lmb_lattice_get_row_major": (C.c_int, [vp, vp, u8p]),
+    "lmb_lattice_set_schedule": (C.c_int, [vp, C.c_int, C.c_uint32, C.c_uint32]),
+    "lmb_lattice_get_schedule": (C.c_int, [vp, C.POINTER(C.c_int), u32p, u32p]),
+    "lmb_lattice_autotune": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(C.c_int), u32p, u32p,
+                                       f32p]),
     "lmb_lattice_device_buffers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
     "lmb_lattice_species_counts": (C.c_int, [vp, C.c_uint32, u64p]),
     "lmb_run": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(RunStats)]),

@@ -16,6 +16,7 @@
 
 #include "lmb.h"
 #include "lmb_device.cuh"
+#include "lmb_fused.h"
 #include "lmb_internal.h"
 
 using namespace lmb;
@@ -70,6 +71,9 @@ struct lmb_lattice {
     uint32_t counts_len;
     bool validated;
     uint32_t max_species, max_site_type;
+    // Schedule: fused tile kernel (one launch per timestep) or per-phase kernels.
+    int schedule;
+    TileShape tile;
     // Pending async run.
     bool pending;
     int pending_cur0;
@@ -539,7 +543,34 @@ extern "C" int lmb_lattice_create(lmb_ctx *c, uint32_t X, uint32_t Y, uint32_t Z
         return cuda_status(e);
     }
     l->validated = false;
+    l->schedule = fused_default_shape(l->g, (int)bps, (int)slots, l->tile) ? LMB_SCHEDULE_FUSED : LMB_SCHEDULE_PHASES;
     *out = l;
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_set_schedule(lmb_lattice *l, int schedule, uint32_t Ty, uint32_t Tz)
+{
+    if (!l) return LMB_E_ARG;
+    if (schedule == LMB_SCHEDULE_PHASES) {
+        l->schedule = schedule;
+        return LMB_OK;
+    }
+    if (schedule != LMB_SCHEDULE_FUSED) return LMB_E_ARG;
+    TileShape t;
+    bool ok = (Ty == 0 && Tz == 0) ? fused_default_shape(l->g, (int)l->bps, (int)l->slots, t)
+                                   : fused_make_shape(l->g, (int)l->bps, (int)l->slots, Ty, Tz, t);
+    if (!ok) return LMB_E_UNSUPPORTED;
+    l->tile = t;
+    l->schedule = schedule;
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_get_schedule(lmb_lattice *l, int *schedule, uint32_t *Ty, uint32_t *Tz)
+{
+    if (!l) return LMB_E_ARG;
+    if (schedule) *schedule = l->schedule;
+    if (Ty) *Ty = l->schedule == LMB_SCHEDULE_FUSED ? l->tile.Ty : 0;
+    if (Tz) *Tz = l->schedule == LMB_SCHEDULE_FUSED ? l->tile.Tz : 0;
     return LMB_OK;
 }
 
@@ -725,6 +756,12 @@ extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed,
     l->pending_cur0 = l->cur;
     for (uint32_t s = 0; s < n; s++) {
         uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
+        if (l->schedule == LMB_SCHEDULE_FUSED) {
+            CK(launch_fused(bps, S, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, l->tile, m->nr > 0,
+                            c->stream));
+            l->cur ^= 1;
+            continue;
+        }
         CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
         CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
         CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
@@ -770,7 +807,8 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
                                 int mode, float *phase_ms, uint32_t *phase_launches, lmb_run_stats *st)
 {
     // Same work as lmb_run with a CUDA event pair around every kernel, on the
-    // lattice's stream.  phase order: x, y, z sweeps, reaction, overflow.
+    // lattice's stream.  phase order: x, y, z sweeps, reaction, overflow,
+    // fused timestep.
     if (!l || !mc || !phase_ms || !phase_launches) return LMB_E_ARG;
     if (l->pending) return LMB_E_STATE;
     lmb_model *m = const_cast<lmb_model *>(mc);
@@ -783,13 +821,22 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
     int rc = validate_for_model(l, m);
     if (rc) return rc;
     CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream));
-    std::vector<cudaEvent_t> ev((size_t)n * 10);
+    std::vector<cudaEvent_t> ev((size_t)n * 12);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     const int bps = (int)l->bps, S = (int)l->slots;
     const int cur0 = l->cur;
+    const bool fused = l->schedule == LMB_SCHEDULE_FUSED;
     for (uint32_t s = 0; s < n; s++) {
         uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
-        cudaEvent_t *E = &ev[(size_t)s * 10];
+        cudaEvent_t *E = &ev[(size_t)s * 12];
+        if (fused) {
+            CK(cudaEventRecord(E[10], c->stream));
+            CK(launch_fused(bps, S, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, l->tile, m->nr > 0,
+                            c->stream));
+            CK(cudaEventRecord(E[11], c->stream));
+            l->cur ^= 1;
+            continue;
+        }
         CK(cudaEventRecord(E[0], c->stream));
         CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
         CK(cudaEventRecord(E[1], c->stream));
@@ -810,14 +857,15 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
     }
     CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    for (int p = 0; p < 5; p++) {
+    for (int p = 0; p < 6; p++) {
         phase_ms[p] = 0.0f;
         phase_launches[p] = 0;
     }
     for (uint32_t s = 0; s < n; s++)
-        for (int p = 0; p < 5; p++) {
+        for (int p = 0; p < 6; p++) {
+            if (fused != (p == 5)) continue;
             float ms = 0.0f;
-            CK(cudaEventElapsedTime(&ms, ev[(size_t)s * 10 + 2 * p], ev[(size_t)s * 10 + 2 * p + 1]));
+            CK(cudaEventElapsedTime(&ms, ev[(size_t)s * 12 + 2 * p], ev[(size_t)s * 12 + 2 * p + 1]));
             phase_ms[p] += ms;
             if (p != 3 || m->nr > 0) phase_launches[p] += 1;
         }
@@ -842,4 +890,79 @@ extern "C" int lmb_run(lmb_lattice *l, const lmb_model *m, uint32_t seed, uint32
     int rc = lmb_run_async(l, m, seed, first, n, mode);
     if (rc != LMB_OK) return rc;
     return lmb_run_wait(l, st);
+}
+
+// Times each candidate schedule for `timesteps` on a copy of the lattice
+// state (restored afterwards) and keeps the fastest.
+extern "C" int lmb_lattice_autotune(lmb_lattice *l, const lmb_model *m, uint32_t seed, uint32_t first,
+                                    uint32_t timesteps, int *schedule, uint32_t *Ty, uint32_t *Tz, float *best_ms)
+{
+    if (!l || !m || timesteps == 0) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    const size_t wbytes = (size_t)l->words * l->g.N * 4;
+    uint32_t *save = nullptr;
+    CK(cudaMalloc(&save, wbytes));
+    cudaError_t e = cudaMemcpyAsync(save, l->buf[l->cur], wbytes, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(save);
+        return cuda_status(e);
+    }
+    const int cur0 = l->cur;
+    const int sched0 = l->schedule;
+    const TileShape tile0 = l->tile;
+    struct Cand { int sched; uint32_t ty, tz; };
+    std::vector<Cand> cands = {{LMB_SCHEDULE_PHASES, 0, 0}};
+    const uint32_t dims[] = {1, 2, 4, 8, 16};
+    for (uint32_t ty : dims)
+        for (uint32_t tz : dims) {
+            TileShape t;
+            if (fused_make_shape(l->g, (int)l->bps, (int)l->slots, ty, tz, t)) cands.push_back({LMB_SCHEDULE_FUSED, ty, tz});
+        }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    Cand bestc = {sched0, tile0.Ty, tile0.Tz};
+    int rc = LMB_OK;
+    for (const Cand &cd : cands) {
+        if (lmb_lattice_set_schedule(l, cd.sched, cd.ty, cd.tz) != LMB_OK) continue;
+        // warm-up launch, then the timed one, each from the saved state
+        for (int rep = 0; rep < 2 && rc == LMB_OK; rep++) {
+            l->cur = cur0;
+            cudaMemcpyAsync(l->buf[l->cur], save, wbytes, cudaMemcpyDeviceToDevice, c->stream);
+            cudaEventRecord(e0, c->stream);
+            rc = lmb_run_async(l, m, seed, first, timesteps, LMB_OVERFLOW_CLASSIC);
+            if (rc != LMB_OK) break;
+            cudaEventRecord(e1, c->stream);
+            lmb_run_stats st;
+            rc = lmb_run_wait(l, &st);
+            if (rc != LMB_OK) break;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep == 1 && ms < best) {
+                best = ms;
+                bestc = cd;
+            }
+        }
+        if (rc != LMB_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    l->cur = cur0;
+    cudaMemcpyAsync(l->buf[l->cur], save, wbytes, cudaMemcpyDeviceToDevice, c->stream);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(save);
+    if (rc != LMB_OK) {
+        l->schedule = sched0;
+        l->tile = tile0;
+        return rc;
+    }
+    lmb_lattice_set_schedule(l, bestc.sched, bestc.ty, bestc.tz);
+    if (schedule) *schedule = bestc.sched;
+    if (Ty) *Ty = bestc.ty;
+    if (Tz) *Tz = bestc.tz;
+    if (best_ms) *best_ms = best;
+    return LMB_OK;
 }

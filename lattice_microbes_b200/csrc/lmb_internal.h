@@ -54,6 +54,8 @@ struct RunState {
     unsigned long long reactions;
     uint32_t max_species; // validation scratch
     uint32_t max_site_type;
+    uint32_t tiles_done;  // fused kernel: blocks finished in this launch
+    uint32_t pad_;
 };
 
 // Kernel launchers (lmb_kernels.cu).  Each returns a cudaError_t.

@@ -20,32 +20,14 @@
 #include "lmb.h"
 #include "lmb_device.cuh"
 #include "lmb_internal.h"
+#include "lmb_overflow.cuh"
+#include "lmb_site.cuh"
 
 namespace lmb {
 
 // ---------------------------------------------------------------------------
 // Diffusion sweep
 // ---------------------------------------------------------------------------
-
-// Appends particles to a new site in order; the (S+1)-th and later ones
-// overflow with seq = position - S (byte_diffusion_1d_dev.cu:199-269).
-template <int BPS, int S>
-struct SiteBuilder {
-    SiteWords<BPS, S> out;
-    int n;
-    __device__ __forceinline__ void init()
-    {
-        out.clear();
-        n = 0;
-    }
-    __device__ __forceinline__ void push(uint32_t p, RunState *rs, OverflowEntry *list, uint32_t cap,
-                                         uint32_t phase, uint32_t site)
-    {
-        if (n < S) out.put(n, p);
-        else push_overflow(rs, list, cap, phase, site, (uint32_t)(n - S), p);
-        n++;
-    }
-};
 
 template <int BPS, int S, int DIM>
 __global__ void __launch_bounds__(256) sweep_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
@@ -76,87 +58,21 @@ __global__ void __launch_bounds__(256) sweep_kernel(const uint32_t *__restrict__
     own.load(src, g.N, i);
     mn.load(src, g.N, im);
     pl.load(src, g.N, ip);
-    SiteBuilder<BPS, S> b;
-    b.init();
     if (own.empty() && mn.empty() && pl.empty()) {
-        b.out.store(dst, g.N, i);
+        own.store(dst, g.N, i);
         return;
     }
     const unsigned long long th = timestep_hash(rs->seed, rs->step, DIM);
     const uint32_t t = __ldg(sites + i), tm = __ldg(sites + im), tp = __ldg(sites + ip);
-    constexpr int CB = CountBits<S>::value;
-    const uint32_t phase = DIM + 1;
-    // Stayers of this site, slot order.
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const uint32_t p = own.slot(k);
-        if (p) {
-            const float r = hash_float(((unsigned long long)i << CB) | (unsigned)k, th);
-            const float qm = lookup_T(m, p, t, tm);
-            const float qp = lookup_T(m, p, t, tp);
-            const bool plus = (r >= 0.5f) && (r < __fadd_rn(qp, 0.5f));
-            if (!plus && !(r < qm)) b.push(p, rs, list, cap, phase, i);
-        }
-    }
-    // PLUS movers of the minus neighbour.
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const uint32_t p = mn.slot(k);
-        if (p) {
-            const float r = hash_float(((unsigned long long)im << CB) | (unsigned)k, th);
-            const float qp = lookup_T(m, p, tm, t);
-            if ((r >= 0.5f) && (r < __fadd_rn(qp, 0.5f))) b.push(p, rs, list, cap, phase, i);
-        }
-    }
-    // MINUS movers of the plus neighbour.
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const uint32_t p = pl.slot(k);
-        if (p) {
-            const float r = hash_float(((unsigned long long)ip << CB) | (unsigned)k, th);
-            const float qm = lookup_T(m, p, tp, t);
-            if (r < qm) b.push(p, rs, list, cap, phase, i);
-        }
-    }
-    b.out.store(dst, g.N, i);
+    const SiteWords<BPS, S> out =
+        sweep_site<BPS, S>(own, mn, pl, t, tm, tp, i, im, ip, th, m, true, DIM + 1, rs, list, cap);
+    out.store(dst, g.N, i);
 }
 
 // ---------------------------------------------------------------------------
 // Reaction
 // ---------------------------------------------------------------------------
 
-// Per-reaction propensity from FP32 counts (byte_reaction_dev.cu:62-102,
-// MPD_GLOBAL_R_MATRIX branch: the self reaction is rate*n*(n-1)).
-template <int BPS, int S>
-__device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_t t, const SiteWords<BPS, S> &s,
-                                                     uint32_t rx)
-{
-    if (!__ldg(m.RL + (size_t)rx * m.nst + t)) return 0.0f;
-    const uint32_t d1 = __ldg(m.D1 + rx), d2 = __ldg(m.D2 + rx);
-    float n1 = 0.0f, n2 = 0.0f;
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const uint32_t p = s.slot(k);
-        if (p > 0) {
-            n1 = __fadd_rn(n1, p == d1 ? 1.0f : 0.0f);
-            n2 = __fadd_rn(n2, p == d2 ? 1.0f : 0.0f);
-        }
-    }
-    const float rate = __ldg(m.rate + rx);
-    switch (__ldg(m.order + rx)) {
-    case 1: return rate;
-    case 2: return __fmul_rn(rate, n1);
-    case 3: return __fmul_rn(__fmul_rn(rate, n1), n2);
-    case 4: return __fmul_rn(__fmul_rn(rate, n1), __fsub_rn(n1, 1.0f));
-    default: return 0.0f;
-    }
-}
-
-constexpr int MAX_STOICH = 32;
-
-// precomp_reaction_kernel (MpdRdmeSolver.cu:1590-1675) with
-// byte_reaction_dev.cu:121-258: table propensity sum in slot order, double
-// precision probability, one reaction at most, in-place update.
 template <int BPS, int S>
 __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ lat, const uint8_t *__restrict__ sites,
                                                        Geometry g, DevTables m, RunState *__restrict__ rs,
@@ -168,145 +84,16 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
     const uint32_t t = __ldg(sites + i);
     SiteWords<BPS, S> s;
     s.load_plain(lat, g.N, i);
-    float a = __ldg(m.qp0 + t);
-    if (s.empty() && a == 0.0f) return;
-    const size_t o1 = (size_t)t * m.ns, o2 = (size_t)t * m.ns * m.ns;
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const uint32_t p1 = s.slot(k);
-        if (p1 > 0) {
-            a = __fadd_rn(a, __ldg(m.qp1 + o1 + (p1 - 1)));
-#pragma unroll
-            for (int j = k + 1; j < S; j++) {
-                const uint32_t p2 = s.slot(j);
-                if (p2 > 0) a = __fadd_rn(a, __ldg(m.qp2 + o2 + (size_t)(p1 - 1) * m.ns + (p2 - 1)));
-            }
-        }
-    }
-    if (a == 0.0f) return;
-    const float prob = (float)(1.0 - exp(-(double)a));
     const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
-    const float r0 = hash_float(((unsigned long long)i << 1) | 0ull, th);
-    if (!(prob > 0.0f && r0 <= prob)) return;
-
-    float rp = __fmul_rn(hash_float(((unsigned long long)i << 1) | 1ull, th), a);
-    uint32_t idx = 0;
-    for (uint32_t rx = 0; rx < m.nr; rx++) {
-        const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
-        if (prop > 0.0f) {
-            if (rp > 0.0f) idx = rx;
-            rp = __fsub_rn(rp, prop);
-        }
-    }
-    atomicAdd(&rs->reactions, 1ull);
-
-    // Stoichiometry of the chosen reaction, ascending species.
-    const uint32_t e0 = __ldg(m.stoich_off + idx), e1 = __ldg(m.stoich_off + idx + 1);
-    const int ne = (int)(e1 - e0) < MAX_STOICH ? (int)(e1 - e0) : MAX_STOICH;
-    uint32_t sp[MAX_STOICH];
-    int dlt[MAX_STOICH];
-    for (int e = 0; e < ne; e++) {
-        sp[e] = __ldg(m.stoich_sp + e0 + e);
-        dlt[e] = __ldg(m.stoich_d + e0 + e);
-    }
-    // Survivors in slot order; a consumed reactant bumps its count.
-    SiteWords<BPS, S> out;
-    out.clear();
-    int n = 0;
-#pragma unroll
-    for (int k = 0; k < S; k++) {
-        const uint32_t q = s.slot(k);
-        if (q > 0) {
-            bool consumed = false;
-            for (int e = 0; e < ne; e++) {
-                if (sp[e] == q - 1) {
-                    if (dlt[e] < 0) {
-                        dlt[e]++;
-                        consumed = true;
-                    }
-                    break;
-                }
-            }
-            if (!consumed) out.put(n++, q);
-        }
-    }
-    // Products by ascending species id; extra ones overflow.
-    uint32_t seq = 0;
-    for (int e = 0; e < ne; e++) {
-        for (int j = 0; j < dlt[e]; j++) {
-            const uint32_t p = sp[e] + 1;
-            if (n < S) out.put(n++, p);
-            else push_overflow(rs, list, cap, 4u, i, seq++, p);
-        }
-    }
-    out.store(lat, g.N, i);
+    if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) s.store(lat, g.N, i);
 }
 
 // ---------------------------------------------------------------------------
-// Overflow resolution (one block)
+// Overflow resolution (one block; the logic is in lmb_overflow.cuh)
 // ---------------------------------------------------------------------------
-
-template <int BPS, int S>
-__device__ uint32_t occupancy_at(const uint32_t *lat, uint32_t N, uint32_t i)
-{
-    SiteWords<BPS, S> s;
-    s.load_plain(lat, N, i);
-    uint32_t k = 0;
-#pragma unroll
-    for (int j = 0; j < S; j++)
-        if (k == (uint32_t)j && s.slot(j) != 0) k++;
-    return k;
-}
-
-// First empty slot of site i gets p (ByteLattice.cpp:265-289); false if full.
-template <int BPS, int S>
-__device__ bool add_particle(uint32_t *lat, uint32_t N, uint32_t i, uint32_t p)
-{
-    SiteWords<BPS, S> s;
-    s.load_plain(lat, N, i);
-#pragma unroll
-    for (int j = 0; j < S; j++) {
-        if (s.slot(j) == 0) {
-            s.put(j, p);
-            s.store(lat, N, i);
-            return true;
-        }
-    }
-    return false;
-}
-
-// Classic reinsertion (MpdRdmeSolver.cu:1103-1189): shells of radius 0..4
-// from Lattice::getNearbySites (Lattice.cpp:106-128: clamped to the lattice,
-// x outer, y, z inner), first site of the same type with a free slot.
-template <int BPS, int S>
-__device__ bool reinsert_classic(uint32_t *lat, const uint8_t *sites, const Geometry &g, uint32_t idx, uint32_t p)
-{
-    const uint32_t xc = idx % g.X, yc = (idx / g.X) % g.Y, zc = idx / g.XY;
-    const uint8_t tc = sites[idx];
-    for (uint32_t radius = 0; radius <= 4; radius++) {
-        const uint32_t mind = radius > 0 ? radius - 1 : 0, maxd = radius;
-        const double min2 = (double)(mind * mind), max2 = (double)(maxd * maxd);
-        const uint32_t x0 = xc >= maxd ? xc - maxd : 0, x1 = (xc + maxd < g.X) ? xc + maxd : g.X - 1;
-        const uint32_t y0 = yc >= maxd ? yc - maxd : 0, y1 = (yc + maxd < g.Y) ? yc + maxd : g.Y - 1;
-        const uint32_t z0 = zc >= maxd ? zc - maxd : 0, z1 = (zc + maxd < g.Z) ? zc + maxd : g.Z - 1;
-        for (uint32_t x = x0; x <= x1; x++)
-            for (uint32_t y = y0; y <= y1; y++)
-                for (uint32_t z = z0; z <= z1; z++) {
-                    const double dx = (double)x - xc, dy = (double)y - yc, dz = (double)z - zc;
-                    const double r2 = dx * dx + dy * dy + dz * dz;
-                    if (!(r2 <= max2 && (r2 > min2 || mind == maxd))) continue;
-                    const uint32_t j = x + y * g.X + z * g.XY;
-                    if (sites[j] == tc && occupancy_at<BPS, S>(lat, g.N, j) < (uint32_t)S)
-                        if (add_particle<BPS, S>(lat, g.N, j, p)) return true;
-                }
-    }
-    return false;
-}
 
 constexpr int RESOLVE_THREADS = 512;
 
-// Sorts the step's overflow entries by key (carried entries first, then
-// (phase, site, seq)) and reinserts them in that order; advances the step.
 template <int BPS, int S>
 __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__restrict__ lat,
                                                                   const uint8_t *__restrict__ sites, Geometry g,
@@ -315,76 +102,7 @@ __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__re
 {
     extern __shared__ OverflowEntry sh[];
     if (rs->status != LMB_OK) return;
-    const uint32_t n = rs->ovf_count;
-    const uint32_t carried = rs->carried;
-    if (n == 0) {
-        if (threadIdx.x == 0) rs->step++;
-        return;
-    }
-    if (n > cap) {
-        if (threadIdx.x == 0) {
-            rs->overflows += (unsigned long long)(n - carried);
-            rs->status = LMB_E_OVERFLOW_EXHAUSTED;
-            rs->failed_step = rs->step;
-        }
-        return;
-    }
-    uint32_t pow2 = 1;
-    while (pow2 < n) pow2 <<= 1;
-    for (uint32_t e = threadIdx.x; e < pow2; e += blockDim.x) {
-        if (e < n) sh[e] = list[e];
-        else {
-            sh[e].key = ~0ull;
-            sh[e].site = 0;
-            sh[e].particle = 0;
-        }
-    }
-    __syncthreads();
-    // Bitonic sort of pow2 entries by key.
-    for (uint32_t k = 2; k <= pow2; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t e = threadIdx.x; e < pow2; e += blockDim.x) {
-                const uint32_t o = e ^ j;
-                if (o > e) {
-                    const bool up = (e & k) == 0;
-                    const OverflowEntry a = sh[e], b = sh[o];
-                    if ((a.key > b.key) == up) {
-                        sh[e] = b;
-                        sh[o] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    if (threadIdx.x != 0) return;
-    rs->overflows += (unsigned long long)(n - carried);
-    if (rs->mode == LMB_OVERFLOW_CLASSIC) {
-        for (uint32_t e = 0; e < n; e++) {
-            if (!reinsert_classic<BPS, S>(lat, sites, g, sh[e].site, sh[e].particle)) {
-                rs->status = LMB_E_OVERFLOW_UNRESOLVED;
-                rs->failed_step = rs->step;
-                return;
-            }
-        }
-        rs->ovf_count = 0;
-        rs->carried = 0;
-    } else {
-        // Relaxed (MpdRdmeSolver.cu:1677-1761): own site only; the rest stay
-        // queued, in order, for the next timestep.
-        uint32_t kept = 0;
-        for (uint32_t e = 0; e < n; e++) {
-            if (!add_particle<BPS, S>(lat, g.N, sh[e].site, sh[e].particle)) {
-                OverflowEntry o = sh[e];
-                o.key = (unsigned long long)kept;  // phase 0, list order
-                list[kept++] = o;
-            }
-        }
-        rs->ovf_count = kept;
-        rs->carried = kept;
-    }
-    __threadfence();
-    rs->step++;
+    resolve_block<BPS, S>(lat, sites, g, rs, list, cap, sh);
 }
 
 // Sets the run state for a new run without a host round trip.  The relaxed
@@ -399,6 +117,7 @@ __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, ui
     rs->mode = mode;
     rs->overflows = 0;
     rs->reactions = 0;
+    rs->tiles_done = 0;
     if (mode == LMB_OVERFLOW_CLASSIC) {
         rs->ovf_count = 0;
         rs->carried = 0;

@@ -180,6 +180,20 @@ class Lattice:
         L.check(L.lib().lmb_lattice_get_row_major(self.handle, p.ctypes.data_as(C.c_void_p), _p(s, L.u8p)))
         return p, s
 
+    def set_schedule(self, schedule, Ty=0, Tz=0):
+        L.check(L.lib().lmb_lattice_set_schedule(self.handle, schedule, Ty, Tz), "lmb_lattice_set_schedule")
+
+    def schedule(self):
+        s, ty, tz = C.c_int(), C.c_uint32(), C.c_uint32()
+        L.check(L.lib().lmb_lattice_get_schedule(self.handle, C.byref(s), C.byref(ty), C.byref(tz)))
+        return s.value, ty.value, tz.value
+
+    def autotune(self, model, seed, first_timestep, timesteps):
+        s, ty, tz, ms = C.c_int(), C.c_uint32(), C.c_uint32(), C.c_float()
+        L.check(L.lib().lmb_lattice_autotune(self.handle, model.handle, seed, first_timestep, timesteps,
+                                             C.byref(s), C.byref(ty), C.byref(tz), C.byref(ms)), "autotune")
+        return s.value, ty.value, tz.value, ms.value
+
     def device_buffers(self):
         a, b = L.vp(), L.vp()
         L.check(L.lib().lmb_lattice_device_buffers(self.handle, C.byref(a), C.byref(b)))
@@ -200,10 +214,10 @@ class Lattice:
 
     def run_profiled(self, model, seed, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
         """Runs with CUDA events around every kernel; returns (stats, phase
-        milliseconds [x, y, z, reaction, overflow], launches per phase)."""
+        milliseconds [x, y, z, reaction, overflow, fused], launches per phase)."""
         st = L.RunStats()
-        ms = np.zeros(5, dtype=np.float32)
-        n = np.zeros(5, dtype=np.uint32)
+        ms = np.zeros(6, dtype=np.float32)
+        n = np.zeros(6, dtype=np.uint32)
         L.check(L.lib().lmb_run_profiled(self.handle, model.handle, seed, first_timestep, timesteps, overflow_mode,
                                          _p(ms, L.f32p), _p(n, L.u32p), C.byref(st)), "lmb_run_profiled")
         return st, ms, n

@@ -24,11 +24,20 @@ def ctx(gpu):
     c.close()
 
 
-def _gpu_run(ctx, tables_or_spec, lattice, sites, seed, step0, nsteps, mode=0, from_spec=False, chunks=None):
+SCHEDULES = ["fused", "phases"]
+
+
+def _gpu_run(ctx, tables_or_spec, lattice, sites, seed, step0, nsteps, mode=0, from_spec=False, chunks=None,
+             schedule="fused", tile=(0, 0)):
+    from lattice_microbes_b200 import _lib as L
     from lattice_microbes_b200.solver import Lattice, Model
     t = tables_or_spec
     model = Model.from_spec(ctx, t) if from_spec else Model.from_tables(ctx, t)
     lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
+    if schedule == "phases":
+        lat.set_schedule(L.LMB_SCHEDULE_PHASES)
+    else:
+        lat.set_schedule(L.LMB_SCHEDULE_FUSED, *tile)
     lat.set_native(lattice, sites)
     if chunks is None:
         chunks = [nsteps]
@@ -45,10 +54,12 @@ def _gpu_run(ctx, tables_or_spec, lattice, sites, seed, step0, nsteps, mode=0, f
     return out, rc, stats
 
 
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("name", case_names())
-def test_golden_fixture(ctx, name):
+def test_golden_fixture(ctx, name, schedule):
     t, g = load_case(name)
-    out, rc, st = _gpu_run(ctx, t, g["lattice_in"], g["sites"], int(g["seed"]), int(g["step0"]), int(g["nsteps"]))
+    out, rc, st = _gpu_run(ctx, t, g["lattice_in"], g["sites"], int(g["seed"]), int(g["step0"]), int(g["nsteps"]),
+                           schedule=schedule)
     assert rc == 0
     assert st[0].overflows == int(g["overflows"])
     assert st[0].reactions == int(g["reactions"])
@@ -58,54 +69,89 @@ def test_golden_fixture(ctx, name):
 VARIANTS = [(4, 1), (8, 1), (16, 1), (32, 1), (4, 4), (8, 4), (16, 4)]
 
 
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("slots,bps", VARIANTS)
 @pytest.mark.parametrize("seed", [0, 1])
-def test_random_problem_vs_oracle(ctx, seed, slots, bps):
+def test_random_problem_vs_oracle(ctx, seed, slots, bps, schedule):
     dens = {4: 0.3, 8: 0.5, 16: 1.2, 32: 2.0}[slots]
     spec = configs.random_problem(seed, X=32, Y=16, Z=16, slots=slots, bytes_per_slot=bps, density=dens)
     t = oracle_tables(spec)
     ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 4321 + seed, 11, 12)
-    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 4321 + seed, 11, 12)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 4321 + seed, 11, 12, schedule=schedule)
     assert rc == rc_ref == 0
     assert (st[0].overflows, st[0].reactions) == (st_ref.overflows, st_ref.reactions)
     assert np.array_equal(out, ref)
 
 
-@pytest.mark.parametrize("shape", [(16, 24, 8), (24, 16, 40), (7, 5, 3), (48, 8, 16), (1, 8, 8)])
-def test_odd_shapes_vs_oracle(ctx, shape):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+@pytest.mark.parametrize("shape", [(16, 24, 8), (24, 16, 40), (7, 5, 3), (48, 8, 16), (1, 8, 8), (200, 2, 1)])
+def test_odd_shapes_vs_oracle(ctx, shape, schedule):
     X, Y, Z = shape
     spec = configs.random_problem(5, X=X, Y=Y, Z=Z, density=0.6)
     t = oracle_tables(spec)
     ref, rc_ref, _ = oracle_run(t, spec.lattice, spec.sites, 99, 0, 10)
-    out, rc, _ = _gpu_run(ctx, t, spec.lattice, spec.sites, 99, 0, 10)
+    out, rc, _ = _gpu_run(ctx, t, spec.lattice, spec.sites, 99, 0, 10, schedule=schedule)
     assert rc == rc_ref
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("slots,bps,dens", [(8, 1, 5.0), (16, 4, 12.0), (8, 4, 6.0)])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
-def test_overflow_storm_vs_oracle(ctx, seed, slots, bps, dens):
+def test_overflow_storm_vs_oracle(ctx, seed, slots, bps, dens, schedule):
     """Heavy overflow traffic; seeds 1-3 end in the reference's two errors
     (list exhausted / no free site), which must stop at the same step with
     the same partial lattice."""
     spec = configs.random_problem(seed, X=32, Y=8, Z=8, slots=slots, bytes_per_slot=bps, density=dens, nst=2)
     t = oracle_tables(spec)
     ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 99 + seed, 5, 8)
-    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 99 + seed, 5, 8)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 99 + seed, 5, 8, schedule=schedule)
     assert rc == rc_ref
     if rc == 0:
         assert st[0].overflows == st_ref.overflows
     assert np.array_equal(out, ref)
 
 
-def test_relaxed_handler_vs_oracle(ctx):
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_relaxed_handler_vs_oracle(ctx, schedule):
     spec = configs.random_problem(2, X=32, Y=8, Z=8, slots=8, bytes_per_slot=1, density=3.0, nst=2)
     t = oracle_tables(spec)
     ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 7, 0, 6, mode=1)
-    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 7, 0, 6, mode=1)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 7, 0, 6, mode=1, schedule=schedule)
     assert rc == rc_ref
     assert st[-1].unresolved == st_ref.unresolved
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("tile", [(1, 1), (2, 4), (4, 2), (8, 8), (16, 8)])
+def test_fused_tile_shapes_vs_oracle(ctx, tile):
+    spec = configs.random_problem(12, X=64, Y=16, Z=32, density=0.8, nst=3)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 1717, 3, 9)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 1717, 3, 9, tile=tile)
+    assert rc == rc_ref == 0
+    assert st[0].overflows == st_ref.overflows
+    assert np.array_equal(out, ref)
+
+
+def test_autotune_keeps_state_and_result(ctx):
+    from lattice_microbes_b200.solver import Lattice, Model
+    spec = configs.config0(seed=7)
+    t = oracle_tables(spec)
+    m = Model.from_spec(ctx, spec)
+    lat = Lattice(ctx, spec.X, spec.Y, spec.Z, 8, 1)
+    lat.set_native(spec.lattice, spec.sites)
+    sched, ty, tz, ms = lat.autotune(m, 5, 0, 20)
+    assert ms > 0
+    assert lat.schedule()[0] == sched
+    p, _ = lat.get_native()
+    assert np.array_equal(p, spec.lattice)  # state restored
+    lat.run(m, 5, 0, 30)
+    out, _ = lat.get_native()
+    ref, _, _ = oracle_run(t, spec.lattice, spec.sites, 5, 0, 30)
+    assert np.array_equal(out, ref)
+    lat.close()
+    m.close()
 
 
 def test_chunked_run_equals_single_run(ctx):
