@@ -212,6 +212,21 @@ def run_ours(a):
     seed = compose_seed(2024, rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
 
+    # The reference's own kernels (compiled for sm_100a from its sources) on
+    # this GPU, with its per-timestep host flow: the GPU bar to beat.
+    ref_gpu = None
+    if rank == 0:
+        try:
+            from tests.cases import oracle_tables
+            from tests.oracle_lib import reference_gpu_time
+            r = reference_gpu_time(oracle_tables(spec), spec.lattice, spec.sites, seed, 0, 1000)
+            if r is not None and r[0] == 0:
+                ref_gpu = {"value": N * 1000 / (r[1] / 1e3), "unit": METRIC, "timesteps": 1000,
+                           "what": "reference device functions built for sm_100a, reference host loop "
+                                   "(4 launches + stream sync + overflow check per timestep)"}
+        except Exception as e:  # checker absent: report why
+            ref_gpu = {"unavailable": str(e)[:200]}
+
     from lattice_microbes_b200 import _lib as LL
     tuned = None
     if a.schedule == "phases":
@@ -354,6 +369,7 @@ def run_ours(a):
             "gpu_launches": int(launches),
             "clocks": clock_info,
             "cpu_baseline": cpu,
+            "reference_kernels_b200": ref_gpu,
             "run_stats": {"overflows": int(st.overflows), "reactions_per_step": int(st.reactions)},
         }
         print(json.dumps(line), flush=True)

@@ -69,22 +69,9 @@ namespace refdev {
 
 using namespace refdev;
 
-/* The native buffers are protected members; the reference's CUDA lattices
- * reach them by derivation, and so does this checker. */
-template <class Base>
-struct OpenLattice : public Base {
-    OpenLattice(lattice_size_t x, lattice_size_t y, lattice_size_t z, unsigned s) : Base(x, y, z, 1.0, s) {}
-    uint32_t *particles() { return this->getParticlesMemory(); }
-    uint8_t *site_types() { return this->getSitesMemory(); }
-};
-#if defined(REF_BYTE)
-typedef OpenLattice<lm::rdme::ByteLattice> RefLattice;
-#else
-typedef OpenLattice<lm::rdme::IntLattice> RefLattice;
-#endif
+static const unsigned REF_LIST_CAP_C = TUNE_MPD_MAX_PARTICLE_OVERFLOWS;
+#include "ref_classic.h"
 
-static const unsigned REF_WORDS = MPD_WORDS_PER_SITE;
-static const unsigned REF_LIST_CAP = TUNE_MPD_MAX_PARTICLE_OVERFLOWS;
 
 /* Model tables kept alive for the duration of a run. */
 static std::vector<float> g_T, g_qp0, g_qp1, g_qp2, g_rate;
@@ -93,13 +80,9 @@ static std::vector<int8_t> g_S;
 static std::vector<uint8_t> g_RL;
 static unsigned g_X, g_Y, g_Z;
 
-struct Entry {
-    uint32_t site, particle, phase, seq;
-};
-
 extern "C" int ref_words_per_site() { return (int)REF_WORDS; }
 extern "C" int ref_slots_per_site() { return MPD_LATTICE_MAX_OCCUPANCY; }
-extern "C" int ref_list_capacity() { return (int)REF_LIST_CAP; }
+extern "C" int ref_list_capacity() { return (int)REF_LIST_CAP_C; }
 
 extern "C" uint32_t ref_device_hash(uint64_t key, uint64_t th)
 {
@@ -315,52 +298,6 @@ static void reaction(unsigned *lat, const uint8_t *sites, uint64_t th, unsigned 
                     }
 }
 
-/* Collects list entries [from, to) as (phase, site, seq) records; the entries
- * of one site come from one thread, in order. */
-static void collect(const unsigned *list, unsigned from, unsigned to, unsigned phase, std::vector<Entry> &out)
-{
-    std::vector<Entry> seg;
-    for (unsigned e = from; e < to && e < REF_LIST_CAP; e++)
-        seg.push_back(Entry{list[2 * e + 1], list[2 * e + 2], phase, 0});
-    std::stable_sort(seg.begin(), seg.end(), [](const Entry &a, const Entry &b) { return a.site < b.site; });
-    for (size_t k = 0; k < seg.size(); k++) {
-        seg[k].seq = (k > 0 && seg[k - 1].site == seg[k].site) ? seg[k - 1].seq + 1 : 0;
-        out.push_back(seg[k]);
-    }
-}
-
-/* MpdRdmeSolver.cu:1113-1150 with the reference lattice class. */
-static int classic_reinsert(unsigned *lat, const uint8_t *sites, const std::vector<Entry> &entries)
-{
-    const size_t N = (size_t)g_X * g_Y * g_Z;
-    RefLattice lattice(g_X, g_Y, g_Z, MPD_LATTICE_MAX_OCCUPANCY);
-    memcpy(lattice.particles(), lat, N * REF_WORDS * sizeof(uint32_t));
-    memcpy(lattice.site_types(), sites, N);
-    for (const Entry &e : entries) {
-        lattice_size_t x = e.site % g_X, y = (e.site / g_X) % g_Y, z = e.site / (g_X * g_Y);
-        bool placed = false;
-        for (unsigned radius = 0; !placed && radius <= TUNE_MPD_MAX_OVERFLOW_REPLACEMENT_DIST; radius++) {
-            std::vector<lattice_coord_t> near = lattice.getNearbySites(x, y, z, radius > 0 ? radius - 1 : 0, radius);
-            for (const lattice_coord_t &s : near) {
-                if (lattice.getOccupancy(s.x, s.y, s.z) < lattice.getMaxOccupancy() &&
-                    lattice.getSiteType(s.x, s.y, s.z) == lattice.getSiteType(x, y, z)) {
-                    lattice.addParticle(s.x, s.y, s.z, e.particle);
-                    placed = true;
-                    break;
-                }
-            }
-        }
-        if (!placed) {
-            /* The reference throws here with the host lattice partly updated;
-             * the checker keeps that partial state for comparison. */
-            memcpy(lat, lattice.particles(), N * REF_WORDS * sizeof(uint32_t));
-            return -7;
-        }
-    }
-    memcpy(lat, lattice.particles(), N * REF_WORDS * sizeof(uint32_t));
-    return 0;
-}
-
 /*
  * Runs nsteps timesteps.  th[4*s + k] is the timestep hash of step s,
  * substep k (computed by the caller with the getTimestepSeed mixing).
@@ -371,7 +308,7 @@ extern "C" int ref_run(uint32_t *lat, const uint8_t *sites, const uint64_t *th, 
 {
     const size_t N = (size_t)g_X * g_Y * g_Z;
     std::vector<unsigned> tmp(N * REF_WORDS);
-    std::vector<unsigned> list(1 + 2 * REF_LIST_CAP, 0u);
+    std::vector<unsigned> list(1 + 2 * REF_LIST_CAP_C, 0u);
     uint64_t ovf = 0, rx = 0;
     for (uint32_t s = 0; s < nsteps; s++) {
         list[0] = 0;
@@ -390,8 +327,8 @@ extern "C" int ref_run(uint32_t *lat, const uint8_t *sites, const uint64_t *th, 
         }
         ovf += list[0];
         int rc = 0;
-        if (list[0] > REF_LIST_CAP) rc = -6;
-        else if (list[0] > 0) rc = classic_reinsert(lat, sites, entries);
+        if (list[0] > REF_LIST_CAP_C) rc = -6;
+        else if (list[0] > 0) rc = classic_reinsert(lat, sites, entries, g_X, g_Y, g_Z);
         if (rc) {
             if (overflows_out) *overflows_out = ovf;
             if (reactions_out) *reactions_out = rx;

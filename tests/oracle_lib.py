@@ -193,3 +193,66 @@ def reference_run(tables, lattice, sites, seed, step0, nsteps):
     rx = C.c_uint64(0)
     rc = lib.ref_run(_ptr(lat, u32p), _ptr(st, u8p), _ptr(th, u64p), nsteps, C.byref(ovf), C.byref(rx))
     return lat, rc, ovf.value, rx.value
+
+
+_refg = {}
+
+
+def reference_gpu(kind, slots, nofma=False):
+    """The reference's device functions compiled for sm_100a (oracle/_ref)."""
+    key = (kind, slots, nofma)
+    if key not in _refg:
+        path = os.path.join(REF_DIR, "libref_gpu_%s%d%s.so" % (kind, slots, "_nofma" if nofma else ""))
+        if not os.path.exists(path):
+            return None
+        lib = C.CDLL(path, mode=C.RTLD_LOCAL)
+        lib.refg_set_model.restype = C.c_int
+        lib.refg_set_model.argtypes = [C.c_uint32] * 6 + [f32p, f32p, f32p, f32p, u32p, u32p, u32p,
+                                                          f32p, i8p, u8p]
+        lib.refg_supported.restype = C.c_int
+        lib.refg_supported.argtypes = [C.c_uint32] * 3
+        lib.refg_run.restype = C.c_int
+        lib.refg_run.argtypes = [u32p, u8p, u64p, C.c_uint32, u64p]
+        lib.refg_time.restype = C.c_int
+        lib.refg_time.argtypes = [u32p, u8p, u64p, C.c_uint32, C.POINTER(C.c_double)]
+        _refg[key] = lib
+    return _refg[key]
+
+
+def _refg_prepare(tables, nofma=False):
+    kind = "byte" if tables.bytes_per_slot == 1 else "int"
+    lib = reference_gpu(kind, tables.slots, nofma)
+    if lib is None or not lib.refg_supported(tables.X, tables.Y, tables.Z):
+        return None
+    t = tables
+    rc = lib.refg_set_model(t.X, t.Y, t.Z, t.ns, t.nst, t.nr, _ptr(t.T, f32p), _ptr(t.qp0, f32p),
+                            _ptr(t.qp1, f32p), _ptr(t.qp2, f32p), _ptr(t.order, u32p), _ptr(t.D1, u32p),
+                            _ptr(t.D2, u32p), _ptr(t.rate, f32p), _ptr(t.S, i8p), _ptr(t.RL, u8p))
+    assert rc == 0, rc
+    return lib
+
+
+def reference_gpu_run(tables, lattice, sites, seed, step0, nsteps, nofma=False):
+    """Replays through the reference kernels on the GPU; None if unavailable."""
+    lib = _refg_prepare(tables, nofma)
+    if lib is None:
+        return None
+    lat = np.ascontiguousarray(lattice, dtype=np.uint32).copy()
+    st = np.ascontiguousarray(sites, dtype=np.uint8)
+    th = timestep_hashes(seed, step0, nsteps)
+    ovf = C.c_uint64(0)
+    rc = lib.refg_run(_ptr(lat, u32p), _ptr(st, u8p), _ptr(th, u64p), nsteps, C.byref(ovf))
+    return lat, rc, ovf.value
+
+
+def reference_gpu_time(tables, lattice, sites, seed, step0, nsteps):
+    """Wall time (ms) of the reference's timestep loop on the GPU."""
+    lib = _refg_prepare(tables)
+    if lib is None:
+        return None
+    lat = np.ascontiguousarray(lattice, dtype=np.uint32).copy()
+    st = np.ascontiguousarray(sites, dtype=np.uint8)
+    th = timestep_hashes(seed, step0, nsteps)
+    ms = C.c_double(0)
+    rc = lib.refg_time(_ptr(lat, u32p), _ptr(st, u8p), _ptr(th, u64p), nsteps, C.byref(ms))
+    return rc, ms.value, lat
