@@ -74,6 +74,16 @@ struct lmb_lattice {
     // Schedule: fused tile kernel (one launch per timestep) or per-phase kernels.
     int schedule;
     TileShape tile;
+    // Captured timestep graphs, one per starting buffer parity.
+    struct Graph {
+        cudaGraphExec_t exec;
+        const void *model;
+        const void *tables;
+        int schedule;
+        uint32_t Ty, Tz;
+        bool reaction;
+        uint64_t kernels;
+    } graph[2];
     // Pending async run.
     bool pending;
     int pending_cur0;
@@ -266,6 +276,18 @@ static int upload_model(lmb_model *m)
     m->dev.stoich_off = (const uint32_t *)(b + off[9]);
     m->dev.stoich_sp = (const uint32_t *)(b + off[10]);
     m->dev.stoich_d = (const int32_t *)(b + off[11]);
+    m->dev.nnz = (uint32_t)m->st_sp.size();
+    m->dev.stage_bytes = 0;
+    {
+        // Tables small enough to copy into shared memory per block (16-byte
+        // aligned pieces, in the order the fused kernel lays them out).
+        size_t bytes = 0;
+        const size_t pieces[] = {m->T.size() * 4, m->qp0.size() * 4, m->qp1.size() * 4, m->qp2.size() * 4,
+                                 (size_t)m->nr * 4, (size_t)m->nr * 4, (size_t)m->nr * 4, (size_t)m->nr * 4,
+                                 m->RL.size(), ((size_t)m->nr + 1) * 4, m->st_sp.size() * 4, m->st_d.size() * 4};
+        for (size_t p : pieces) bytes += (p + 15) & ~(size_t)15;
+        if (bytes <= 8 * 1024) m->dev.stage_bytes = (uint32_t)bytes;
+    }
     m->dirty = false;
     return LMB_OK;
 }
@@ -586,6 +608,8 @@ extern "C" int lmb_lattice_destroy(lmb_lattice *l)
     if (l->list) cudaFree(l->list);
     if (l->counts_dev) cudaFree(l->counts_dev);
     if (l->rs_host) cudaFreeHost(l->rs_host);
+    for (auto &gr : l->graph)
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
     delete l;
     return LMB_OK;
 }
@@ -712,6 +736,82 @@ extern "C" int lmb_lattice_species_counts(lmb_lattice *l, uint32_t ns, uint64_t 
 // Timesteps
 // ---------------------------------------------------------------------------
 
+
+// ---------------------------------------------------------------------------
+// Timestep enqueue and graph capture
+// ---------------------------------------------------------------------------
+
+static const uint32_t GRAPH_STEPS = 32;  // even: a replay returns to the same buffer parity
+
+// Queues one timestep (schedule of the lattice) and flips the buffer index.
+static cudaError_t enqueue_step(lmb_lattice *l, lmb_model *m, cudaStream_t st)
+{
+    const int bps = (int)l->bps, S = (int)l->slots;
+    uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
+    cudaError_t e;
+    if (l->schedule == LMB_SCHEDULE_FUSED) {
+        e = launch_fused(bps, S, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, l->tile, m->nr > 0, st);
+        l->cur ^= 1;
+        return e;
+    }
+    if ((e = launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess) return e;
+    if ((e = launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess) return e;
+    if ((e = launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess) return e;
+    l->cur ^= 1;
+    if (m->nr > 0 &&
+        (e = launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess)
+        return e;
+    return launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, st);
+}
+
+// Captures GRAPH_STEPS timesteps starting at the current buffer parity, or
+// keeps the graph captured before for the same model storage and schedule.
+// Every kernel reads the step index from the run state, so one graph serves
+// any run.
+static int ensure_graph(lmb_lattice *l, lmb_model *m)
+{
+    lmb_lattice::Graph &gr = l->graph[l->cur];
+    const bool same = gr.exec && gr.model == m && gr.tables == m->dev_block && gr.schedule == l->schedule &&
+                      gr.Ty == l->tile.Ty && gr.Tz == l->tile.Tz && gr.reaction == (m->nr > 0);
+    if (same) return LMB_OK;
+    if (gr.exec) {
+        cudaGraphExecDestroy(gr.exec);
+        gr.exec = nullptr;
+    }
+    cudaStream_t st = l->ctx->stream;
+    const int cur0 = l->cur;
+    const uint64_t launches0 = lmb_kernel_launches();
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return LMB_E_UNSUPPORTED;
+    }
+    cudaError_t e = cudaSuccess;
+    for (uint32_t s = 0; s < GRAPH_STEPS && e == cudaSuccess; s++) e = enqueue_step(l, m, st);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    l->cur = cur0;
+    const uint64_t captured = lmb_kernel_launches() - launches0;
+    count_launch((uint64_t)0 - captured);  // captured launches run only when replayed
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_status(e != cudaSuccess ? e : e2);
+    }
+    e = cudaGraphInstantiate(&gr.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        gr.exec = nullptr;
+        return cuda_status(e);
+    }
+    gr.model = m;
+    gr.tables = m->dev_block;
+    gr.schedule = l->schedule;
+    gr.Ty = l->tile.Ty;
+    gr.Tz = l->tile.Tz;
+    gr.reaction = m->nr > 0;
+    gr.kernels = captured;
+    return LMB_OK;
+}
+
 static int validate_for_model(lmb_lattice *l, const lmb_model *m)
 {
     if (!l->validated) {
@@ -752,24 +852,19 @@ extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed,
     int rc = validate_for_model(l, m);
     if (rc) return rc;
     CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream));
-    const int bps = (int)l->bps, S = (int)l->slots;
     l->pending_cur0 = l->cur;
-    for (uint32_t s = 0; s < n; s++) {
-        uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
-        if (l->schedule == LMB_SCHEDULE_FUSED) {
-            CK(launch_fused(bps, S, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, l->tile, m->nr > 0,
-                            c->stream));
-            l->cur ^= 1;
-            continue;
+    uint32_t done = 0;
+    // Whole graphs of GRAPH_STEPS timesteps, then single launches.
+    // A stream that cannot be captured (the legacy default stream) runs
+    // every timestep as single launches.
+    if (n >= 2 * GRAPH_STEPS && ensure_graph(l, m) == LMB_OK) {
+        lmb_lattice::Graph &gr = l->graph[l->cur];
+        for (; done + GRAPH_STEPS <= n; done += GRAPH_STEPS) {
+            CK(cudaGraphLaunch(gr.exec, c->stream));
+            count_launch(gr.kernels);
         }
-        CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
-        CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
-        CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
-        l->cur ^= 1;
-        if (m->nr > 0)
-            CK(launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
-        CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, c->stream));
     }
+    for (; done < n; done++) CK(enqueue_step(l, m, c->stream));
     CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));
     l->pending = true;
     l->pending_first = first;

@@ -12,6 +12,14 @@
 
 namespace lmb {
 
+// Model-table read.  The tables live in global memory, or in shared memory
+// when a kernel stages them there, so the load is a generic one.
+template <typename T>
+__device__ __forceinline__ T tload(const T *p)
+{
+    return *p;
+}
+
 // Counter hash of (key ^ timestep hash), upper 32 bits
 // (rdme/dev/xor_random_dev.cu:46-53).
 __device__ __forceinline__ uint32_t mix_hash(unsigned long long v, unsigned long long th)
@@ -109,7 +117,7 @@ struct SiteWords {
 __device__ __forceinline__ float lookup_T(const DevTables &m, uint32_t p, uint32_t src, uint32_t dst)
 {
     if ((uint32_t)(p - 1u) >= m.ns || dst >= m.nst || src >= m.nst) return 0.0f;
-    return __ldg(m.T + ((size_t)src * m.nst + dst) * m.ns + (p - 1u));
+    return tload(m.T + ((size_t)src * m.nst + dst) * m.ns + (p - 1u));
 }
 
 // Queues one overflowed particle; the list index comes from an atomic, the

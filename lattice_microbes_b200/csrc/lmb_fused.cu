@@ -43,125 +43,354 @@ __device__ __forceinline__ void store_smem(uint32_t *buf, uint32_t R, uint32_t l
     for (int k = 0; k < SiteWords<BPS, S>::W; k++) buf[(size_t)k * R + l] = s.w[k];
 }
 
+// Copies the model tables into shared memory at `dst` (stage_bytes long,
+// 16-byte aligned pieces) and returns a table set pointing there.
+__device__ __forceinline__ DevTables stage_tables(const DevTables &m, uint8_t *dst, uint32_t tid, uint32_t nthr)
+{
+    DevTables s = m;
+    const void *srcs[12] = {m.T, m.qp0, m.qp1, m.qp2, m.order, m.D1, m.D2, m.rate, m.RL, m.stoich_off,
+                            m.stoich_sp, m.stoich_d};
+    const uint32_t sizes[12] = {m.nst * m.nst * m.ns * 4, m.nst * 4, m.nst * m.ns * 4, m.nst * m.ns * m.ns * 4,
+                                m.nr * 4, m.nr * 4, m.nr * 4, m.nr * 4, m.nr * m.nst, (m.nr + 1) * 4, m.nnz * 4,
+                                m.nnz * 4};
+    void *outs[12];
+    uint32_t off = 0;
+    for (int k = 0; k < 12; k++) {
+        outs[k] = dst + off;
+        const uint8_t *sp = (const uint8_t *)srcs[k];
+        for (uint32_t b = tid; b < sizes[k]; b += nthr) dst[off + b] = sp[b];
+        off += (sizes[k] + 15u) & ~15u;
+    }
+    s.T = (const float *)outs[0];
+    s.qp0 = (const float *)outs[1];
+    s.qp1 = (const float *)outs[2];
+    s.qp2 = (const float *)outs[3];
+    s.order = (const uint32_t *)outs[4];
+    s.D1 = (const uint32_t *)outs[5];
+    s.D2 = (const uint32_t *)outs[6];
+    s.rate = (const float *)outs[7];
+    s.RL = (const uint8_t *)outs[8];
+    s.stoich_off = (const uint32_t *)outs[9];
+    s.stoich_sp = (const uint32_t *)outs[10];
+    s.stoich_d = (const int32_t *)outs[11];
+    return s;
+}
+
+template <int BPS, int S>
+__device__ __noinline__ SiteWords<BPS, S> react_site_ool(SiteWords<BPS, S> s, uint32_t t, uint32_t gi,
+                                                         unsigned long long th, const DevTables &m, RunState *rs,
+                                                         OverflowEntry *list, uint32_t cap)
+{
+    react_site<BPS, S>(s, t, gi, th, m, rs, list, cap);
+    return s;
+}
+
+// Row flags of the loaded region.
+constexpr uint8_t ROW_OWNED = 1;
+
+// Bit x of the result is set when site x or one of its x neighbours (periodic
+// in the row of X sites) is occupied; `row` holds the row's MW mask words.
+__device__ __forceinline__ uint32_t x_neighbourhood(const uint32_t *row, uint32_t w, uint32_t MW, uint32_t X)
+{
+    const uint32_t cur = row[w];
+    const uint32_t prev = w > 0 ? row[w - 1] : 0u, next = w + 1 < MW ? row[w + 1] : 0u;
+    uint32_t a = cur | (cur << 1) | (cur >> 1) | (prev >> 31) | (next << 31);
+    // Periodic ends: x = 0 sees x = X - 1 and the other way round.
+    const uint32_t last_bit = (X - 1) & 31u, last_word = (X - 1) >> 5;
+    if (w == 0 && ((row[last_word] >> last_bit) & 1u)) a |= 1u;
+    if (w == last_word && (row[0] & 1u)) a |= 1u << last_bit;
+    const uint32_t valid = (w == last_word && (X & 31u)) ? ((1u << (X & 31u)) - 1u) : 0xffffffffu;
+    return a & valid;
+}
+
+// Warp-cooperative list append: every lane of the warp calls this with its
+// mask word (0 if none); entries (row << 16 | x) land contiguously in `work`
+// with one shared atomic per warp.
+__device__ __forceinline__ void warp_append(uint32_t b, uint32_t r, uint32_t w, uint32_t *work, uint32_t *count)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n = __popc(b);
+    uint32_t incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) return;
+    uint32_t base = 0;
+    if (lane == 31) base = atomicAdd(count, total);
+    base = __shfl_sync(0xffffffffu, base, 31) + incl - n;
+    while (b) {
+        const uint32_t k = __ffs(b) - 1;
+        b &= b - 1;
+        work[base++] = (r << 16) | (w * 32 + k);
+    }
+}
+
 template <int BPS, int S>
 __global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_t *__restrict__ src,
                                                                    uint32_t *__restrict__ dst,
                                                                    const uint8_t *__restrict__ sites, Geometry g,
-                                                                   DevTables m, RunState *__restrict__ rs,
+                                                                   const __grid_constant__ DevTables m,
+                                                                   RunState *__restrict__ rs,
                                                                    OverflowEntry *__restrict__ list, uint32_t cap,
-                                                                   TileShape ts, int with_reaction)
+                                                                   const __grid_constant__ TileShape ts,
+                                                                   int with_reaction)
 {
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_last;
+    __shared__ uint32_t s_cnt[4];
+    // Per region row: lattice index of its x = 0 site and its flags, and the
+    // region rows the y and z sweeps produce.  Filled once: no sweep divides.
+    __shared__ uint32_t rowbase[FUSED_MAX_ROWS];
+    __shared__ uint16_t yrow[FUSED_MAX_ROWS], zrow[FUSED_MAX_ROWS];
+    __shared__ uint8_t rowflag[FUSED_MAX_ROWS];
     constexpr int W = SiteWords<BPS, S>::W;
     if (rs->status != LMB_OK) return;
-    const uint32_t X = g.X, Y = g.Y, Z = g.Z, R = ts.R, Ry = ts.Ry, Ty = ts.Ty, Tz = ts.Tz;
-    uint32_t *A = smem;
-    uint32_t *B = smem + (size_t)W * R;
-    uint8_t *T = (uint8_t *)(smem + (size_t)2 * W * R);
+    const uint32_t X = g.X, R = ts.R, Ry = ts.Ry, Ty = ts.Ty, Tz = ts.Tz, MW = ts.MW;
     const uint32_t tyi = blockIdx.x % ts.tiles_y, tzi = blockIdx.x / ts.tiles_y;
     const uint32_t y0 = tyi * Ty, z0 = tzi * Tz;
     const uint32_t seed = rs->seed, step = rs->step;
     const uint32_t tx = threadIdx.x, ty = threadIdx.y, bx = blockDim.x, by = blockDim.y;
-    // Region row r = lz * Ry + ly maps to lattice row (y0 - 1 + ly, z0 - 1 + lz), periodic.
-#define GY(ly) ((y0 + (ly) + Y - 1) % Y)
-#define GZ(lz) ((z0 + (lz) + Z - 1) % Z)
+    const uint32_t tid = tx + ty * bx, nthr = bx * by;
+    const uint32_t rows = Ry * ts.Rz, yrows = Ty * ts.Rz, orows = Ty * Tz;
+    // Shared layout: A[W][R], B[W][R] particle words (valid where the
+    // occupancy bit is set), work[R] site list, T[R] site types, then
+    // occA / occB [rows * MW] occupancy bit masks.
+    uint32_t *A = smem;
+    uint32_t *B = A + W * R;
+    uint32_t *work = B + W * R;
+    uint8_t *T = (uint8_t *)(work + R);
+    uint32_t *occA = (uint32_t *)(T + ((R + 15u) & ~15u));
+    uint32_t *occB = occA + rows * MW;
+    uint8_t *tables = (uint8_t *)(occB + rows * MW);
+    // The model tables, from shared memory when they are small; the table set
+    // itself is kept in shared memory so that calls take it by reference
+    // without a per-thread copy.
+    __shared__ DevTables s_mt;
+    {
+        const DevTables staged = m.stage_bytes ? stage_tables(m, tables, tid, nthr) : m;
+        if (tid == 0) s_mt = staged;
+    }
+    const DevTables &mt = s_mt;
 
-    // Load the region.
-    const uint32_t rows = Ry * ts.Rz;
-    for (uint32_t r = ty; r < rows; r += by) {
+    for (uint32_t r = tid; r < rows; r += nthr) {
         const uint32_t ly = r % Ry, lz = r / Ry;
-        const uint32_t gbase = GY(ly) * X + GZ(lz) * g.XY;
-        for (uint32_t x = tx; x < X; x += bx) {
-            const uint32_t l = r * X + x, gi = gbase + x;
+        rowbase[r] = ((y0 + ly + g.Y - 1) % g.Y) * X + ((z0 + lz + g.Z - 1) % g.Z) * g.XY;
+        rowflag[r] = ly >= 1 && ly <= Ty && lz >= 1 && lz <= Tz ? ROW_OWNED : 0;
+    }
+    for (uint32_t q = tid; q < yrows; q += nthr) yrow[q] = (uint16_t)((q / Ty) * Ry + 1 + q % Ty);
+    for (uint32_t q = tid; q < orows; q += nthr) zrow[q] = (uint16_t)((1 + q / Ty) * Ry + 1 + q % Ty);
+    if (tid < 4) s_cnt[tid] = 0;
+    __syncthreads();
+
+    // ---- load the region ----
+    if (ts.vec) {
+        // 16-byte loads: an item is 4 consecutive sites of one row, read from
+        // every word plane (W 16-byte loads), with its 4 occupancy bits OR-ed
+        // into the row's mask word.  Up to four items in flight per thread.
+        for (uint32_t i = tid; i < rows * MW; i += nthr) occA[i] = 0u;
+        const uint32_t q4 = X / 4, nq = rows * q4;
+        constexpr int U = W >= 4 ? 1 : 4 / W;
+        __syncthreads();
+        for (uint32_t i0 = tid; i0 < nq; i0 += U * nthr) {
+            uint4 v[U][W];
+            uint32_t rr[U], cc[U];
 #pragma unroll
-            for (int k = 0; k < W; k++) A[(size_t)k * R + l] = __ldg(src + (size_t)k * g.N + gi);
-            T[l] = __ldg(sites + gi);
+            for (int u = 0; u < U; u++) {
+                const uint32_t i = i0 + u * nthr;
+                rr[u] = ~0u;
+                if (i < nq) {
+                    const uint32_t r = i / q4, c = i - r * q4;
+                    rr[u] = r;
+                    cc[u] = c;
+#pragma unroll
+                    for (int k = 0; k < W; k++) v[u][k] = __ldg((const uint4 *)(src + (size_t)k * g.N + rowbase[r]) + c);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (rr[u] == ~0u) continue;
+                const uint32_t r = rr[u], x = 4 * cc[u];
+                uint4 o = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+                for (int k = 0; k < W; k++) {
+                    *(uint4 *)(A + k * R + r * X + x) = v[u][k];
+                    o.x |= v[u][k].x;
+                    o.y |= v[u][k].y;
+                    o.z |= v[u][k].z;
+                    o.w |= v[u][k].w;
+                }
+                const uint32_t bits = (o.x ? 1u : 0u) | (o.y ? 2u : 0u) | (o.z ? 4u : 0u) | (o.w ? 8u : 0u);
+                if (bits) atomicOr(&occA[r * MW + (x >> 5)], bits << (x & 31u));
+            }
         }
-    }
-    __syncthreads();
-
-    // x sweep of every loaded row: A -> B.
-    {
-        const unsigned long long th = timestep_hash(seed, step, 0);
+        const uint32_t q16 = X / 16, nt = rows * q16;
+        for (uint32_t i = tid; i < nt; i += nthr) {
+            const uint32_t r = i / q16, c = i - r * q16;
+            *((uint4 *)(T + r * X) + c) = __ldg((const uint4 *)(sites + rowbase[r]) + c);
+        }
+    } else {
+        // Rows not 16-byte aligned: one word per thread.
         for (uint32_t r = ty; r < rows; r += by) {
-            const uint32_t ly = r % Ry, lz = r / Ry;
-            const bool owned_row = ly >= 1 && ly <= Ty && lz >= 1 && lz <= Tz;
-            const uint32_t gbase = GY(ly) * X + GZ(lz) * g.XY;
-            for (uint32_t x = tx; x < X; x += bx) {
-                const uint32_t xm = x == 0 ? X - 1 : x - 1, xp = x == X - 1 ? 0 : x + 1;
-                const uint32_t l = r * X + x, lm = r * X + xm, lp = r * X + xp;
-                SiteWords<BPS, S> own, mn, pl;
-                load_smem<BPS, S>(A, R, l, own);
-                load_smem<BPS, S>(A, R, lm, mn);
-                load_smem<BPS, S>(A, R, lp, pl);
-                if (!(own.empty() && mn.empty() && pl.empty()))
-                    own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], gbase + x, gbase + xm, gbase + xp, th,
-                                             m, owned_row, 1u, rs, list, cap);
-                store_smem<BPS, S>(B, R, l, own);
+            const uint32_t gbase = rowbase[r];
+            for (uint32_t xb = 0; xb < X; xb += bx) {
+                const uint32_t x = xb + tx;
+                bool occ = false;
+                if (x < X) {
+                    const uint32_t l = r * X + x, gi = gbase + x;
+                    uint32_t o = 0;
+#pragma unroll
+                    for (int k = 0; k < W; k++) {
+                        const uint32_t v = __ldg(src + (size_t)k * g.N + gi);
+                        A[k * R + l] = v;
+                        o |= v;
+                    }
+                    T[l] = __ldg(sites + gi);
+                    occ = o != 0;
+                }
+                const uint32_t mask = __ballot_sync(0xffffffffu, occ);
+                if ((tx & 31u) == 0 && (x >> 5) < MW) occA[r * MW + (x >> 5)] = mask;
             }
         }
     }
     __syncthreads();
 
-    // y sweep of the owned y rows of every loaded z plane: B -> A.
-    {
-        const unsigned long long th = timestep_hash(seed, step, 1);
-        const uint32_t yrows = Ty * ts.Rz;
-        for (uint32_t q = ty; q < yrows; q += by) {
-            const uint32_t ly = 1 + q % Ty, lz = q / Ty;
-            const uint32_t r = lz * Ry + ly;
-            const bool owned_row = lz >= 1 && lz <= Tz;
-            const uint32_t gz = GZ(lz) * g.XY;
-            const uint32_t gb = GY(ly) * X + gz, gbm = GY(ly - 1) * X + gz, gbp = GY(ly + 1) * X + gz;
-            for (uint32_t x = tx; x < X; x += bx) {
-                const uint32_t l = r * X + x, lm = l - X, lp = l + X;
-                SiteWords<BPS, S> own, mn, pl;
-                load_smem<BPS, S>(B, R, l, own);
-                load_smem<BPS, S>(B, R, lm, mn);
-                load_smem<BPS, S>(B, R, lp, pl);
-                if (!(own.empty() && mn.empty() && pl.empty()))
-                    own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], gb + x, gbm + x, gbp + x, th, m,
-                                             owned_row, 2u, rs, list, cap);
-                store_smem<BPS, S>(A, R, l, own);
-            }
-        }
-    }
-    __syncthreads();
+    uint32_t *src_w = A, *dst_w = B, *src_o = occA, *dst_o = occB;
+#pragma unroll 1
+    for (int phase = 0; phase < 3; phase++) {
+        const unsigned long long th = timestep_hash(seed, step, (uint32_t)phase);
+        const uint16_t *orow = phase == 0 ? nullptr : (phase == 1 ? yrow : zrow);
+        const uint32_t nout = phase == 0 ? rows : (phase == 1 ? yrows : orows);
+        const uint32_t d = phase == 1 ? 1u : Ry;  // row step of the y / z neighbours
+        uint32_t *cnt = &s_cnt[phase];
 
-    // z sweep of the owned rows (A), then the reaction in registers, then the
-    // single write of the owned rows.
-    {
-        const unsigned long long thz = timestep_hash(seed, step, 2);
-        const unsigned long long thr = timestep_hash(seed, step, 3);
-        const uint32_t orows = Ty * Tz;
-        for (uint32_t q = ty; q < orows; q += by) {
-            const uint32_t ly = 1 + q % Ty, lz = 1 + q / Ty;
-            const uint32_t r = lz * Ry + ly;
-            const uint32_t gyx = GY(ly) * X;
-            const uint32_t gb = gyx + GZ(lz) * g.XY, gbm = gyx + GZ(lz - 1) * g.XY, gbp = gyx + GZ(lz + 1) * g.XY;
-            const uint32_t RX = Ry * X;
-            for (uint32_t x = tx; x < X; x += bx) {
-                const uint32_t l = r * X + x, lm = l - RX, lp = l + RX;
-                SiteWords<BPS, S> own, mn, pl;
-                load_smem<BPS, S>(A, R, l, own);
-                load_smem<BPS, S>(A, R, lm, mn);
-                load_smem<BPS, S>(A, R, lp, pl);
-                if (!(own.empty() && mn.empty() && pl.empty()))
-                    own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], gb + x, gbm + x, gbp + x, thz, m,
-                                             true, 3u, rs, list, cap);
-                if (with_reaction) react_site<BPS, S>(own, T[l], gb + x, thr, m, rs, list, cap);
-                own.store(dst, g.N, gb + x);
+        // 1. Active outputs: occupied or next to an occupied site on the axis.
+        for (uint32_t i0 = 0; i0 < nout * MW; i0 += nthr) {
+            const uint32_t i = i0 + tid;
+            uint32_t a = 0, r = 0, w = 0;
+            if (i < nout * MW) {
+                const uint32_t q = i / MW;
+                w = i - q * MW;
+                r = orow ? orow[q] : q;
+                if (phase == 0) a = x_neighbourhood(src_o + r * MW, w, MW, X);
+                else a = src_o[r * MW + w] | src_o[(r - d) * MW + w] | src_o[(r + d) * MW + w];
+                dst_o[r * MW + w] = 0u;
+            }
+            warp_append(a, r, w, work, cnt);
+        }
+        __syncthreads();
+
+        // 2. The sweep rule for each active output.
+        const uint32_t nact = *cnt;
+        for (uint32_t j = tid; j < nact; j += nthr) {
+            const uint32_t e = work[j], r = e >> 16, x = e & 0xFFFFu, l = r * X + x;
+            uint32_t rm = r, rp = r, xm = x, xp = x;
+            if (phase == 0) {
+                xm = x == 0 ? X - 1 : x - 1;
+                xp = x == X - 1 ? 0 : x + 1;
+            } else {
+                rm = r - d;
+                rp = r + d;
+            }
+            const uint32_t lm = rm * X + xm, lp = rp * X + xp;
+            SiteWords<BPS, S> own, mn, pl;
+            own.clear();
+            mn.clear();
+            pl.clear();
+            if ((src_o[r * MW + (x >> 5)] >> (x & 31u)) & 1u) load_smem<BPS, S>(src_w, R, l, own);
+            if ((src_o[rm * MW + (xm >> 5)] >> (xm & 31u)) & 1u) load_smem<BPS, S>(src_w, R, lm, mn);
+            if ((src_o[rp * MW + (xp >> 5)] >> (xp & 31u)) & 1u) load_smem<BPS, S>(src_w, R, lp, pl);
+            const bool record = phase == 2 || (rowflag[r] & ROW_OWNED);
+            own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], rowbase[r] + x, rowbase[rm] + xm,
+                                     rowbase[rp] + xp, th, mt, record, (uint32_t)phase + 1, rs, list, cap);
+            if (!own.empty()) {
+                store_smem<BPS, S>(dst_w, R, l, own);
+                atomicOr(&dst_o[r * MW + (x >> 5)], 1u << (x & 31u));
             }
         }
+        __syncthreads();
+        uint32_t *t0 = src_w;
+        src_w = dst_w;
+        dst_w = t0;
+        t0 = src_o;
+        src_o = dst_o;
+        dst_o = t0;
     }
-#undef GY
-#undef GZ
+    // After three sweeps the owned rows are in src_w / src_o.
+
+    // Reaction on the owned sites that can react: the occupied ones, or every
+    // site when the model has zeroth-order reactions.
+    if (with_reaction) {
+        const unsigned long long th = timestep_hash(seed, step, 3);
+        bool zeroth = false;
+        for (uint32_t t = 0; t < mt.nst; t++) zeroth |= mt.qp0[t] != 0.0f;
+        for (uint32_t i0 = 0; i0 < orows * MW; i0 += nthr) {
+            const uint32_t i = i0 + tid;
+            uint32_t a = 0, r = 0, w = 0;
+            if (i < orows * MW) {
+                const uint32_t q = i / MW;
+                w = i - q * MW;
+                r = zrow[q];
+                const uint32_t all = (w + 1 < MW || !(X & 31u)) ? 0xffffffffu : ((1u << (X & 31u)) - 1u);
+                a = zeroth ? all : src_o[r * MW + w];
+            }
+            warp_append(a, r, w, work, &s_cnt[3]);
+        }
+        __syncthreads();
+        const uint32_t n = s_cnt[3];
+        for (uint32_t j = tid; j < n; j += nthr) {
+            const uint32_t e = work[j], r = e >> 16, x = e & 0xFFFFu, l = r * X + x;
+            const bool occ = (src_o[r * MW + (x >> 5)] >> (x & 31u)) & 1u;
+            SiteWords<BPS, S> s;
+            s.clear();
+            if (occ) load_smem<BPS, S>(src_w, R, l, s);
+            else if (mt.qp0[T[l]] == 0.0f) continue;
+            s = react_site_ool<BPS, S>(s, T[l], rowbase[r] + x, th, mt, rs, list, cap);
+            store_smem<BPS, S>(src_w, R, l, s);
+            if (s.empty()) atomicAnd(&src_o[r * MW + (x >> 5)], ~(1u << (x & 31u)));
+            else atomicOr(&src_o[r * MW + (x >> 5)], 1u << (x & 31u));
+        }
+        __syncthreads();
+    }
+
+    // Dense write of the owned rows (empty sites as zeros).
+    if (ts.vec) {
+        // Four sites per thread: a 16-byte store per word plane.
+        const uint32_t q4 = X / 4, n4 = orows * q4;
+        for (uint32_t i = tid; i < n4; i += nthr) {
+            const uint32_t q = i / q4, c = i - q * q4, r = zrow[q], x = 4 * c;
+            const uint32_t bits = (src_o[r * MW + (x >> 5)] >> (x & 31u)) & 0xFu;
+#pragma unroll
+            for (int k = 0; k < W; k++) {
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (bits) {
+                    const uint32_t *a = src_w + k * R + r * X + x;
+                    v.x = (bits & 1u) ? a[0] : 0u;
+                    v.y = (bits & 2u) ? a[1] : 0u;
+                    v.z = (bits & 4u) ? a[2] : 0u;
+                    v.w = (bits & 8u) ? a[3] : 0u;
+                }
+                *((uint4 *)(dst + (size_t)k * g.N + rowbase[r]) + c) = v;
+            }
+        }
+    } else
+    for (uint32_t q = ty; q < orows; q += by) {
+        const uint32_t r = zrow[q];
+        const uint32_t gb = rowbase[r];
+        for (uint32_t x = tx; x < X; x += bx) {
+            SiteWords<BPS, S> s;
+            s.clear();
+            if ((src_o[r * MW + (x >> 5)] >> (x & 31u)) & 1u) load_smem<BPS, S>(src_w, R, r * X + x, s);
+            s.store(dst, g.N, gb + x);
+        }
+    }
 
     // The last block to finish resolves the overflow queue and advances the
     // step counter.
     __syncthreads();
-    if (tx == 0 && ty == 0) {
+    if (tid == 0) {
         __threadfence();
         const uint32_t prev = atomicAdd(&rs->tiles_done, 1u);
         s_last = prev == gridDim.x - 1;
@@ -169,9 +398,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_
     __syncthreads();
     if (s_last) {
         __threadfence();
-        if (tx == 0 && ty == 0) rs->tiles_done = 0;
-        // Flatten the 2-D block for the shared resolver.
-        resolve_block_flat<BPS, S>(dst, sites, g, rs, list, cap, (OverflowEntry *)smem, tx + ty * bx, bx * by);
+        if (tid == 0) rs->tiles_done = 0;
+        resolve_block_flat<BPS, S>(dst, sites, g, rs, list, cap, (OverflowEntry *)smem, tid, nthr);
     }
 }
 
@@ -181,23 +409,24 @@ __global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_
 
 static size_t region_bytes(uint32_t X, uint32_t Ty, uint32_t Tz, uint32_t W)
 {
-    const size_t R = (size_t)X * (Ty + 2) * (Tz + 2);
-    return ((2 * (size_t)W * R * 4 + R) + 15) & ~(size_t)15;
+    const size_t rows = (size_t)(Ty + 2) * (Tz + 2), R = (size_t)X * rows, MW = (X + 31) / 32;
+    return 2 * (size_t)W * R * 4 + R * 4 + ((R + 15) & ~(size_t)15) + 2 * rows * MW * 4;
 }
 
-size_t fused_smem_bytes(const TileShape &ts, uint32_t X, uint32_t W, uint32_t cap)
+size_t fused_smem_bytes(const TileShape &ts, uint32_t X, uint32_t W, uint32_t cap, uint32_t stage_bytes)
 {
-    const size_t tile = region_bytes(X, ts.Ty, ts.Tz, W);
+    const size_t tile = region_bytes(X, ts.Ty, ts.Tz, W) + stage_bytes;
     const size_t sort = (size_t)pow2_at_least(cap) * sizeof(OverflowEntry);
     return tile > sort ? tile : sort;
 }
 
 bool fused_make_shape(const Geometry &g, int bps, int slots, uint32_t Ty, uint32_t Tz, TileShape &ts)
 {
-    if (!slots_supported(bps, slots)) return false;
+    if (!slots_supported(bps, slots) || slots > 16) return false;  // 2-bit codes of 16 slots per word
     if (Ty == 0 || Tz == 0 || Ty > g.Y || Tz > g.Z || g.Y % Ty || g.Z % Tz) return false;
     const uint32_t W = bps == 1 ? slots / 4 : slots;
     if (g.X > 1024) return false;
+    if ((Ty + 2) * (Tz + 2) > FUSED_MAX_ROWS) return false;
     if (region_bytes(g.X, Ty, Tz, W) > FUSED_MAX_SMEM) return false;
     ts.Ty = Ty;
     ts.Tz = Tz;
@@ -206,6 +435,9 @@ bool fused_make_shape(const Geometry &g, int bps, int slots, uint32_t Ty, uint32
     ts.tiles_y = g.Y / Ty;
     ts.tiles_z = g.Z / Tz;
     ts.R = g.X * ts.Ry * ts.Rz;
+    ts.MW = (g.X + 31) / 32;
+    // 16-byte row loads need 16-byte aligned rows: X words and X type bytes.
+    ts.vec = (g.X % 16u) == 0;
     uint32_t bx = ((g.X + 31) / 32) * 32;
     if (bx > 128) bx = 128;
     ts.bx = bx;
@@ -238,12 +470,30 @@ bool fused_default_shape(const Geometry &g, int bps, int slots, TileShape &ts)
     return found;
 }
 
-#define FUSED_DISPATCH(BPS_, S_)                                                                                   \
-    if (bps == BPS_ && slots == S_) {                                                                              \
-        auto kern = fused_step_kernel<BPS_, S_>;                                                                   \
-        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        kern<<<grid, block, smem, stream>>>(src, dst, sites, g, m, rs, list, cap, ts, with_reaction);             \
-        return cudaGetLastError();                                                                                 \
+// The dynamic shared-memory limit is raised once per instantiation (per
+// device) to the largest size any launch needs; setting it on every launch
+// costs host time comparable to the kernel itself.
+template <int BPS, int S>
+static cudaError_t ensure_smem_limit(size_t smem)
+{
+    static size_t granted[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (smem <= 48 * 1024 || smem <= granted[dev]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(fused_step_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess) granted[dev] = smem;
+    return e;
+}
+
+#define FUSED_DISPATCH(BPS_, S_)                                                                       \
+    if (bps == BPS_ && slots == S_) {                                                                  \
+        cudaError_t e = ensure_smem_limit<BPS_, S_>(smem);                                             \
+        if (e != cudaSuccess) return e;                                                                \
+        fused_step_kernel<BPS_, S_><<<grid, block, smem, stream>>>(src, dst, sites, g, m, rs, list, cap, ts, \
+                                                                   with_reaction);                     \
+        return cudaGetLastError();                                                                     \
     }
 
 cudaError_t launch_fused(int bps, int slots, const uint32_t *src, uint32_t *dst, const uint8_t *sites,
@@ -251,13 +501,12 @@ cudaError_t launch_fused(int bps, int slots, const uint32_t *src, uint32_t *dst,
                          const TileShape &ts, int with_reaction, cudaStream_t stream)
 {
     const uint32_t W = bps == 1 ? slots / 4 : slots;
-    const size_t smem = fused_smem_bytes(ts, g.X, W, cap);
+    const size_t smem = fused_smem_bytes(ts, g.X, W, cap, m.stage_bytes);
     const dim3 grid(ts.tiles_y * ts.tiles_z), block(ts.bx, ts.by);
     count_launch();
     FUSED_DISPATCH(1, 4)
     FUSED_DISPATCH(1, 8)
     FUSED_DISPATCH(1, 16)
-    FUSED_DISPATCH(1, 32)
     FUSED_DISPATCH(4, 4)
     FUSED_DISPATCH(4, 8)
     FUSED_DISPATCH(4, 16)

@@ -12,6 +12,7 @@ namespace lmb {
 constexpr int FUSED_THREADS = 256;
 constexpr size_t FUSED_MAX_SMEM = 200 * 1024;       // per block, below the 227 KB limit
 constexpr size_t FUSED_PREFERRED_SMEM = 100 * 1024; // default plan: two blocks per SM
+constexpr uint32_t FUSED_MAX_ROWS = 324;            // (Ty + 2) * (Tz + 2), up to 16 x 16 tiles
 
 // A block owns Ty x Tz full x-rows; its region adds one halo row on each side
 // in y and z: R = X * (Ty + 2) * (Tz + 2) sites.
@@ -20,12 +21,14 @@ struct TileShape {
     uint32_t Ry, Rz;
     uint32_t tiles_y, tiles_z;
     uint32_t R;
+    uint32_t MW;  // 32-bit occupancy mask words per row
+    uint32_t vec;  // region rows are 16-byte aligned: load them with 16-byte accesses
     uint32_t bx, by;
 };
 
 bool fused_make_shape(const Geometry &g, int bytes_per_slot, int slots, uint32_t Ty, uint32_t Tz, TileShape &ts);
 bool fused_default_shape(const Geometry &g, int bytes_per_slot, int slots, TileShape &ts);
-size_t fused_smem_bytes(const TileShape &ts, uint32_t X, uint32_t W, uint32_t cap);
+size_t fused_smem_bytes(const TileShape &ts, uint32_t X, uint32_t W, uint32_t cap, uint32_t stage_bytes);
 cudaError_t launch_fused(int bytes_per_slot, int slots, const uint32_t *src, uint32_t *dst, const uint8_t *sites,
                          const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
                          const TileShape &ts, int with_reaction, cudaStream_t stream);

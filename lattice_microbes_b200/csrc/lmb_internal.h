@@ -27,6 +27,8 @@ struct DevTables {
     const uint32_t *stoich_off;  // [nr+1]
     const uint32_t *stoich_sp;   // 0-based species
     const int32_t *stoich_d;     // stoichiometric change
+    uint32_t nnz;                // entries of the sparse stoichiometry
+    uint32_t stage_bytes;        // shared-memory copy size of all tables, 0 if too large to stage
 };
 
 // One queued overflow: the sort key orders entries by (phase, site, seq);

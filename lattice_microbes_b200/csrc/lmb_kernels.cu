@@ -302,8 +302,13 @@ cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sit
     const size_t smem = (size_t)pow2 * sizeof(OverflowEntry);
     count_launch();
     LMB_DISPATCH_ALL({
-        if (smem > 48 * 1024)
+        static bool raised[64] = {false};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (smem > 48 * 1024 && dev >= 0 && dev < 64 && !raised[dev]) {
             cudaFuncSetAttribute(resolve_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            raised[dev] = true;
+        }
         resolve_kernel<BPS, S><<<1, RESOLVE_THREADS, smem, stream>>>(lat, sites, g, rs, list, cap);
     })
 }

@@ -89,8 +89,8 @@ template <int BPS, int S>
 __device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_t t, const SiteWords<BPS, S> &s,
                                                      uint32_t rx)
 {
-    if (!__ldg(m.RL + (size_t)rx * m.nst + t)) return 0.0f;
-    const uint32_t d1 = __ldg(m.D1 + rx), d2 = __ldg(m.D2 + rx);
+    if (!tload(m.RL + (size_t)rx * m.nst + t)) return 0.0f;
+    const uint32_t d1 = tload(m.D1 + rx), d2 = tload(m.D2 + rx);
     float n1 = 0.0f, n2 = 0.0f;
 #pragma unroll
     for (int k = 0; k < S; k++) {
@@ -100,8 +100,8 @@ __device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_
             n2 = __fadd_rn(n2, p == d2 ? 1.0f : 0.0f);
         }
     }
-    const float rate = __ldg(m.rate + rx);
-    switch (__ldg(m.order + rx)) {
+    const float rate = tload(m.rate + rx);
+    switch (tload(m.order + rx)) {
     case 1: return rate;
     case 2: return __fmul_rn(rate, n1);
     case 3: return __fmul_rn(__fmul_rn(rate, n1), n2);
@@ -118,18 +118,18 @@ template <int BPS, int S>
 __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uint32_t gi, unsigned long long th,
                                            const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap)
 {
-    float a = __ldg(m.qp0 + t);
+    float a = tload(m.qp0 + t);
     if (s.empty() && a == 0.0f) return false;
     const size_t o1 = (size_t)t * m.ns, o2 = (size_t)t * m.ns * m.ns;
 #pragma unroll
     for (int k = 0; k < S; k++) {
         const uint32_t p1 = s.slot(k);
         if (p1 > 0) {
-            a = __fadd_rn(a, __ldg(m.qp1 + o1 + (p1 - 1)));
+            a = __fadd_rn(a, tload(m.qp1 + o1 + (p1 - 1)));
 #pragma unroll
             for (int j = k + 1; j < S; j++) {
                 const uint32_t p2 = s.slot(j);
-                if (p2 > 0) a = __fadd_rn(a, __ldg(m.qp2 + o2 + (size_t)(p1 - 1) * m.ns + (p2 - 1)));
+                if (p2 > 0) a = __fadd_rn(a, tload(m.qp2 + o2 + (size_t)(p1 - 1) * m.ns + (p2 - 1)));
             }
         }
     }
@@ -150,13 +150,13 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
     atomicAdd(&rs->reactions, 1ull);
 
     // Stoichiometry of the chosen reaction, ascending species.
-    const uint32_t e0 = __ldg(m.stoich_off + idx), e1 = __ldg(m.stoich_off + idx + 1);
+    const uint32_t e0 = tload(m.stoich_off + idx), e1 = tload(m.stoich_off + idx + 1);
     const int ne = (int)(e1 - e0) < MAX_STOICH ? (int)(e1 - e0) : MAX_STOICH;
     uint32_t sp[MAX_STOICH];
     int dlt[MAX_STOICH];
     for (int e = 0; e < ne; e++) {
-        sp[e] = __ldg(m.stoich_sp + e0 + e);
-        dlt[e] = __ldg(m.stoich_d + e0 + e);
+        sp[e] = tload(m.stoich_sp + e0 + e);
+        dlt[e] = tload(m.stoich_d + e0 + e);
     }
     // Survivors in slot order; a consumed reactant bumps its count.
     SiteWords<BPS, S> out;
