@@ -26,11 +26,25 @@ static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches += n; }
 }  // namespace lmb
 
+// A context lives until its handle and every model and lattice made from it
+// are destroyed, whatever the order of those calls.
 struct lmb_ctx {
     int device;
     cudaStream_t stream;
     bool own_stream;
+    std::atomic<int> refs;
 };
+
+static void ctx_retain(lmb_ctx *c) { c->refs.fetch_add(1); }
+
+static void ctx_release(lmb_ctx *c)
+{
+    if (c->refs.fetch_sub(1) == 1) {
+        cudaSetDevice(c->device);
+        if (c->own_stream) cudaStreamDestroy(c->stream);
+        delete c;
+    }
+}
 
 struct lmb_model {
     lmb_ctx *ctx;
@@ -148,6 +162,7 @@ extern "C" int lmb_ctx_create_on_stream(int device, void *stream, lmb_ctx **out)
     lmb_ctx *c = new (std::nothrow) lmb_ctx;
     if (!c) return LMB_E_NOMEM;
     c->device = device;
+    c->refs.store(1);
     c->own_stream = stream == nullptr;
     if (stream) c->stream = (cudaStream_t)stream;
     else {
@@ -166,9 +181,7 @@ extern "C" int lmb_ctx_create(int device, lmb_ctx **out) { return lmb_ctx_create
 extern "C" int lmb_ctx_destroy(lmb_ctx *c)
 {
     if (!c) return LMB_E_ARG;
-    cudaSetDevice(c->device);
-    if (c->own_stream) cudaStreamDestroy(c->stream);
-    delete c;
+    ctx_release(c);
     return LMB_OK;
 }
 
@@ -318,12 +331,14 @@ static int build_stoich(lmb_model *m)
 extern "C" int lmb_model_get_tables(const lmb_model *m, float *T, float *qp0, float *qp1, float *qp2,
                                     uint32_t *order, uint32_t *D1, uint32_t *D2, float *rate, int8_t *S,
                                     uint8_t *RL);
+static void free_model(lmb_model *m);
 
 static lmb_model *new_model(lmb_ctx *c, uint32_t ns, uint32_t nst, uint32_t nr)
 {
     lmb_model *m = new (std::nothrow) lmb_model;
     if (!m) return nullptr;
     m->ctx = c;
+    if (c) ctx_retain(c);
     m->ns = ns;
     m->nst = nst;
     m->nr = nr;
@@ -419,8 +434,7 @@ extern "C" int lmb_model_create(lmb_ctx *c, const lmb_model_desc *d, uint32_t X,
     rc = build_model_host(d, X, Y, Z, m);
     if (rc == LMB_OK) rc = upload_model(m);
     if (rc != LMB_OK) {
-        if (m->dev_block) cudaFree(m->dev_block);
-        delete m;
+        free_model(m);
         return rc;
     }
     *out = m;
@@ -437,7 +451,7 @@ extern "C" int lmb_tables_build(const lmb_model_desc *d, uint32_t X, uint32_t Y,
     if (!m) return LMB_E_NOMEM;
     rc = build_model_host(d, X, Y, Z, m);
     if (rc == LMB_OK) rc = lmb_model_get_tables(m, T, qp0, qp1, qp2, order, D1, D2, rate, S, RL);
-    delete m;
+    free_model(m);
     return rc;
 }
 
@@ -465,14 +479,13 @@ extern "C" int lmb_model_create_from_tables(lmb_ctx *c, const lmb_tables *t, lmb
     }
     for (float q : m->T)
         if (q > 0.50f) {
-            delete m;
+            free_model(m);
             return LMB_E_MODEL;
         }
     int rc = build_stoich(m);
     if (rc == LMB_OK) rc = upload_model(m);
     if (rc != LMB_OK) {
-        if (m->dev_block) cudaFree(m->dev_block);
-        delete m;
+        free_model(m);
         return rc;
     }
     *out = m;
@@ -507,15 +520,21 @@ extern "C" int lmb_model_set_reaction_rate(lmb_model *m, uint32_t reaction, doub
     return LMB_OK;
 }
 
-extern "C" int lmb_model_destroy(lmb_model *m)
+static void free_model(lmb_model *m)
 {
-    if (!m) return LMB_E_ARG;
-    if (m->dev_block) {
+    if (m->dev_block && m->ctx) {
         cudaSetDevice(m->ctx->device);
         cudaStreamSynchronize(m->ctx->stream);
         cudaFree(m->dev_block);
     }
+    if (m->ctx) ctx_release(m->ctx);
     delete m;
+}
+
+extern "C" int lmb_model_destroy(lmb_model *m)
+{
+    if (!m) return LMB_E_ARG;
+    free_model(m);
     return LMB_OK;
 }
 
@@ -536,8 +555,9 @@ extern "C" int lmb_lattice_create(lmb_ctx *c, uint32_t X, uint32_t Y, uint32_t Z
     CK(cudaSetDevice(c->device));
     lmb_lattice *l = new (std::nothrow) lmb_lattice;
     if (!l) return LMB_E_NOMEM;
-    memset(l, 0, sizeof(*l));
+    memset((void *)l, 0, sizeof(*l));
     l->ctx = c;
+    ctx_retain(c);
     l->g.X = X;
     l->g.Y = Y;
     l->g.Z = Z;
@@ -610,7 +630,9 @@ extern "C" int lmb_lattice_destroy(lmb_lattice *l)
     if (l->rs_host) cudaFreeHost(l->rs_host);
     for (auto &gr : l->graph)
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
+    lmb_ctx *c = l->ctx;
     delete l;
+    ctx_release(c);
     return LMB_OK;
 }
 

@@ -264,7 +264,7 @@ def test_invalid_species_rejected(ctx):
 def test_graph_replay_long_run_vs_oracle(ctx, schedule):
     """Runs long enough to replay captured timestep graphs (and a remainder
     launched directly), in two calls that start at different buffer parities."""
-    spec = configs.random_problem(21, X=32, Y=16, Z=16, density=0.9, nst=2)
+    spec = configs.config0(seed=3, nA=40000, nB=40000)  # dense: thousands of overflows
     t = oracle_tables(spec)
     ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 31337, 0, 141)
     out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 31337, 0, 141, chunks=[73, 68], schedule=schedule)
