@@ -184,6 +184,24 @@ int lmb_lattice_device_buffers(lmb_lattice *lattice, void **particles, void **si
  * device: counts[s] for s = 0..number_species (counts[0] is 0). */
 int lmb_lattice_species_counts(lmb_lattice *lattice, uint32_t number_species, uint64_t *counts);
 
+/* Species counts for callers that cannot allocate device memory (a host
+ * program whose own pool allocator owns the device memory, a hook or
+ * callback where cudaMalloc would synchronize or exceed a memory cap, a
+ * serving loop with a fixed footprint).  No counterpart in the reference: it
+ * has no device-side count at all.  `particles` is a native lattice in
+ * device memory; `counts` (host, number_species + 1 entries) receives the
+ * totals as lmb_lattice_species_counts gives them.  The device-side totals
+ * live in one fixed 32 KiB array per device that stays allocated until the
+ * process exits; sizes above LMB_NOALLOC_MAX_SPECIES species return
+ * LMB_E_UNSUPPORTED.  The first call on a device looks up that array's
+ * address, so make it before any stream capture.  Each call clears the array
+ * on `cuda_stream` before counting and waits for the result; calls whose
+ * work overlaps on the GPU share the array and race. */
+#define LMB_NOALLOC_MAX_SPECIES 4095
+int lmb_species_counts_noalloc(const uint32_t *particles, uint32_t X, uint32_t Y, uint32_t Z,
+                               uint32_t particles_per_site, uint32_t bytes_per_particle, uint32_t number_species,
+                               uint64_t *counts, void *cuda_stream);
+
 /* ---- timesteps -----------------------------------------------------------
  * number_timesteps calls of MpdRdmeSolver::runTimestep (MpdRdmeSolver.cu:
  * 996-1193), timestep indices first_timestep.., with `seed` the composed

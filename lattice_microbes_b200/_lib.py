@@ -23,6 +23,8 @@ LMB_E_UNSUPPORTED = -9
 LMB_OVERFLOW_CLASSIC = 0
 LMB_OVERFLOW_RELAXED = 1
 
+LMB_NOALLOC_MAX_SPECIES = 4095
+
 LMB_SCHEDULE_FUSED = 0
 LMB_SCHEDULE_PHASES = 1
 
@@ -93,6 +95,8 @@ PROTOTYPES = {
                                        f32p]),
     "lmb_lattice_device_buffers": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp)]),
     "lmb_lattice_species_counts": (C.c_int, [vp, C.c_uint32, u64p]),
+    "lmb_species_counts_noalloc": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                             C.c_uint32, u64p, vp]),
     "lmb_run": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(RunStats)]),
     "lmb_run_async": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int]),
     "lmb_run_wait": (C.c_int, [vp, C.POINTER(RunStats)]),
