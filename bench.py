@@ -49,6 +49,8 @@ def parse():
                     help="timesteps per core in the CPU baseline sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
     return ap.parse_args()
 
@@ -215,7 +217,7 @@ def run_ours(a):
     # The reference's own kernels (compiled for sm_100a from its sources) on
     # this GPU, with its per-timestep host flow: the GPU bar to beat.
     ref_gpu = None
-    if rank == 0:
+    if rank == 0 and not a.no_reference_gpu:
         try:
             from tests.cases import oracle_tables
             from tests.oracle_lib import reference_gpu_time
