@@ -164,11 +164,11 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_sweep():
-    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+def ncu_traffic_per_launch(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        return d.get("sweep_dram_bytes_per_launch")
+        return d.get("kernel_dram_bytes_per_launch") if d.get("kernel", "").startswith(kernel) else None
     except Exception:
         return None
 
@@ -351,7 +351,7 @@ def run_ours(a):
                 "peak": peak,
                 "unit": "GB/s",
                 "frac": achieved / peak,
-                "traffic": ncu_traffic_per_sweep(),
+                "traffic": ncu_traffic_per_launch("fused_step_kernel" if phase_n[5] > 0 else "sweep_kernel"),
                 "kernel": kern,
                 "ms_per_launch": launch_ms,
                 "algorithmic_bytes_per_launch": alg_bytes,
