@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
+    ap.add_argument("--workload", choices=["rodcell", "batch"], default="rodcell",
+                    help="rodcell: one 64x64x128 lattice (default); batch: 256 bimolecular replicates of "
+                         "uneven size in one launch per timestep")
+    ap.add_argument("--replicates", type=int, default=256)
     return ap.parse_args()
 
 
@@ -425,9 +429,111 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(a):
+    """Batched replicates: config-0 chemistry (A + B <-> C, 32 nm, tau = 50 us)
+    on cubic lattices with edges drawn from {16, 24, 32, 48, 64}, all advanced
+    by one launch per timestep.  Metric: replicates/s, a replicate being one
+    10,000-timestep trajectory.  Compared with the plain solver running the
+    same replicates one after another (each lattice alone, graph replay)."""
+    import numpy as np
+    import torch
+
+    from lattice_microbes_b200 import configs
+    from lattice_microbes_b200.solver import Batch, Context, Lattice, Model, compose_seed, kernel_launches
+
+    torch.cuda.set_device(0)
+    T = a.timesteps_per_step if a.timesteps_per_step != TIMESTEPS_PER_STEP else 200
+    edges = configs.batch_edges(seed=7, count=a.replicates)
+    ctx = Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    lats, models, specs = [], [], []
+    for k, e in enumerate(edges):
+        spec = configs.config0(seed=k + 1, edge=e)
+        m = Model.from_spec(ctx, spec)
+        lat = Lattice(ctx, e, e, e, 8, 1)
+        lat.set_native(spec.lattice, spec.sites)
+        lats.append(lat)
+        models.append(m)
+        specs.append(spec)
+    seeds = [compose_seed(2024, k) for k in range(len(lats))]
+    sites_total = sum(e ** 3 for e in edges)
+    batch = Batch(ctx, lats, models)
+    step = 0
+    for _ in range(a.warmup):
+        batch.run(seeds, step, T)
+        step += T
+    times = []
+    launches0 = kernel_launches()
+    clocks = ClockSampler(0)
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for _ in range(a.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            batch.run_async(seeds, step, T)
+            e1.record(stream)
+            batch.wait()
+            times.append(e0.elapsed_time(e1))
+            step += T
+    clock_info = clocks.stop()
+    launches = kernel_launches() - launches0
+    ms_step = sum(times) / a.steps / T                       # per timestep, all replicates
+    rep_per_s = len(lats) / (10000 * ms_step / 1e3)
+
+    # Plain solver, one replicate at a time: per-timestep time of one lattice
+    # of each edge, summed over the replicates.
+    per_edge = {}
+    for e in sorted(set(edges)):
+        k = edges.index(e)
+        lat, m = lats[k], models[k]
+        lat.run(m, seeds[k], 0, 64)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            lat.run_async(m, seeds[k], 64, T)
+            e1.record(stream)
+            lat.wait()
+        per_edge[e] = e0.elapsed_time(e1) / T
+    seq_ms_step = sum(per_edge[e] for e in edges)
+    seq_rep_per_s = len(lats) / (10000 * seq_ms_step / 1e3)
+    line = {
+        "metric": "replicates/s",
+        "value": rep_per_s,
+        "unit": "replicates/s",
+        "n_gpus": 1,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": sum(times) / a.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (seeded bimolecular replicates, lattice_microbes_b200.configs.config0)",
+        "config": {"workload": "batch of %d bimolecular replicates, edges {16,24,32,48,64}, %d sites"
+                               % (len(lats), sites_total),
+                   "timesteps_per_step": T, "trajectory_timesteps": 10000},
+        "site_steps_per_s": sites_total / (ms_step / 1e3),
+        "sequential_plain": {"value": seq_rep_per_s, "unit": "replicates/s",
+                             "ms_per_timestep_by_edge": per_edge},
+        "speedup_vs_sequential": rep_per_s / seq_rep_per_s,
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for lat, m in zip(lats, models):
+        lat.close()
+        m.close()
+    ctx.close()
+
+
 if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)

@@ -223,6 +223,26 @@ int lmb_run_profiled(lmb_lattice *lattice, const lmb_model *model, uint32_t seed
                      uint32_t number_timesteps, int overflow_mode, float *phase_ms, uint32_t *phase_launches,
                      lmb_run_stats *stats);
 
+/* ---- batches ---------------------------------------------------------------
+ * Many lattices (replicates, uneven sizes) advanced together: one launch per
+ * timestep covers every tile of every lattice, replayed from a captured CUDA
+ * graph.  Replaces running the reference's ReplicateRunner threads
+ * (core/ReplicateRunner.cpp:84-166), one MpdRdmeSolver each, on one device.
+ * All lattices share the context, slot count and bytes per slot and use the
+ * fused schedule; each has its own model (rates scale with its site count)
+ * and its own seed.  Each lattice gives the same result as lmb_run on it. */
+typedef struct lmb_batch lmb_batch;
+int lmb_batch_create(lmb_ctx *ctx, uint32_t count, lmb_lattice *const *lattices, const lmb_model *const *models,
+                     lmb_batch **out);
+/* seeds[count]; stats[count] may be NULL.  Returns the first error of any
+ * lattice; the others still ran. */
+int lmb_batch_run(lmb_batch *batch, const uint32_t *seeds, uint32_t first_timestep, uint32_t number_timesteps,
+                  int overflow_mode, lmb_run_stats *stats);
+int lmb_batch_run_async(lmb_batch *batch, const uint32_t *seeds, uint32_t first_timestep,
+                        uint32_t number_timesteps, int overflow_mode);
+int lmb_batch_wait(lmb_batch *batch, lmb_run_stats *stats);
+int lmb_batch_destroy(lmb_batch *batch);
+
 /* Launch counters for the bench's kernel accounting. */
 uint64_t lmb_kernel_launches(void);
 

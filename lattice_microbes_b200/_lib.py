@@ -102,6 +102,11 @@ PROTOTYPES = {
     "lmb_run_wait": (C.c_int, [vp, C.POINTER(RunStats)]),
     "lmb_run_profiled": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, f32p, u32p,
                                    C.POINTER(RunStats)]),
+    "lmb_batch_create": (C.c_int, [vp, C.c_uint32, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    "lmb_batch_run": (C.c_int, [vp, u32p, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(RunStats)]),
+    "lmb_batch_run_async": (C.c_int, [vp, u32p, C.c_uint32, C.c_uint32, C.c_int]),
+    "lmb_batch_wait": (C.c_int, [vp, C.POINTER(RunStats)]),
+    "lmb_batch_destroy": (C.c_int, [vp]),
     "lmb_kernel_launches": (C.c_uint64, []),
 }
 

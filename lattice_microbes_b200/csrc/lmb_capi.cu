@@ -1083,3 +1083,240 @@ extern "C" int lmb_lattice_autotune(lmb_lattice *l, const lmb_model *m, uint32_t
     if (best_ms) *best_ms = best;
     return LMB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batches: many lattices advanced by one launch per timestep
+// ---------------------------------------------------------------------------
+
+struct lmb_batch {
+    lmb_ctx *ctx;
+    std::vector<lmb_lattice *> lats;
+    std::vector<const lmb_model *> models;
+    int bps, slots;
+    // Device side: job table, run-state pointers, seeds, gathered states.
+    FusedJob *jobs;
+    RunState **rs_ptrs;
+    uint32_t *seeds;
+    RunState *states;
+    RunState *states_host;  // pinned
+    std::vector<FusedJob> jobs_host;
+    uint32_t total_tiles;
+    size_t smem;
+    cudaGraphExec_t graph;
+    uint64_t graph_kernels;
+    uint32_t graph_tiles;  // launch shape the graph was captured with
+    size_t graph_smem;
+    bool pending;
+    uint32_t pending_first, pending_n;
+    std::vector<int> cur0;
+};
+
+static const uint32_t BATCH_GRAPH_STEPS = 32;
+
+extern "C" int lmb_batch_create(lmb_ctx *c, uint32_t count, lmb_lattice *const *lattices,
+                                const lmb_model *const *models, lmb_batch **out)
+{
+    if (!c || !lattices || !models || !out || count == 0) return LMB_E_ARG;
+    *out = nullptr;
+    const int bps = (int)lattices[0]->bps, slots = (int)lattices[0]->slots;
+    for (uint32_t j = 0; j < count; j++) {
+        lmb_lattice *l = lattices[j];
+        const lmb_model *m = models[j];
+        if (!l || !m || l->ctx != c || m->ctx != c) return LMB_E_ARG;
+        if ((int)l->bps != bps || (int)l->slots != slots) return LMB_E_ARG;
+        if (m->has_desc && (m->X != l->g.X || m->Y != l->g.Y || m->Z != l->g.Z)) return LMB_E_ARG;
+        if (l->schedule != LMB_SCHEDULE_FUSED) return LMB_E_UNSUPPORTED;
+    }
+    CK(cudaSetDevice(c->device));
+    lmb_batch *b = new (std::nothrow) lmb_batch;
+    if (!b) return LMB_E_NOMEM;
+    b->ctx = c;
+    ctx_retain(c);
+    b->lats.assign(lattices, lattices + count);
+    b->models.assign(models, models + count);
+    b->bps = bps;
+    b->slots = slots;
+    b->jobs = nullptr;
+    b->rs_ptrs = nullptr;
+    b->seeds = nullptr;
+    b->states = nullptr;
+    b->states_host = nullptr;
+    b->graph = nullptr;
+    b->graph_kernels = 0;
+    b->graph_tiles = 0;
+    b->graph_smem = 0;
+    b->pending = false;
+    b->total_tiles = 0;
+    b->smem = 0;
+    cudaError_t e = cudaMalloc(&b->jobs, sizeof(FusedJob) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->rs_ptrs, sizeof(RunState *) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->seeds, sizeof(uint32_t) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->states, sizeof(RunState) * count);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->states_host, sizeof(RunState) * count);
+    std::vector<RunState *> ptrs(count);
+    for (uint32_t j = 0; j < count; j++) ptrs[j] = lattices[j]->rs;
+    if (e == cudaSuccess) e = cudaMemcpy(b->rs_ptrs, ptrs.data(), sizeof(RunState *) * count, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        lmb_batch_destroy(b);
+        return cuda_status(e);
+    }
+    *out = b;
+    return LMB_OK;
+}
+
+extern "C" int lmb_batch_destroy(lmb_batch *b)
+{
+    if (!b) return LMB_E_ARG;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->jobs) cudaFree(b->jobs);
+    if (b->rs_ptrs) cudaFree(b->rs_ptrs);
+    if (b->seeds) cudaFree(b->seeds);
+    if (b->states) cudaFree(b->states);
+    if (b->states_host) cudaFreeHost(b->states_host);
+    lmb_ctx *c = b->ctx;
+    delete b;
+    ctx_release(c);
+    return LMB_OK;
+}
+
+// Fills the job table for a run starting from every lattice's current buffer.
+static int batch_prepare(lmb_batch *b)
+{
+    const uint32_t count = (uint32_t)b->lats.size();
+    b->jobs_host.resize(count);
+    b->cur0.resize(count);
+    uint32_t tiles = 0;
+    size_t smem = 0;
+    for (uint32_t j = 0; j < count; j++) {
+        lmb_lattice *l = b->lats[j];
+        lmb_model *m = const_cast<lmb_model *>(b->models[j]);
+        if (l->pending) return LMB_E_STATE;
+        if (m->dirty) {
+            int rc = upload_model(m);
+            if (rc) return rc;
+        }
+        int rc = validate_for_model(l, m);
+        if (rc) return rc;
+        FusedJob &jb = b->jobs_host[j];
+        jb.buf[0] = l->buf[0];
+        jb.buf[1] = l->buf[1];
+        jb.sites = l->sites;
+        jb.g = l->g;
+        jb.m = m->dev;
+        jb.rs = l->rs;
+        jb.list = l->list;
+        jb.cap = l->cap;
+        jb.ts = l->tile;
+        jb.with_reaction = m->nr > 0;
+        jb.cur0 = (uint32_t)l->cur;
+        jb.tile_begin = tiles;
+        b->cur0[j] = l->cur;
+        tiles += l->tile.tiles_y * l->tile.tiles_z;
+        const size_t sm = fused_smem_bytes(l->tile, l->g.X, l->words, l->cap, m->dev.stage_bytes);
+        if (sm > smem) smem = sm;
+    }
+    b->total_tiles = tiles;
+    b->smem = smem;
+    CK(cudaMemcpyAsync(b->jobs, b->jobs_host.data(), sizeof(FusedJob) * count, cudaMemcpyHostToDevice,
+                       b->ctx->stream));
+    return LMB_OK;
+}
+
+extern "C" int lmb_batch_run_async(lmb_batch *b, const uint32_t *seeds, uint32_t first, uint32_t n, int mode)
+{
+    if (!b || !seeds) return LMB_E_ARG;
+    if (b->pending) return LMB_E_STATE;
+    if (mode != LMB_OVERFLOW_CLASSIC && mode != LMB_OVERFLOW_RELAXED) return LMB_E_ARG;
+    lmb_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    int rc = batch_prepare(b);
+    if (rc) return rc;
+    const uint32_t count = (uint32_t)b->lats.size();
+    CK(cudaMemcpyAsync(b->seeds, seeds, sizeof(uint32_t) * count, cudaMemcpyHostToDevice, c->stream));
+    CK(launch_begin_batch(b->rs_ptrs, b->seeds, count, first, n, (uint32_t)mode, c->stream));
+    uint32_t done = 0;
+    if (n >= 2 * BATCH_GRAPH_STEPS) {
+        // One graph of BATCH_GRAPH_STEPS launches (parities 0, 1, ...) serves
+        // every run: the job table it reads is rewritten before each run.
+        static_assert(BATCH_GRAPH_STEPS % 2 == 0, "graph must return to parity 0");
+        if (b->graph && (b->graph_tiles != b->total_tiles || b->graph_smem != b->smem)) {
+            cudaGraphExecDestroy(b->graph);  // a lattice changed its tile plan
+            b->graph = nullptr;
+        }
+        if (!b->graph) {
+            const uint64_t l0 = lmb_kernel_launches();
+            if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                cudaError_t e = cudaSuccess;
+                for (uint32_t s = 0; s < BATCH_GRAPH_STEPS && e == cudaSuccess; s++)
+                    e = launch_fused_batch(b->bps, b->slots, b->jobs, count, b->total_tiles, b->smem, s & 1u, c->stream);
+                cudaGraph_t graph = nullptr;
+                const cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+                const uint64_t captured = lmb_kernel_launches() - l0;
+                count_launch((uint64_t)0 - captured);
+                if (e == cudaSuccess && e2 == cudaSuccess && cudaGraphInstantiate(&b->graph, graph, 0) == cudaSuccess) {
+                    b->graph_kernels = captured;
+                    b->graph_tiles = b->total_tiles;
+                    b->graph_smem = b->smem;
+                } else {
+                    b->graph = nullptr;
+                }
+                if (graph) cudaGraphDestroy(graph);
+            } else {
+                cudaGetLastError();
+            }
+        }
+        if (b->graph) {
+            for (; done + BATCH_GRAPH_STEPS <= n; done += BATCH_GRAPH_STEPS) {
+                CK(cudaGraphLaunch(b->graph, c->stream));
+                count_launch(b->graph_kernels);
+            }
+        }
+    }
+    for (; done < n; done++)
+        CK(launch_fused_batch(b->bps, b->slots, b->jobs, count, b->total_tiles, b->smem, done & 1u, c->stream));
+    CK(launch_gather_states(b->rs_ptrs, count, b->states, c->stream));
+    CK(cudaMemcpyAsync(b->states_host, b->states, sizeof(RunState) * count, cudaMemcpyDeviceToHost, c->stream));
+    b->pending = true;
+    b->pending_first = first;
+    b->pending_n = n;
+    for (lmb_lattice *l : b->lats) l->pending = true;
+    return LMB_OK;
+}
+
+extern "C" int lmb_batch_wait(lmb_batch *b, lmb_run_stats *stats)
+{
+    if (!b) return LMB_E_ARG;
+    if (!b->pending) return LMB_E_STATE;
+    lmb_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    b->pending = false;
+    for (lmb_lattice *l : b->lats) l->pending = false;
+    CK(cudaStreamSynchronize(c->stream));
+    int first_error = LMB_OK;
+    for (size_t j = 0; j < b->lats.size(); j++) {
+        const RunState &h = b->states_host[j];
+        lmb_lattice *l = b->lats[j];
+        const uint32_t done = h.status == LMB_OK ? b->pending_n : h.failed_step - b->pending_first;
+        l->cur = b->cur0[j] ^ (int)((h.status == LMB_OK ? done : done + 1) & 1u);
+        if (stats) {
+            stats[j].status = h.status;
+            stats[j].steps_done = done;
+            stats[j].failed_step = h.status == LMB_OK ? 0 : h.failed_step;
+            stats[j].unresolved = h.mode == LMB_OVERFLOW_RELAXED ? h.ovf_count : 0;
+            stats[j].overflows = h.overflows;
+            stats[j].reactions = h.reactions;
+        }
+        if (h.status != LMB_OK && first_error == LMB_OK) first_error = h.status;
+    }
+    return first_error;
+}
+
+extern "C" int lmb_batch_run(lmb_batch *b, const uint32_t *seeds, uint32_t first, uint32_t n, int mode,
+                             lmb_run_stats *stats)
+{
+    int rc = lmb_batch_run_async(b, seeds, first, n, mode);
+    if (rc != LMB_OK) return rc;
+    return lmb_batch_wait(b, stats);
+}

@@ -128,15 +128,15 @@ __device__ __forceinline__ void warp_append(uint32_t b, uint32_t r, uint32_t w, 
     }
 }
 
+// One timestep of one tile (`tile` of the lattice's `ntiles`), run by the
+// whole block.  The block is flat (FUSED_THREADS threads); the tile's
+// logical bx x by layout (bx a multiple of 32, so a warp is 32 consecutive x
+// of one row) comes from the tile shape.
 template <int BPS, int S>
-__global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_t *__restrict__ src,
-                                                                   uint32_t *__restrict__ dst,
-                                                                   const uint8_t *__restrict__ sites, Geometry g,
-                                                                   const __grid_constant__ DevTables m,
-                                                                   RunState *__restrict__ rs,
-                                                                   OverflowEntry *__restrict__ list, uint32_t cap,
-                                                                   const __grid_constant__ TileShape ts,
-                                                                   int with_reaction)
+__device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
+                                           const uint8_t *__restrict__ sites, const Geometry &g, const DevTables &m,
+                                           RunState *__restrict__ rs, OverflowEntry *__restrict__ list, uint32_t cap,
+                                           const TileShape &ts, int with_reaction, uint32_t tile, uint32_t ntiles)
 {
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_last;
@@ -149,11 +149,11 @@ __global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_
     constexpr int W = SiteWords<BPS, S>::W;
     if (rs->status != LMB_OK) return;
     const uint32_t X = g.X, R = ts.R, Ry = ts.Ry, Ty = ts.Ty, Tz = ts.Tz, MW = ts.MW;
-    const uint32_t tyi = blockIdx.x % ts.tiles_y, tzi = blockIdx.x / ts.tiles_y;
+    const uint32_t tyi = tile % ts.tiles_y, tzi = tile / ts.tiles_y;
     const uint32_t y0 = tyi * Ty, z0 = tzi * Tz;
     const uint32_t seed = rs->seed, step = rs->step;
-    const uint32_t tx = threadIdx.x, ty = threadIdx.y, bx = blockDim.x, by = blockDim.y;
-    const uint32_t tid = tx + ty * bx, nthr = bx * by;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t bx = ts.bx, by = nthr / bx, tx = tid % bx, ty = tid / bx;
     const uint32_t rows = Ry * ts.Rz, yrows = Ty * ts.Rz, orows = Ty * Tz;
     // Shared layout: A[W][R], B[W][R] particle words (valid where the
     // occupancy bit is set), work[R] site list, T[R] site types, then
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_
     if (tid == 0) {
         __threadfence();
         const uint32_t prev = atomicAdd(&rs->tiles_done, 1u);
-        s_last = prev == gridDim.x - 1;
+        s_last = prev == ntiles - 1;
     }
     __syncthreads();
     if (s_last) {
@@ -401,6 +401,39 @@ __global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_
         if (tid == 0) rs->tiles_done = 0;
         resolve_block_flat<BPS, S>(dst, sites, g, rs, list, cap, (OverflowEntry *)smem, tid, nthr);
     }
+}
+
+template <int BPS, int S>
+__global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_t *__restrict__ src,
+                                                                   uint32_t *__restrict__ dst,
+                                                                   const uint8_t *__restrict__ sites, Geometry g,
+                                                                   const __grid_constant__ DevTables m,
+                                                                   RunState *__restrict__ rs,
+                                                                   OverflowEntry *__restrict__ list, uint32_t cap,
+                                                                   const __grid_constant__ TileShape ts,
+                                                                   int with_reaction)
+{
+    fused_tile<BPS, S>(src, dst, sites, g, m, rs, list, cap, ts, with_reaction, blockIdx.x, gridDim.x);
+}
+
+// A batch of lattices advanced together: block b runs the tile of the job
+// whose tile range holds b.  The buffers a job reads and writes alternate
+// with `parity` (flipped every timestep), from the job's buffer index at the
+// start of the run.
+template <int BPS, int S>
+__global__ void __launch_bounds__(FUSED_THREADS) fused_batch_kernel(const FusedJob *__restrict__ jobs,
+                                                                    uint32_t njobs, uint32_t parity)
+{
+    uint32_t lo = 0, hi = njobs;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (jobs[mid].tile_begin <= blockIdx.x) lo = mid;
+        else hi = mid;
+    }
+    const FusedJob &j = jobs[lo];
+    const uint32_t c = j.cur0 ^ parity;
+    fused_tile<BPS, S>(j.buf[c], j.buf[c ^ 1], j.sites, j.g, j.m, j.rs, j.list, j.cap, j.ts, j.with_reaction,
+                       blockIdx.x - j.tile_begin, j.ts.tiles_y * j.ts.tiles_z);
 }
 
 // ---------------------------------------------------------------------------
@@ -502,7 +535,7 @@ cudaError_t launch_fused(int bps, int slots, const uint32_t *src, uint32_t *dst,
 {
     const uint32_t W = bps == 1 ? slots / 4 : slots;
     const size_t smem = fused_smem_bytes(ts, g.X, W, cap, m.stage_bytes);
-    const dim3 grid(ts.tiles_y * ts.tiles_z), block(ts.bx, ts.by);
+    const dim3 grid(ts.tiles_y * ts.tiles_z), block(FUSED_THREADS);
     count_launch();
     FUSED_DISPATCH(1, 4)
     FUSED_DISPATCH(1, 8)
@@ -510,6 +543,41 @@ cudaError_t launch_fused(int bps, int slots, const uint32_t *src, uint32_t *dst,
     FUSED_DISPATCH(4, 4)
     FUSED_DISPATCH(4, 8)
     FUSED_DISPATCH(4, 16)
+    return cudaErrorInvalidValue;
+}
+
+template <int BPS, int S>
+static cudaError_t ensure_batch_smem_limit(size_t smem)
+{
+    static size_t granted[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (smem <= 48 * 1024 || smem <= granted[dev]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(fused_batch_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess) granted[dev] = smem;
+    return e;
+}
+
+#define BATCH_DISPATCH(BPS_, S_)                                                                      \
+    if (bps == BPS_ && slots == S_) {                                                                 \
+        cudaError_t e = ensure_batch_smem_limit<BPS_, S_>(smem);                                      \
+        if (e != cudaSuccess) return e;                                                               \
+        fused_batch_kernel<BPS_, S_><<<total_tiles, FUSED_THREADS, smem, stream>>>(jobs, njobs, parity); \
+        return cudaGetLastError();                                                                    \
+    }
+
+cudaError_t launch_fused_batch(int bps, int slots, const FusedJob *jobs, uint32_t njobs, uint32_t total_tiles,
+                               size_t smem, uint32_t parity, cudaStream_t stream)
+{
+    count_launch();
+    BATCH_DISPATCH(1, 4)
+    BATCH_DISPATCH(1, 8)
+    BATCH_DISPATCH(1, 16)
+    BATCH_DISPATCH(4, 4)
+    BATCH_DISPATCH(4, 8)
+    BATCH_DISPATCH(4, 16)
     return cudaErrorInvalidValue;
 }
 

@@ -26,6 +26,26 @@ struct TileShape {
     uint32_t bx, by;
 };
 
+// One lattice of a batch run: both buffers (the run starts from buf[cur0]),
+// its model, run state, overflow queue and tile plan, and where its tiles
+// start in the batch's block numbering.
+struct FusedJob {
+    uint32_t *buf[2];
+    const uint8_t *sites;
+    Geometry g;
+    DevTables m;
+    RunState *rs;
+    OverflowEntry *list;
+    uint32_t cap;
+    TileShape ts;
+    int with_reaction;
+    uint32_t cur0;
+    uint32_t tile_begin;
+};
+
+cudaError_t launch_fused_batch(int bytes_per_slot, int slots, const FusedJob *jobs, uint32_t njobs,
+                               uint32_t total_tiles, size_t smem, uint32_t parity, cudaStream_t stream);
+
 bool fused_make_shape(const Geometry &g, int bytes_per_slot, int slots, uint32_t Ty, uint32_t Tz, TileShape &ts);
 bool fused_default_shape(const Geometry &g, int bytes_per_slot, int slots, TileShape &ts);
 size_t fused_smem_bytes(const TileShape &ts, uint32_t X, uint32_t W, uint32_t cap, uint32_t stage_bytes);

@@ -72,6 +72,9 @@ cudaError_t launch_resolve(int bytes_per_slot, int slots, uint32_t *lat, const u
                            cudaStream_t stream);
 cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
                              cudaStream_t stream);
+cudaError_t launch_begin_batch(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,
+                               uint32_t n, uint32_t mode, cudaStream_t stream);
+cudaError_t launch_gather_states(RunState *const *rs_ptrs, uint32_t count, RunState *out, cudaStream_t stream);
 cudaError_t launch_counts(int bytes_per_slot, int slots, const uint32_t *lat, const Geometry &g,
                           uint32_t ns, unsigned long long *counts, cudaStream_t stream);
 cudaError_t launch_validate(int bytes_per_slot, int slots, const uint32_t *lat, const uint8_t *sites,

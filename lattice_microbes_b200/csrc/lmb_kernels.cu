@@ -124,6 +124,49 @@ __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, ui
     }
 }
 
+// Batch forms: run state j lives at *rs_ptrs[j]; seeds[j] is its seed.
+__global__ void begin_batch_kernel(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,
+                                   uint32_t n, uint32_t mode)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    RunState *rs = rs_ptrs[j];
+    rs->seed = seeds[j];
+    rs->step = first;
+    rs->end_step = first + n;
+    rs->status = LMB_OK;
+    rs->failed_step = 0;
+    rs->mode = mode;
+    rs->overflows = 0;
+    rs->reactions = 0;
+    rs->tiles_done = 0;
+    if (mode == LMB_OVERFLOW_CLASSIC) {
+        rs->ovf_count = 0;
+        rs->carried = 0;
+    }
+}
+
+__global__ void gather_states_kernel(RunState *const *rs_ptrs, uint32_t count, RunState *out)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < count) out[j] = *rs_ptrs[j];
+}
+
+cudaError_t launch_begin_batch(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,
+                               uint32_t n, uint32_t mode, cudaStream_t stream)
+{
+    count_launch();
+    begin_batch_kernel<<<(count + 127) / 128, 128, 0, stream>>>(rs_ptrs, seeds, count, first, n, mode);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_states(RunState *const *rs_ptrs, uint32_t count, RunState *out, cudaStream_t stream)
+{
+    count_launch();
+    gather_states_kernel<<<(count + 127) / 128, 128, 0, stream>>>(rs_ptrs, count, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
                              cudaStream_t stream)
 {

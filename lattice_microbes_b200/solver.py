@@ -244,6 +244,53 @@ class Lattice:
             pass
 
 
+class Batch:
+    """Many lattices advanced together (lmb_batch): one launch per timestep
+    for all of them.  Each lattice ends where lmb_run alone would take it."""
+
+    def __init__(self, ctx, lattices, models):
+        n = len(lattices)
+        la = (L.vp * n)(*[l.handle for l in lattices])
+        mo = (L.vp * n)(*[m.handle for m in models])
+        h = L.vp()
+        L.check(L.lib().lmb_batch_create(ctx.handle, n, la, mo, C.byref(h)), "lmb_batch_create")
+        self.ctx, self.handle = ctx, h
+        self.lattices, self.models = list(lattices), list(models)
+
+    def run(self, seeds, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC, check=True):
+        n = len(self.lattices)
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        stats = (L.RunStats * n)()
+        rc = L.lib().lmb_batch_run(self.handle, _p(sd, L.u32p), first_timestep, timesteps, overflow_mode, stats)
+        if check:
+            L.check(rc, "lmb_batch_run")
+        return rc, list(stats)
+
+    def run_async(self, seeds, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
+        self._seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        L.check(L.lib().lmb_batch_run_async(self.handle, _p(self._seeds, L.u32p), first_timestep, timesteps,
+                                            overflow_mode), "lmb_batch_run_async")
+
+    def wait(self, check=True):
+        n = len(self.lattices)
+        stats = (L.RunStats * n)()
+        rc = L.lib().lmb_batch_wait(self.handle, stats)
+        if check:
+            L.check(rc, "lmb_batch_wait")
+        return rc, list(stats)
+
+    def close(self):
+        if self.handle:
+            L.lib().lmb_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def compose_seed(seed_top, replicate):
     return L.lib().lmb_compose_seed(seed_top, replicate)
 
