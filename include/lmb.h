@@ -228,9 +228,11 @@ int lmb_run_profiled(lmb_lattice *lattice, const lmb_model *model, uint32_t seed
  * timestep covers every tile of every lattice, replayed from a captured CUDA
  * graph.  Replaces running the reference's ReplicateRunner threads
  * (core/ReplicateRunner.cpp:84-166), one MpdRdmeSolver each, on one device.
- * All lattices share the context, slot count and bytes per slot and use the
- * fused schedule; each has its own model (rates scale with its site count)
- * and its own seed.  Each lattice gives the same result as lmb_run on it. */
+ * All lattices share the context, slot count (16 at most) and bytes per
+ * slot; each has its own model (rates scale with its site count) and its own
+ * seed.  The batch tiles each lattice with its largest efficient tile (the
+ * batch itself fills the GPU).  Each lattice gives the same result as lmb_run
+ * on it. */
 typedef struct lmb_batch lmb_batch;
 int lmb_batch_create(lmb_ctx *ctx, uint32_t count, lmb_lattice *const *lattices, const lmb_model *const *models,
                      lmb_batch **out);

@@ -1100,6 +1100,7 @@ struct lmb_batch {
     RunState *states;
     RunState *states_host;  // pinned
     std::vector<FusedJob> jobs_host;
+    std::vector<TileShape> tiles;  // batch plan per lattice
     uint32_t total_tiles;
     size_t smem;
     cudaGraphExec_t graph;
@@ -1125,8 +1126,10 @@ extern "C" int lmb_batch_create(lmb_ctx *c, uint32_t count, lmb_lattice *const *
         if (!l || !m || l->ctx != c || m->ctx != c) return LMB_E_ARG;
         if ((int)l->bps != bps || (int)l->slots != slots) return LMB_E_ARG;
         if (m->has_desc && (m->X != l->g.X || m->Y != l->g.Y || m->Z != l->g.Z)) return LMB_E_ARG;
-        if (l->schedule != LMB_SCHEDULE_FUSED) return LMB_E_UNSUPPORTED;
     }
+    std::vector<TileShape> plan(count);
+    for (uint32_t j = 0; j < count; j++)
+        if (!fused_batch_shape(lattices[j]->g, bps, slots, plan[j])) return LMB_E_UNSUPPORTED;
     CK(cudaSetDevice(c->device));
     lmb_batch *b = new (std::nothrow) lmb_batch;
     if (!b) return LMB_E_NOMEM;
@@ -1134,6 +1137,7 @@ extern "C" int lmb_batch_create(lmb_ctx *c, uint32_t count, lmb_lattice *const *
     ctx_retain(c);
     b->lats.assign(lattices, lattices + count);
     b->models.assign(models, models + count);
+    b->tiles = plan;
     b->bps = bps;
     b->slots = slots;
     b->jobs = nullptr;
@@ -1208,13 +1212,13 @@ static int batch_prepare(lmb_batch *b)
         jb.rs = l->rs;
         jb.list = l->list;
         jb.cap = l->cap;
-        jb.ts = l->tile;
+        jb.ts = b->tiles[j];
         jb.with_reaction = m->nr > 0;
         jb.cur0 = (uint32_t)l->cur;
         jb.tile_begin = tiles;
         b->cur0[j] = l->cur;
-        tiles += l->tile.tiles_y * l->tile.tiles_z;
-        const size_t sm = fused_smem_bytes(l->tile, l->g.X, l->words, l->cap, m->dev.stage_bytes);
+        tiles += b->tiles[j].tiles_y * b->tiles[j].tiles_z;
+        const size_t sm = fused_smem_bytes(b->tiles[j], l->g.X, l->words, l->cap, m->dev.stage_bytes);
         if (sm > smem) smem = sm;
     }
     b->total_tiles = tiles;

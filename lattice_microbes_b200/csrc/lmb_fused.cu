@@ -520,6 +520,31 @@ static cudaError_t ensure_smem_limit(size_t smem)
     return e;
 }
 
+// Batch plan: the batch already fills the GPU with many lattices, so each
+// lattice takes the tile with the least halo overhead that still lets two
+// blocks share an SM.
+bool fused_batch_shape(const Geometry &g, int bps, int slots, TileShape &ts)
+{
+    const uint32_t cands[] = {1, 2, 4, 8, 16};
+    bool found = false;
+    double best = 1e30;
+    for (uint32_t Ty : cands)
+        for (uint32_t Tz : cands) {
+            TileShape t;
+            if (!fused_make_shape(g, bps, slots, Ty, Tz, t)) continue;
+            const uint32_t W = bps == 1 ? slots / 4 : slots;
+            if (region_bytes(g.X, Ty, Tz, W) > FUSED_PREFERRED_SMEM) continue;
+            const double halo = (double)(Ty + 2) * (Tz + 2) / ((double)Ty * Tz);
+            const double score = halo - 1e-6 * Ty * Tz;
+            if (score < best) {
+                best = score;
+                ts = t;
+                found = true;
+            }
+        }
+    return found;
+}
+
 #define FUSED_DISPATCH(BPS_, S_)                                                                       \
     if (bps == BPS_ && slots == S_) {                                                                  \
         cudaError_t e = ensure_smem_limit<BPS_, S_>(smem);                                             \
