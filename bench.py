@@ -13,10 +13,14 @@ N > 1 is launched through torch.distributed.run: every rank runs its own
 replicate (its own seed) on its own GPU with no data exchange (replicas only);
 the value is all ranks' site-steps over the slowest rank's device time.
 
---impl reference times the reference's own MPD code on the host cores: the
-reference device functions compiled for the CPU from the reference sources
-(oracle/_ref), one replicate per host core as ReplicateRunner runs replicates,
-each bench step a bounded sample of the same workload.
+--impl reference times the reference's own CPU RDME solver on the host
+cores: lm::rdme::NextSubvolumeSolver compiled from the reference sources
+(oracle/_ref), one replicate of the same workload per host core as
+ReplicateRunner runs replicates, each bench step a bounded stretch of
+simulated time; its site-steps are sites x simulated time / tau.  The
+default run reports the same figure as cpu_baseline, and beside it the
+reference's MPD device functions compiled for the host (the reference has no
+CPU MPD solver of its own).
 """
 import argparse
 import json
@@ -46,16 +50,20 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--timesteps-per-step", type=int, default=TIMESTEPS_PER_STEP)
     ap.add_argument("--cpu-sample-timesteps", type=int, default=0,
-                    help="timesteps per core in the CPU baseline sample (0 = auto)")
+                    help="timesteps per core of the reference MPD functions on the host (0 = auto)")
+    ap.add_argument("--cpu-sample-time", type=float, default=0.0,
+                    help="simulated seconds per core of the reference NextSubvolumeSolver (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
-    ap.add_argument("--workload", choices=["rodcell", "batch"], default="rodcell",
+    ap.add_argument("--workload", choices=["rodcell", "batch", "cme", "serve"], default="rodcell",
                     help="rodcell: one 64x64x128 lattice (default); batch: 256 bimolecular replicates of "
-                         "uneven size in one launch per timestep")
-    ap.add_argument("--replicates", type=int, default=256)
+                         "uneven size in one launch per timestep; cme: 65,536 two-state gene replicates "
+                         "(direct method) to t = 3600 s; serve: a Poisson stream of solve requests")
+    ap.add_argument("--replicates", type=int, default=0, help="batch: 256, cme: 65536 (0 = default)")
+    ap.add_argument("--requests", type=int, default=48, help="serve: requests of the stream to replay")
     return ap.parse_args()
 
 
@@ -64,7 +72,7 @@ def parse():
 # --------------------------------------------------------------------------
 
 def _cpu_worker(args):
-    """One replicate of the reference MPD code on one core (spawned)."""
+    """One replicate of the reference MPD device functions on one core (spawned)."""
     seed, timesteps = args
     sys.path.insert(0, ROOT)
     from lattice_microbes_b200 import configs
@@ -81,7 +89,8 @@ def _cpu_worker(args):
 
 
 def cpu_reference_sample(timesteps, cores):
-    """Runs `cores` replicates in parallel; returns (site-steps/s, sample)."""
+    """Reference MPD device functions, `cores` replicates in parallel;
+    returns (site-steps/s, sample)."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
@@ -93,6 +102,39 @@ def cpu_reference_sample(timesteps, cores):
     value = nsites * timesteps * cores / wall
     sample = ("%d replicates x %d timesteps of the rod-cell workload, one per core, reference device "
               "functions compiled for the host; %.1f s wall" % (cores, timesteps, wall))
+    return value, sample
+
+
+def _nsm_worker(args):
+    """One replicate of the reference NextSubvolumeSolver on one core (spawned)."""
+    seed, sim_time = args
+    sys.path.insert(0, ROOT)
+    from lattice_microbes_b200 import configs
+    from tests import ref_cpu_lib
+    if not ref_cpu_lib.available():
+        return None
+    spec = configs.config1(seed=seed)
+    t0 = time.perf_counter()
+    ref_cpu_lib.nsm_run(spec, 1000 + seed, seed + 1, sim_time, sim_time / 4)
+    return time.perf_counter() - t0
+
+
+def cpu_nsm_sample(sim_time, cores):
+    """Reference NextSubvolumeSolver, `cores` replicates of the rod-cell
+    workload in parallel, each to `sim_time` seconds; returns (site-steps/s,
+    sample) with site-steps = sites x sim_time / tau per replicate."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_nsm_worker, [(s, sim_time) for s in range(cores)])
+    if any(r is None for r in res):
+        return None, "reference CPU solvers not built (oracle/_ref)"
+    wall = max(res)
+    nsites, tau = 64 * 64 * 128, 25e-6
+    value = nsites * (sim_time / tau) * cores / wall
+    sample = ("%d replicates of the rod-cell workload, one per core, each %.4g s of simulated time (%d "
+              "MPD-timestep equivalents), reference NextSubvolumeSolver built from its sources; %.1f s wall"
+              % (cores, sim_time, round(sim_time / tau), wall))
     return value, sample
 
 
@@ -197,12 +239,15 @@ def run_ours(a):
 
     # CPU baseline first (spawned workers, before any GPU work on this rank).
     cpu = None
+    cpu_mpd = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = host_cores()
-        ts = a.cpu_sample_timesteps or 60
-        val, sample = cpu_reference_sample(ts, cores)
+        val, sample = cpu_nsm_sample(a.cpu_sample_time or 0.04, cores)
         if val is not None:
             cpu = {"value": val, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample}
+        val, sample = cpu_reference_sample(a.cpu_sample_timesteps or 60, cores)
+        if val is not None:
+            cpu_mpd = {"value": val, "unit": METRIC, "cores": cores, "sample": sample}
 
     from lattice_microbes_b200 import configs
     from lattice_microbes_b200.solver import Context, Lattice, Model, compose_seed, kernel_launches
@@ -375,6 +420,7 @@ def run_ours(a):
             "gpu_launches": int(launches),
             "clocks": clock_info,
             "cpu_baseline": cpu,
+            "reference_mpd_on_host_cores": cpu_mpd,
             "reference_kernels_b200": ref_gpu,
             "run_stats": {"overflows": int(st.overflows), "reactions_per_step": int(st.reactions)},
         }
@@ -393,12 +439,12 @@ def run_reference(a):
     if rank != 0:
         return
     cores = host_cores()
-    ts = a.cpu_sample_timesteps or 20
+    sim_time = a.cpu_sample_time or 0.01
     vals, samples = [], []
-    for _ in range(a.warmup if a.warmup < 1 else 1):
-        cpu_reference_sample(max(2, ts // 4), cores)
+    for _ in range(min(a.warmup, 1)):
+        cpu_nsm_sample(sim_time / 4, cores)
     for _ in range(a.steps):
-        v, s = cpu_reference_sample(ts, cores)
+        v, s = cpu_nsm_sample(sim_time, cores)
         if v is None:
             print(json.dumps({"impl": "reference", "unavailable": s}))
             return
@@ -443,7 +489,7 @@ def run_batch(a):
 
     torch.cuda.set_device(0)
     T = a.timesteps_per_step if a.timesteps_per_step != TIMESTEPS_PER_STEP else 200
-    edges = configs.batch_edges(seed=7, count=a.replicates)
+    edges = configs.batch_edges(seed=7, count=a.replicates or 256)
     ctx = Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
     lats, models, specs = [], [], []
@@ -529,11 +575,254 @@ def run_batch(a):
     ctx.close()
 
 
+def _gd_worker(args):
+    """Reference GillespieDSolver replicates on one core (spawned)."""
+    first, count = args
+    sys.path.insert(0, ROOT)
+    from lattice_microbes_b200 import configs
+    from tests import ref_cpu_lib
+    if not ref_cpu_lib.available():
+        return None
+    m = configs.two_state_gene()
+    t0 = time.perf_counter()
+    for k in range(first, first + count):
+        ref_cpu_lib.gillespie_run(m.ns, m.rtype, m.K, m.S, m.D, m.init, 77, k + 1, m.max_time, m.write_interval)
+    return time.perf_counter() - t0
+
+
+def cpu_gillespie_sample(per_core, cores):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_gd_worker, [(c * per_core, per_core) for c in range(cores)])
+    if any(r is None for r in res):
+        return None, "reference CPU solvers not built (oracle/_ref)"
+    wall = max(res)
+    value = per_core * cores / wall
+    return value, ("%d replicates per core on %d cores of the two-state gene model to t = 3600 s, reference "
+                   "GillespieDSolver built from its sources; %.1f s wall" % (per_core, cores, wall))
+
+
+def run_cme(a):
+    """GillespieD CME ensemble: 65,536 replicates of the two-state gene model
+    (configs.two_state_gene) to t = 3600 s, counts every 600 s, one GPU
+    thread per replicate.  Metric: replicates/s (trajectories to 3600 s)."""
+    import numpy as np
+    import torch
+
+    from lattice_microbes_b200 import configs
+    from lattice_microbes_b200.solver import CMEEnsemble, Context, kernel_launches
+
+    reps = a.replicates or 65536
+    cores = host_cores()
+    cpu = None
+    if not a.no_cpu_baseline:
+        v, sample = cpu_gillespie_sample(64, cores)
+        if v is not None:
+            cpu = {"value": v, "unit": "replicates/s", "cores": cores, "kind": "reference", "sample": sample}
+    torch.cuda.set_device(0)
+    ctx = Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))
+    m = configs.two_state_gene()
+    ens = CMEEnsemble(ctx, m, reps)
+    for k in range(a.warmup):
+        ens.run(1000 + k, m.max_time, m.write_interval)
+    times, events = [], 0
+    launches0 = kernel_launches()
+    clocks = ClockSampler(0)
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(a.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            ens.begin(k + 1, m.max_time, m.write_interval)
+            e0.record(stream)
+            ens.advance_async(m.max_time)
+            e1.record(stream)
+            torch.cuda.synchronize(0)
+            times.append(e0.elapsed_time(e1))
+            events += ens.stats()[0]
+    clock_info = clocks.stop()
+    launches = kernel_launches() - launches0
+    ms = sum(times) / a.steps
+    value = reps / (ms / 1e3)
+    # End to end through the public API: initial counts in, records out.
+    init = np.tile(m.init, (reps, 1)).astype(np.uint32)
+    e2e = []
+    for k in range(a.steps):
+        t0 = time.perf_counter()
+        ens.set_initial_counts(init)
+        ens.run(k + 1, m.max_time, m.write_interval)
+        out = ens.counts()
+        e2e.append(time.perf_counter() - t0)
+    entries = ens.entries()
+    ens.close()
+    ctx.close()
+    line = {
+        "metric": "replicates/s",
+        "value": value,
+        "unit": "replicates/s",
+        "n_gpus": 1,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int32 counts, f32 propensities, f64 time",
+        "data": "synthetic (two-state gene model, lattice_microbes_b200.configs.two_state_gene)",
+        "config": {"workload": "GillespieD CME ensemble, %d replicates of the two-state gene model to t = 3600 s, "
+                               "counts every 600 s" % reps,
+                   "l2": "state and records (%d MB) are L2-resident; the kernel is issue-bound" %
+                         max(1, reps * (entries * 4 * 4 + 64) >> 20)},
+        "events_per_s": events / a.steps / (ms / 1e3),
+        "e2e": {"value": reps / (sum(e2e) / a.steps), "unit": "replicates/s",
+                "h2d_bytes_per_step": int(init.nbytes), "d2h_bytes_per_step": int(out.nbytes)},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(a):
+    """Serving: the first --requests requests of a seeded Poisson stream
+    (50 req/s; edges 16..128, 2..50 species, 0.5..2 particles per site,
+    1k..20k timesteps; configs.serve_stream) replayed at their arrival times
+    into the solve server (continuous batching, 150 GB budget, ByteLattice
+    16 slots).  Compared with sequential plain runs: the same requests solved
+    one at a time in arrival order (lmb_run each), their latencies computed
+    from the same arrival times."""
+    import numpy as np
+    import torch
+
+    from lattice_microbes_b200 import configs
+    from lattice_microbes_b200.solver import Context, Lattice, Model, Server, compose_seed, kernel_launches
+
+    torch.cuda.set_device(0)
+    stream_reqs = configs.serve_stream(seed=4, count=a.requests)
+    specs = []
+    for r in stream_reqs:
+        sp = configs.serve_problem(r)
+        specs.append(_to_byte16(sp))
+    seeds = [compose_seed(2024, r.index) for r in stream_reqs]
+    site_steps = sum(float(s.nsites) * r.timesteps for s, r in zip(specs, stream_reqs))
+    ctx = Context(0)
+    # Warm-up: one small solve through the server.
+    srv = Server(ctx, slots=16, bytes_per_slot=1, hbm_budget_bytes=150 << 30, max_active=256, chunk_timesteps=256)
+    for k in range(a.warmup):
+        srv.submit(10 ** 6 + k, specs[0], 1, 64)
+    while True:
+        act, q = srv.step()
+        while srv.pop_result(with_lattice=False) is not None:
+            pass
+        if act == 0 and q == 0:
+            break
+    launches0 = kernel_launches()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    submitted, done = 0, {}
+    while len(done) < len(stream_reqs):
+        now = time.perf_counter() - t0
+        while submitted < len(stream_reqs) and stream_reqs[submitted].arrival <= now:
+            r = stream_reqs[submitted]
+            srv.submit(r.index, specs[submitted], seeds[submitted], r.timesteps)
+            submitted += 1
+        act, q = srv.step()
+        while True:
+            res = srv.pop_result(with_lattice=False)
+            if res is None:
+                break
+            info = res[0]
+            done[info.id] = (time.perf_counter() - t0, info.stats.status)
+        if act == 0 and q == 0 and submitted < len(stream_reqs):
+            time.sleep(max(0.0, stream_reqs[submitted].arrival - (time.perf_counter() - t0)))
+    makespan = time.perf_counter() - t0
+    clock_info = clocks.stop()
+    launches = kernel_launches() - launches0
+    st = srv.status()
+    srv.close()
+    lat = np.array([done[r.index][0] - r.arrival for r in stream_reqs])
+    failed = sum(1 for v in done.values() if v[1] != 0)
+
+    # Sequential plain solver: one solve at a time, arrival order.
+    solo_s = []
+    for sp, r, sd in zip(specs, stream_reqs, seeds):
+        m = Model.from_spec(ctx, sp)
+        L2 = Lattice(ctx, sp.X, sp.Y, sp.Z, 16, 1)
+        torch.cuda.synchronize(0)
+        s0 = time.perf_counter()
+        L2.set_native(sp.lattice, sp.sites)
+        L2.run(m, sd, 0, r.timesteps)
+        L2.species_counts(sp.ns)
+        solo_s.append(time.perf_counter() - s0)
+        L2.close()
+        m.close()
+    finish, seq_lat = 0.0, []
+    for r, d in zip(stream_reqs, solo_s):
+        finish = max(finish, r.arrival) + d
+        seq_lat.append(finish - r.arrival)
+    seq_lat = np.array(seq_lat)
+    ctx.close()
+    line = {
+        "metric": "solves/s",
+        "value": len(stream_reqs) / makespan,
+        "unit": "solves/s",
+        "n_gpus": 1,
+        "steps": 1,
+        "warmup": a.warmup,
+        "ms_per_step": makespan * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (seeded Poisson request stream, lattice_microbes_b200.configs.serve_stream)",
+        "config": {"workload": "serving: first %d requests of a 50 req/s Poisson stream, edges 16..128, 2..50 "
+                               "species, 0.5..2 particles/site, 1k..20k timesteps, ByteLattice-16, 150 GB budget, "
+                               "256 slots, 256-timestep chunks" % len(stream_reqs),
+                   "site_steps": site_steps},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "mean": float(lat.mean())},
+        "site_steps_per_s": site_steps / makespan,
+        "peak_resident": {"solves": int(st.peak_active), "bytes": int(st.peak_bytes)},
+        "failed": failed,
+        "sequential_plain": {"solves_per_s": len(stream_reqs) / finish,
+                             "latency_s": {"p50": float(np.percentile(seq_lat, 50)),
+                                           "p99": float(np.percentile(seq_lat, 99))},
+                             "site_steps_per_s": site_steps / sum(solo_s)},
+        "speedup_vs_sequential": (len(stream_reqs) / makespan) / (len(stream_reqs) / finish),
+        "e2e": {"value": len(stream_reqs) / makespan, "unit": "solves/s",
+                "h2d_bytes_per_step": int(sum(s.lattice.nbytes + s.sites.nbytes for s in specs)),
+                "d2h_bytes_per_step": 0},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _to_byte16(spec):
+    """The request's particles in a 16-slot ByteLattice (the serving layout)."""
+    import numpy as np
+    from lattice_microbes_b200 import configs
+    N = spec.nsites
+    slots = configs.native_to_slots(spec.lattice, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+    lat = configs.empty_lattice(spec.X, spec.Y, spec.Z, 16, 1)
+    for k in range(spec.slots):
+        lat[(k // 4) * N:(k // 4 + 1) * N] |= slots[:, k].astype(np.uint32) << np.uint32(8 * (k % 4))
+    spec.lattice, spec.slots = lat, 16
+    return spec
+
+
 if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "cme":
+        run_cme(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)

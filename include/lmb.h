@@ -243,7 +243,104 @@ int lmb_batch_run(lmb_batch *batch, const uint32_t *seeds, uint32_t first_timest
 int lmb_batch_run_async(lmb_batch *batch, const uint32_t *seeds, uint32_t first_timestep,
                         uint32_t number_timesteps, int overflow_mode);
 int lmb_batch_wait(lmb_batch *batch, lmb_run_stats *stats);
+/* Per-lattice timestep ranges: lattice j runs timesteps firsts[j] ..
+ * firsts[j] + counts[j] - 1 with seeds[j]; the launches cover the longest
+ * range and a lattice whose range is done sits them out.  Each lattice still
+ * gives lmb_run's result for its range.  Used for continuous batching, where
+ * the lattices of a batch are at different points of their runs. */
+int lmb_batch_run_ranges_async(lmb_batch *batch, const uint32_t *seeds, const uint32_t *firsts,
+                               const uint32_t *counts, int overflow_mode);
+/* Replaces the batch's lattices (same context, slot count and bytes per
+ * slot); no run may be pending. */
+int lmb_batch_set_lattices(lmb_batch *batch, uint32_t count, lmb_lattice *const *lattices,
+                           const lmb_model *const *models);
 int lmb_batch_destroy(lmb_batch *batch);
+
+/* ---- serving: continuous batching of solves ------------------------------------
+ * A request is one MPD-RDME solve: a model (as lmb_model_create takes it), a
+ * native lattice with its site types, the composed seed and a timestep
+ * count.  The server keeps every admitted solve's lattice resident on the
+ * device and advances all of them together, one launch per timestep for
+ * all (lmb_batch_run_ranges_async).  Each lmb_server_step admits queued
+ * requests in arrival order while fewer than max_active solves are resident
+ * and their device bytes fit hbm_budget_bytes, runs chunk_timesteps
+ * timesteps of every resident solve (fewer for a solve near its end), and
+ * retires the solves that are done.  A solve's result is lmb_run's result
+ * for it alone, bit for bit.  Replaces the reference's one-solver-per-thread
+ * replicate runner (core/ReplicateRunner.cpp:84-166) for many independent
+ * solves on one device. */
+typedef struct lmb_server lmb_server;
+typedef struct {
+    uint64_t id;                 /* caller's tag, returned with the result */
+    const lmb_model_desc *model; /* copied by lmb_server_submit */
+    uint32_t X, Y, Z;
+    const uint32_t *particles;   /* native lattice, copied */
+    const uint8_t *sites;        /* site types, copied */
+    uint32_t seed;               /* composed 32-bit solver seed */
+    uint32_t timesteps;          /* timesteps 0 .. timesteps - 1 */
+} lmb_request;
+typedef struct {
+    uint64_t id;
+    lmb_run_stats stats;         /* status LMB_E_NOMEM: larger than the budget */
+    uint32_t X, Y, Z;
+    uint32_t number_species;
+    double t_submit, t_admit, t_done; /* seconds on the server's steady clock */
+} lmb_result_info;
+typedef struct {
+    uint32_t active, queued, ready, peak_active;
+    uint64_t bytes_in_use, peak_bytes, completed;
+    uint64_t next_ready_words;   /* particle words of the next result */
+} lmb_server_status_info;
+int lmb_server_create(lmb_ctx *ctx, uint32_t particles_per_site, uint32_t bytes_per_particle,
+                      uint64_t hbm_budget_bytes, uint32_t max_active, uint32_t chunk_timesteps,
+                      lmb_server **out);
+int lmb_server_destroy(lmb_server *server);
+int lmb_server_submit(lmb_server *server, const lmb_request *request);
+/* Admit, run one chunk, retire; blocks until the chunk is done. */
+int lmb_server_step(lmb_server *server, uint32_t *active, uint32_t *queued);
+/* Pops the oldest finished solve: its info, native lattice (optional) and
+ * species counts [0..number_species] (optional).  LMB_E_STATE when none. */
+int lmb_server_pop_result(lmb_server *server, lmb_result_info *info, uint32_t *particles,
+                          uint64_t particles_words, uint64_t *species_counts, uint32_t counts_len);
+int lmb_server_status(const lmb_server *server, lmb_server_status_info *status);
+
+/* ---- CME ensembles -----------------------------------------------------------
+ * Many independent replicates of a well-mixed model, each advanced by the
+ * direct method of lm::cme::GillespieDSolver (cme/GillespieDSolver.cpp:
+ * 107-382), one GPU thread per replicate.  Replaces running one
+ * GillespieDSolver per replicate thread (core/ReplicateRunner.cpp:84-166).
+ * The model arguments are those of CMESolver::buildModel (cme/CMESolver.h:
+ * 200-201) with reaction types LMB_REACTION_ZEROTH..SECOND_SELF; at most 32
+ * species and 64 reactions.  Counts are int32 and propensities FP32; time is
+ * FP64.  Random numbers come from the counter hash keyed by (seed, replicate,
+ * event), so a replicate's trajectory depends on neither the ensemble size
+ * nor how the run is cut into segments. */
+typedef struct lmb_cme lmb_cme;
+int lmb_cme_create(lmb_ctx *ctx, uint32_t number_species, uint32_t number_reactions,
+                   const uint32_t *reaction_types, const double *K, uint32_t k_cols, const int32_t *S,
+                   const uint32_t *D, uint32_t replicates, lmb_cme **out);
+int lmb_cme_destroy(lmb_cme *cme);
+/* Initial counts: [number_species] for every replicate (per_replicate = 0) or
+ * [replicates][number_species].  Takes effect at the next lmb_cme_begin. */
+int lmb_cme_set_initial_counts(lmb_cme *cme, const uint32_t *counts, int per_replicate);
+/* Starts a run to t_end recording the counts every write_interval seconds
+ * from t = 0, as GillespieDSolver records them (the counts before the first
+ * event past each write time, GillespieDSolver.cpp:202-213, 329-338).
+ * lmb_cme_entries gives the number of records. */
+int lmb_cme_begin(lmb_cme *cme, uint32_t seed, double t_end, double write_interval);
+/* Enqueues the segment up to time `until` (clamped to t_end) on the
+ * context stream and returns. */
+int lmb_cme_advance_async(lmb_cme *cme, double until);
+/* begin + one segment to t_end + wait. */
+int lmb_cme_run(lmb_cme *cme, uint32_t seed, double t_end, double write_interval);
+int lmb_cme_entries(const lmb_cme *cme, uint32_t *entries);
+/* Waits and copies the records out as [replicates][entries][number_species]
+ * (one SpeciesCounts data set per replicate). */
+int lmb_cme_get_counts(lmb_cme *cme, uint32_t *counts);
+/* Device pointer of the records, laid out [entries][number_species][replicates]. */
+int lmb_cme_device_counts(lmb_cme *cme, void **counts);
+/* Waits; total events applied and replicates that reached t_end. */
+int lmb_cme_stats(lmb_cme *cme, uint64_t *events, uint32_t *finished);
 
 /* Launch counters for the bench's kernel accounting. */
 uint64_t lmb_kernel_launches(void);

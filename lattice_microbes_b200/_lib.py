@@ -63,6 +63,29 @@ class RunStats(C.Structure):
     ]
 
 
+class Request(C.Structure):
+    _fields_ = [
+        ("id", C.c_uint64), ("model", C.POINTER(ModelDesc)), ("X", C.c_uint32), ("Y", C.c_uint32),
+        ("Z", C.c_uint32), ("particles", u32p), ("sites", u8p), ("seed", C.c_uint32), ("timesteps", C.c_uint32),
+    ]
+
+
+class ResultInfo(C.Structure):
+    _fields_ = [
+        ("id", C.c_uint64), ("stats", RunStats), ("X", C.c_uint32), ("Y", C.c_uint32), ("Z", C.c_uint32),
+        ("number_species", C.c_uint32), ("t_submit", C.c_double), ("t_admit", C.c_double),
+        ("t_done", C.c_double),
+    ]
+
+
+class ServerStatus(C.Structure):
+    _fields_ = [
+        ("active", C.c_uint32), ("queued", C.c_uint32), ("ready", C.c_uint32), ("peak_active", C.c_uint32),
+        ("bytes_in_use", C.c_uint64), ("peak_bytes", C.c_uint64), ("completed", C.c_uint64),
+        ("next_ready_words", C.c_uint64),
+    ]
+
+
 # name -> (restype, argtypes); kept in the order of include/lmb.h.
 PROTOTYPES = {
     "lmb_abi_version": (C.c_int, []),
@@ -106,7 +129,27 @@ PROTOTYPES = {
     "lmb_batch_run": (C.c_int, [vp, u32p, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(RunStats)]),
     "lmb_batch_run_async": (C.c_int, [vp, u32p, C.c_uint32, C.c_uint32, C.c_int]),
     "lmb_batch_wait": (C.c_int, [vp, C.POINTER(RunStats)]),
+    "lmb_batch_run_ranges_async": (C.c_int, [vp, u32p, u32p, u32p, C.c_int]),
+    "lmb_batch_set_lattices": (C.c_int, [vp, C.c_uint32, C.POINTER(vp), C.POINTER(vp)]),
     "lmb_batch_destroy": (C.c_int, [vp]),
+    "lmb_server_create": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
+                                    C.POINTER(vp)]),
+    "lmb_server_destroy": (C.c_int, [vp]),
+    "lmb_server_submit": (C.c_int, [vp, C.POINTER(Request)]),
+    "lmb_server_step": (C.c_int, [vp, u32p, u32p]),
+    "lmb_server_pop_result": (C.c_int, [vp, C.POINTER(ResultInfo), u32p, C.c_uint64, u64p, C.c_uint32]),
+    "lmb_server_status": (C.c_int, [vp, C.POINTER(ServerStatus)]),
+    "lmb_cme_create": (C.c_int, [vp, C.c_uint32, C.c_uint32, u32p, f64p, C.c_uint32, i32p, u32p, C.c_uint32,
+                                 C.POINTER(vp)]),
+    "lmb_cme_destroy": (C.c_int, [vp]),
+    "lmb_cme_set_initial_counts": (C.c_int, [vp, u32p, C.c_int]),
+    "lmb_cme_begin": (C.c_int, [vp, C.c_uint32, C.c_double, C.c_double]),
+    "lmb_cme_advance_async": (C.c_int, [vp, C.c_double]),
+    "lmb_cme_run": (C.c_int, [vp, C.c_uint32, C.c_double, C.c_double]),
+    "lmb_cme_entries": (C.c_int, [vp, u32p]),
+    "lmb_cme_get_counts": (C.c_int, [vp, u32p]),
+    "lmb_cme_device_counts": (C.c_int, [vp, C.POINTER(vp)]),
+    "lmb_cme_stats": (C.c_int, [vp, u64p, u32p]),
     "lmb_kernel_launches": (C.c_uint64, []),
 }
 

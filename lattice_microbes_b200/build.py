@@ -15,7 +15,7 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "liblmb200.so")
 
-SOURCES = ["lmb_kernels.cu", "lmb_fused.cu", "lmb_capi.cu", "lmb_noalloc.cu"]
+SOURCES = ["lmb_kernels.cu", "lmb_fused.cu", "lmb_capi.cu", "lmb_noalloc.cu", "lmb_cme.cu", "lmb_serve.cu"]
 HEADERS = ["lmb_internal.h", "lmb_device.cuh", "lmb_site.cuh", "lmb_overflow.cuh", "lmb_fused.h"]
 
 NVCC_FLAGS = [

@@ -429,6 +429,144 @@ def random_problem(seed, X=32, Y=16, Z=16, slots=8, bytes_per_slot=1, ns=6, nst=
                      K, S, Dm, DF, RL, lat, sites, steps)
 
 
+# --------------------------------------------------------------------------
+# Config 3 (CME part): two-state gene expression, well mixed
+# --------------------------------------------------------------------------
+
+@dataclass
+class CMESpec:
+    """A well-mixed model as CMESolver::buildModel receives it
+    (cme/CMESolver.h:200-201): reaction types, rate constants (one column),
+    species-major stoichiometry S[NS, R] and dependency D[NS, R], initial
+    counts."""
+    name: str
+    ns: int
+    rtype: np.ndarray          # [R] uint32
+    K: np.ndarray              # [R] float64
+    S: np.ndarray              # [NS, R] int32
+    D: np.ndarray              # [NS, R] uint32
+    init: np.ndarray           # [NS] uint32
+    max_time: float
+    write_interval: float
+    species_names: List[str] = field(default_factory=list)
+
+    @property
+    def nr(self):
+        return int(len(self.rtype))
+
+
+def two_state_gene(max_time=3600.0, write_interval=600.0):
+    """The two-state gene model of lm::cme::TwoStateExpression
+    (cme/TwoStateExpression.cpp:74-107): species gene-inactive, gene-active,
+    mRNA, protein; reactions activation, inactivation, transcription (active
+    gene -> + mRNA), translation (mRNA -> + protein), mRNA decay, protein
+    decay, all first order.  Rates (per second) lie in 0.01..10: activation
+    0.05, inactivation 0.2, transcription 2, translation 10, mRNA decay 0.5,
+    protein decay 0.01.  One inactive gene, no mRNA or protein at t = 0."""
+    S = np.array([[-1, 1, 0, 0, 0, 0],
+                  [1, -1, 0, 0, 0, 0],
+                  [0, 0, 1, 0, -1, 0],
+                  [0, 0, 0, 1, 0, -1]], dtype=np.int32)
+    D = np.array([[1, 0, 0, 0, 0, 0],
+                  [0, 1, 1, 0, 0, 0],
+                  [0, 0, 0, 1, 1, 0],
+                  [0, 0, 0, 0, 0, 1]], dtype=np.uint32)
+    rtype = np.full(6, FIRST, dtype=np.uint32)
+    K = np.array([0.05, 0.2, 2.0, 10.0, 0.5, 0.01])
+    init = np.array([1, 0, 0, 0], dtype=np.uint32)
+    return CMESpec("two-state-gene", 4, rtype, K, S, D, init, max_time, write_interval,
+                   ["gene_inactive", "gene_active", "mRNA", "protein"])
+
+
+# --------------------------------------------------------------------------
+# Config 4: serving stream of solve requests
+# --------------------------------------------------------------------------
+
+@dataclass
+class ServeRequest:
+    index: int
+    arrival: float      # seconds after the stream starts
+    edge: int
+    ns: int
+    density: float      # particles per site
+    timesteps: int
+    seed: int           # generator seed of the request's model and lattice
+
+
+def serve_stream(seed=4, count=1000, rate=50.0, edges=tuple(range(16, 129, 8)), ns_range=(2, 50),
+                 density_range=(0.5, 2.0), steps_range=(1000, 20000)):
+    """A seeded Poisson arrival stream of solve requests: exponential
+    inter-arrival times at `rate` per second, cubic lattice edge, species
+    count, particle density and timestep count drawn uniformly."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    out = []
+    for k in range(count):
+        out.append(ServeRequest(
+            index=k, arrival=float(t[k]), edge=int(rng.choice(edges)),
+            ns=int(rng.integers(ns_range[0], ns_range[1] + 1)),
+            density=float(rng.uniform(*density_range)),
+            timesteps=int(rng.integers(steps_range[0], steps_range[1] + 1)),
+            seed=int(rng.integers(1, 2 ** 31))))
+    return out
+
+
+def serve_problem(req, spacing=32e-9, tau=50e-6):
+    """The model and lattice of one serving request: `req.ns` species with
+    per-species D log-uniform in [1e-14, 5e-12] m^2/s, about one reaction per
+    species (first order 0.1..10 /s, second order 1e5..1e7 /M/s, no two
+    second-order reactions on the same pair), particles spread evenly over
+    the species at `req.density` per site, one site type, ByteLattice 8."""
+    rng = np.random.default_rng(req.seed)
+    X = Y = Z = req.edge
+    N = X * Y * Z
+    ns, nst = req.ns, 1
+    nr = ns
+    DF = np.exp(rng.uniform(np.log(1e-14), np.log(5e-12), size=ns)).reshape(1, 1, ns)
+    rtype = np.zeros(nr, dtype=np.uint32)
+    K = np.zeros(nr)
+    S = np.zeros((ns, nr), dtype=np.int32)
+    Dm = np.zeros((ns, nr), dtype=np.uint32)
+    pairs = set()
+    for j in range(nr):
+        if ns >= 2 and rng.random() < 0.5:
+            while True:
+                a, b = sorted(int(v) for v in rng.choice(ns, size=2, replace=False))
+                if (a, b) not in pairs or len(pairs) >= ns * (ns - 1) // 2:
+                    break
+            if (a, b) in pairs:
+                rtype[j] = FIRST
+                K[j] = float(np.exp(rng.uniform(np.log(0.1), np.log(10.0))))
+                S[a, j] -= 1
+                Dm[a, j] = 1
+            else:
+                pairs.add((a, b))
+                rtype[j] = SECOND
+                K[j] = lm_rate(float(np.exp(rng.uniform(np.log(1e5), np.log(1e7)))), 2, spacing, N)
+                S[a, j] -= 1
+                S[b, j] -= 1
+                Dm[a, j] = Dm[b, j] = 1
+        else:
+            a = int(rng.integers(ns))
+            rtype[j] = FIRST
+            K[j] = float(np.exp(rng.uniform(np.log(0.1), np.log(10.0))))
+            S[a, j] -= 1
+            Dm[a, j] = 1
+        S[int(rng.integers(ns)), j] += 1
+    RL = np.ones((nr, nst), dtype=np.uint32)
+    lat = empty_lattice(X, Y, Z, 8, 1)
+    sites = np.zeros(N, dtype=np.uint8)
+    total = int(round(req.density * N))
+    per = np.full(ns, total // ns)
+    per[: total - per.sum()] += 1
+    occ = None
+    for sp in range(ns):
+        if per[sp]:
+            occ = place_particles(lat, sites, X, Y, Z, 8, 1, sp + 1, int(per[sp]), 0, rng, occ)
+    return ModelSpec("serve-%d" % req.index, X, Y, Z, 8, 1, ns, nst, tau, spacing, rtype, K, S, Dm, DF, RL,
+                     lat, sites, req.timesteps)
+
+
 def batch_edges(seed=7, count=256, edges=(16, 24, 32, 48, 64)):
     rng = np.random.default_rng(seed)
     return [int(e) for e in rng.choice(edges, size=count)]

@@ -26,26 +26,6 @@ static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint64_t n) { g_launches += n; }
 }  // namespace lmb
 
-// A context lives until its handle and every model and lattice made from it
-// are destroyed, whatever the order of those calls.
-struct lmb_ctx {
-    int device;
-    cudaStream_t stream;
-    bool own_stream;
-    std::atomic<int> refs;
-};
-
-static void ctx_retain(lmb_ctx *c) { c->refs.fetch_add(1); }
-
-static void ctx_release(lmb_ctx *c)
-{
-    if (c->refs.fetch_sub(1) == 1) {
-        cudaSetDevice(c->device);
-        if (c->own_stream) cudaStreamDestroy(c->stream);
-        delete c;
-    }
-}
-
 struct lmb_model {
     lmb_ctx *ctx;
     uint32_t ns, nst, nr;
@@ -1093,10 +1073,14 @@ struct lmb_batch {
     std::vector<lmb_lattice *> lats;
     std::vector<const lmb_model *> models;
     int bps, slots;
-    // Device side: job table, run-state pointers, seeds, gathered states.
+    uint32_t capacity;  // lattices the device arrays hold
+    // Device side: job table, run-state pointers, seeds, per-lattice
+    // timestep ranges, gathered states.
     FusedJob *jobs;
     RunState **rs_ptrs;
     uint32_t *seeds;
+    uint32_t *firsts;
+    uint32_t *counts;
     RunState *states;
     RunState *states_host;  // pinned
     std::vector<FusedJob> jobs_host;
@@ -1106,66 +1090,132 @@ struct lmb_batch {
     cudaGraphExec_t graph;
     uint64_t graph_kernels;
     uint32_t graph_tiles;  // launch shape the graph was captured with
+    uint32_t graph_jobs;
     size_t graph_smem;
     bool pending;
-    uint32_t pending_first, pending_n;
+    std::vector<uint32_t> pending_first, pending_n;
     std::vector<int> cur0;
 };
 
 static const uint32_t BATCH_GRAPH_STEPS = 32;
 
-extern "C" int lmb_batch_create(lmb_ctx *c, uint32_t count, lmb_lattice *const *lattices,
-                                const lmb_model *const *models, lmb_batch **out)
+static void batch_free_arrays(lmb_batch *b)
 {
-    if (!c || !lattices || !models || !out || count == 0) return LMB_E_ARG;
-    *out = nullptr;
-    const int bps = (int)lattices[0]->bps, slots = (int)lattices[0]->slots;
+    if (b->jobs) cudaFree(b->jobs);
+    if (b->rs_ptrs) cudaFree(b->rs_ptrs);
+    if (b->seeds) cudaFree(b->seeds);
+    if (b->firsts) cudaFree(b->firsts);
+    if (b->counts) cudaFree(b->counts);
+    if (b->states) cudaFree(b->states);
+    if (b->states_host) cudaFreeHost(b->states_host);
+    b->jobs = nullptr;
+    b->rs_ptrs = nullptr;
+    b->seeds = b->firsts = b->counts = nullptr;
+    b->states = b->states_host = nullptr;
+    b->capacity = 0;
+}
+
+static int batch_reserve(lmb_batch *b, uint32_t count)
+{
+    if (count <= b->capacity) return LMB_OK;
+    CK(cudaStreamSynchronize(b->ctx->stream));
+    batch_free_arrays(b);
+    cudaError_t e = cudaMalloc(&b->jobs, sizeof(FusedJob) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->rs_ptrs, sizeof(RunState *) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->seeds, sizeof(uint32_t) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->firsts, sizeof(uint32_t) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->counts, sizeof(uint32_t) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&b->states, sizeof(RunState) * count);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->states_host, sizeof(RunState) * count);
+    if (e != cudaSuccess) {
+        batch_free_arrays(b);
+        return cuda_status(e);
+    }
+    b->capacity = count;
+    return LMB_OK;
+}
+
+// Checks and plans a member set; fills `plan`.
+static int batch_check_members(lmb_ctx *c, uint32_t count, lmb_lattice *const *lattices,
+                               const lmb_model *const *models, int bps, int slots, std::vector<TileShape> &plan)
+{
+    plan.resize(count);
     for (uint32_t j = 0; j < count; j++) {
         lmb_lattice *l = lattices[j];
         const lmb_model *m = models[j];
         if (!l || !m || l->ctx != c || m->ctx != c) return LMB_E_ARG;
         if ((int)l->bps != bps || (int)l->slots != slots) return LMB_E_ARG;
         if (m->has_desc && (m->X != l->g.X || m->Y != l->g.Y || m->Z != l->g.Z)) return LMB_E_ARG;
+        if (!fused_batch_shape(l->g, bps, slots, plan[j])) return LMB_E_UNSUPPORTED;
     }
-    std::vector<TileShape> plan(count);
-    for (uint32_t j = 0; j < count; j++)
-        if (!fused_batch_shape(lattices[j]->g, bps, slots, plan[j])) return LMB_E_UNSUPPORTED;
+    return LMB_OK;
+}
+
+static int batch_set(lmb_batch *b, uint32_t count, lmb_lattice *const *lattices, const lmb_model *const *models,
+                     std::vector<TileShape> &plan)
+{
+    int rc = batch_reserve(b, count);
+    if (rc) return rc;
+    b->lats.assign(lattices, lattices + count);
+    b->models.assign(models, models + count);
+    b->tiles.swap(plan);
+    std::vector<RunState *> ptrs(count);
+    for (uint32_t j = 0; j < count; j++) ptrs[j] = lattices[j]->rs;
+    CK(cudaMemcpyAsync(b->rs_ptrs, ptrs.data(), sizeof(RunState *) * count, cudaMemcpyHostToDevice,
+                       b->ctx->stream));
+    CK(cudaStreamSynchronize(b->ctx->stream));
+    return LMB_OK;
+}
+
+extern "C" int lmb_batch_create(lmb_ctx *c, uint32_t count, lmb_lattice *const *lattices,
+                                const lmb_model *const *models, lmb_batch **out)
+{
+    if (!c || !lattices || !models || !out || count == 0 || !lattices[0]) return LMB_E_ARG;
+    *out = nullptr;
+    const int bps = (int)lattices[0]->bps, slots = (int)lattices[0]->slots;
+    std::vector<TileShape> plan;
+    int rc = batch_check_members(c, count, lattices, models, bps, slots, plan);
+    if (rc) return rc;
     CK(cudaSetDevice(c->device));
     lmb_batch *b = new (std::nothrow) lmb_batch;
     if (!b) return LMB_E_NOMEM;
     b->ctx = c;
     ctx_retain(c);
-    b->lats.assign(lattices, lattices + count);
-    b->models.assign(models, models + count);
-    b->tiles = plan;
     b->bps = bps;
     b->slots = slots;
+    b->capacity = 0;
     b->jobs = nullptr;
     b->rs_ptrs = nullptr;
-    b->seeds = nullptr;
+    b->seeds = b->firsts = b->counts = nullptr;
     b->states = nullptr;
     b->states_host = nullptr;
     b->graph = nullptr;
     b->graph_kernels = 0;
     b->graph_tiles = 0;
+    b->graph_jobs = 0;
     b->graph_smem = 0;
     b->pending = false;
     b->total_tiles = 0;
     b->smem = 0;
-    cudaError_t e = cudaMalloc(&b->jobs, sizeof(FusedJob) * count);
-    if (e == cudaSuccess) e = cudaMalloc(&b->rs_ptrs, sizeof(RunState *) * count);
-    if (e == cudaSuccess) e = cudaMalloc(&b->seeds, sizeof(uint32_t) * count);
-    if (e == cudaSuccess) e = cudaMalloc(&b->states, sizeof(RunState) * count);
-    if (e == cudaSuccess) e = cudaMallocHost(&b->states_host, sizeof(RunState) * count);
-    std::vector<RunState *> ptrs(count);
-    for (uint32_t j = 0; j < count; j++) ptrs[j] = lattices[j]->rs;
-    if (e == cudaSuccess) e = cudaMemcpy(b->rs_ptrs, ptrs.data(), sizeof(RunState *) * count, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
+    rc = batch_set(b, count, lattices, models, plan);
+    if (rc) {
         lmb_batch_destroy(b);
-        return cuda_status(e);
+        return rc;
     }
     *out = b;
     return LMB_OK;
+}
+
+extern "C" int lmb_batch_set_lattices(lmb_batch *b, uint32_t count, lmb_lattice *const *lattices,
+                                      const lmb_model *const *models)
+{
+    if (!b || !lattices || !models || count == 0) return LMB_E_ARG;
+    if (b->pending) return LMB_E_STATE;
+    std::vector<TileShape> plan;
+    int rc = batch_check_members(b->ctx, count, lattices, models, b->bps, b->slots, plan);
+    if (rc) return rc;
+    CK(cudaSetDevice(b->ctx->device));
+    return batch_set(b, count, lattices, models, plan);
 }
 
 extern "C" int lmb_batch_destroy(lmb_batch *b)
@@ -1174,11 +1224,7 @@ extern "C" int lmb_batch_destroy(lmb_batch *b)
     cudaSetDevice(b->ctx->device);
     cudaStreamSynchronize(b->ctx->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    if (b->jobs) cudaFree(b->jobs);
-    if (b->rs_ptrs) cudaFree(b->rs_ptrs);
-    if (b->seeds) cudaFree(b->seeds);
-    if (b->states) cudaFree(b->states);
-    if (b->states_host) cudaFreeHost(b->states_host);
+    batch_free_arrays(b);
     lmb_ctx *c = b->ctx;
     delete b;
     ctx_release(c);
@@ -1228,7 +1274,12 @@ static int batch_prepare(lmb_batch *b)
     return LMB_OK;
 }
 
-extern "C" int lmb_batch_run_async(lmb_batch *b, const uint32_t *seeds, uint32_t first, uint32_t n, int mode)
+// Queues a batch run: lattice j advances through timesteps firsts[j] ..
+// firsts[j] + counts[j] - 1 (or first .. first + n - 1 for all when the
+// arrays are null); the launch count is the longest range, and a lattice
+// whose range is done sits out the remaining launches.
+static int batch_run(lmb_batch *b, const uint32_t *seeds, uint32_t first, uint32_t n, const uint32_t *firsts,
+                     const uint32_t *counts, int mode)
 {
     if (!b || !seeds) return LMB_E_ARG;
     if (b->pending) return LMB_E_STATE;
@@ -1238,15 +1289,29 @@ extern "C" int lmb_batch_run_async(lmb_batch *b, const uint32_t *seeds, uint32_t
     int rc = batch_prepare(b);
     if (rc) return rc;
     const uint32_t count = (uint32_t)b->lats.size();
+    b->pending_first.assign(count, first);
+    b->pending_n.assign(count, n);
+    uint32_t launches = n;
+    if (firsts && counts) {
+        launches = 0;
+        for (uint32_t j = 0; j < count; j++) {
+            b->pending_first[j] = firsts[j];
+            b->pending_n[j] = counts[j];
+            if (counts[j] > launches) launches = counts[j];
+        }
+        CK(cudaMemcpyAsync(b->firsts, firsts, sizeof(uint32_t) * count, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(b->counts, counts, sizeof(uint32_t) * count, cudaMemcpyHostToDevice, c->stream));
+    }
     CK(cudaMemcpyAsync(b->seeds, seeds, sizeof(uint32_t) * count, cudaMemcpyHostToDevice, c->stream));
-    CK(launch_begin_batch(b->rs_ptrs, b->seeds, count, first, n, (uint32_t)mode, c->stream));
+    CK(launch_begin_batch(b->rs_ptrs, b->seeds, count, first, n, firsts && counts ? b->firsts : nullptr,
+                          firsts && counts ? b->counts : nullptr, (uint32_t)mode, c->stream));
     uint32_t done = 0;
-    if (n >= 2 * BATCH_GRAPH_STEPS) {
+    if (launches >= 2 * BATCH_GRAPH_STEPS) {
         // One graph of BATCH_GRAPH_STEPS launches (parities 0, 1, ...) serves
         // every run: the job table it reads is rewritten before each run.
         static_assert(BATCH_GRAPH_STEPS % 2 == 0, "graph must return to parity 0");
-        if (b->graph && (b->graph_tiles != b->total_tiles || b->graph_smem != b->smem)) {
-            cudaGraphExecDestroy(b->graph);  // a lattice changed its tile plan
+        if (b->graph && (b->graph_tiles != b->total_tiles || b->graph_smem != b->smem || b->graph_jobs != count)) {
+            cudaGraphExecDestroy(b->graph);  // the member set or a tile plan changed
             b->graph = nullptr;
         }
         if (!b->graph) {
@@ -1262,6 +1327,7 @@ extern "C" int lmb_batch_run_async(lmb_batch *b, const uint32_t *seeds, uint32_t
                 if (e == cudaSuccess && e2 == cudaSuccess && cudaGraphInstantiate(&b->graph, graph, 0) == cudaSuccess) {
                     b->graph_kernels = captured;
                     b->graph_tiles = b->total_tiles;
+                    b->graph_jobs = count;
                     b->graph_smem = b->smem;
                 } else {
                     b->graph = nullptr;
@@ -1272,21 +1338,31 @@ extern "C" int lmb_batch_run_async(lmb_batch *b, const uint32_t *seeds, uint32_t
             }
         }
         if (b->graph) {
-            for (; done + BATCH_GRAPH_STEPS <= n; done += BATCH_GRAPH_STEPS) {
+            for (; done + BATCH_GRAPH_STEPS <= launches; done += BATCH_GRAPH_STEPS) {
                 CK(cudaGraphLaunch(b->graph, c->stream));
                 count_launch(b->graph_kernels);
             }
         }
     }
-    for (; done < n; done++)
+    for (; done < launches; done++)
         CK(launch_fused_batch(b->bps, b->slots, b->jobs, count, b->total_tiles, b->smem, done & 1u, c->stream));
     CK(launch_gather_states(b->rs_ptrs, count, b->states, c->stream));
     CK(cudaMemcpyAsync(b->states_host, b->states, sizeof(RunState) * count, cudaMemcpyDeviceToHost, c->stream));
     b->pending = true;
-    b->pending_first = first;
-    b->pending_n = n;
     for (lmb_lattice *l : b->lats) l->pending = true;
     return LMB_OK;
+}
+
+extern "C" int lmb_batch_run_async(lmb_batch *b, const uint32_t *seeds, uint32_t first, uint32_t n, int mode)
+{
+    return batch_run(b, seeds, first, n, nullptr, nullptr, mode);
+}
+
+extern "C" int lmb_batch_run_ranges_async(lmb_batch *b, const uint32_t *seeds, const uint32_t *firsts,
+                                          const uint32_t *counts, int mode)
+{
+    if (!firsts || !counts) return LMB_E_ARG;
+    return batch_run(b, seeds, 0, 0, firsts, counts, mode);
 }
 
 extern "C" int lmb_batch_wait(lmb_batch *b, lmb_run_stats *stats)
@@ -1302,7 +1378,7 @@ extern "C" int lmb_batch_wait(lmb_batch *b, lmb_run_stats *stats)
     for (size_t j = 0; j < b->lats.size(); j++) {
         const RunState &h = b->states_host[j];
         lmb_lattice *l = b->lats[j];
-        const uint32_t done = h.status == LMB_OK ? b->pending_n : h.failed_step - b->pending_first;
+        const uint32_t done = h.status == LMB_OK ? b->pending_n[j] : h.failed_step - b->pending_first[j];
         l->cur = b->cur0[j] ^ (int)((h.status == LMB_OK ? done : done + 1) & 1u);
         if (stats) {
             stats[j].status = h.status;

@@ -147,7 +147,9 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     __shared__ uint16_t yrow[FUSED_MAX_ROWS], zrow[FUSED_MAX_ROWS];
     __shared__ uint8_t rowflag[FUSED_MAX_ROWS];
     constexpr int W = SiteWords<BPS, S>::W;
-    if (rs->status != LMB_OK) return;
+    // A failed run stops; in a batch, a lattice whose own timestep range is
+    // done sits out the remaining launches.
+    if (rs->status != LMB_OK || rs->step >= rs->end_step) return;
     const uint32_t X = g.X, R = ts.R, Ry = ts.Ry, Ty = ts.Ty, Tz = ts.Tz, MW = ts.MW;
     const uint32_t tyi = tile % ts.tiles_y, tzi = tile / ts.tiles_y;
     const uint32_t y0 = tyi * Ty, z0 = tzi * Tz;

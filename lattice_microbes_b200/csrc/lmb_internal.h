@@ -4,6 +4,29 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
+// A context: one device and one stream.  It lives until its handle and every
+// model, lattice, batch and CME ensemble made from it are destroyed, whatever
+// the order of those calls.
+struct lmb_ctx {
+    int device;
+    cudaStream_t stream;
+    bool own_stream;
+    std::atomic<int> refs;
+};
+
+static inline void ctx_retain(lmb_ctx *c) { c->refs.fetch_add(1); }
+
+static inline void ctx_release(lmb_ctx *c)
+{
+    if (c->refs.fetch_sub(1) == 1) {
+        cudaSetDevice(c->device);
+        if (c->own_stream) cudaStreamDestroy(c->stream);
+        delete c;
+    }
+}
+
 namespace lmb {
 
 // Lattice geometry; site i = x + y*X + z*X*Y.
@@ -73,7 +96,8 @@ cudaError_t launch_resolve(int bytes_per_slot, int slots, uint32_t *lat, const u
 cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
                              cudaStream_t stream);
 cudaError_t launch_begin_batch(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,
-                               uint32_t n, uint32_t mode, cudaStream_t stream);
+                               uint32_t n, const uint32_t *firsts, const uint32_t *counts, uint32_t mode,
+                               cudaStream_t stream);
 cudaError_t launch_gather_states(RunState *const *rs_ptrs, uint32_t count, RunState *out, cudaStream_t stream);
 cudaError_t launch_counts(int bytes_per_slot, int slots, const uint32_t *lat, const Geometry &g,
                           uint32_t ns, unsigned long long *counts, cudaStream_t stream);

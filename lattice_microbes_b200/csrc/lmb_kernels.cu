@@ -125,15 +125,18 @@ __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, ui
 }
 
 // Batch forms: run state j lives at *rs_ptrs[j]; seeds[j] is its seed.
+// Run state of every lattice of a batch: timesteps first .. first + n - 1, or
+// per-lattice ranges firsts[j] / counts[j] when those arrays are given.
 __global__ void begin_batch_kernel(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,
-                                   uint32_t n, uint32_t mode)
+                                   uint32_t n, const uint32_t *firsts, const uint32_t *counts, uint32_t mode)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
     RunState *rs = rs_ptrs[j];
+    const uint32_t f = firsts ? firsts[j] : first;
     rs->seed = seeds[j];
-    rs->step = first;
-    rs->end_step = first + n;
+    rs->step = f;
+    rs->end_step = f + (counts ? counts[j] : n);
     rs->status = LMB_OK;
     rs->failed_step = 0;
     rs->mode = mode;
@@ -153,10 +156,12 @@ __global__ void gather_states_kernel(RunState *const *rs_ptrs, uint32_t count, R
 }
 
 cudaError_t launch_begin_batch(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,
-                               uint32_t n, uint32_t mode, cudaStream_t stream)
+                               uint32_t n, const uint32_t *firsts, const uint32_t *counts, uint32_t mode,
+                               cudaStream_t stream)
 {
     count_launch();
-    begin_batch_kernel<<<(count + 127) / 128, 128, 0, stream>>>(rs_ptrs, seeds, count, first, n, mode);
+    begin_batch_kernel<<<(count + 127) / 128, 128, 0, stream>>>(rs_ptrs, seeds, count, first, n, firsts, counts,
+                                                                mode);
     return cudaGetLastError();
 }
 

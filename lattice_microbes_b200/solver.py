@@ -279,9 +279,182 @@ class Batch:
             L.check(rc, "lmb_batch_wait")
         return rc, list(stats)
 
+    def run_ranges_async(self, seeds, firsts, counts, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
+        """Lattice j runs timesteps firsts[j] .. firsts[j] + counts[j] - 1."""
+        self._seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        self._firsts = np.ascontiguousarray(firsts, dtype=np.uint32)
+        self._counts = np.ascontiguousarray(counts, dtype=np.uint32)
+        L.check(L.lib().lmb_batch_run_ranges_async(self.handle, _p(self._seeds, L.u32p), _p(self._firsts, L.u32p),
+                                                   _p(self._counts, L.u32p), overflow_mode),
+                "lmb_batch_run_ranges_async")
+
+    def set_lattices(self, lattices, models):
+        n = len(lattices)
+        la = (L.vp * n)(*[l.handle for l in lattices])
+        mo = (L.vp * n)(*[m.handle for m in models])
+        L.check(L.lib().lmb_batch_set_lattices(self.handle, n, la, mo), "lmb_batch_set_lattices")
+        self.lattices, self.models = list(lattices), list(models)
+
     def close(self):
         if self.handle:
             L.lib().lmb_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _model_desc(spec):
+    """lmb_model_desc for a ModelSpec-like object; returns (desc, arrays to keep alive)."""
+    ns, nst, nr = spec.ns, spec.nst, spec.nr
+    keep = dict(
+        rtype=np.ascontiguousarray(spec.rtype, dtype=np.uint32) if nr else np.zeros(1, np.uint32),
+        K=np.ascontiguousarray(spec.K, dtype=np.float64) if nr else np.zeros(1),
+        S=np.ascontiguousarray(spec.S, dtype=np.int32).reshape(-1) if nr else np.zeros(1, np.int32),
+        D=np.ascontiguousarray(spec.D, dtype=np.uint32).reshape(-1) if nr else np.zeros(1, np.uint32),
+        DF=np.ascontiguousarray(spec.DF, dtype=np.float64).reshape(-1),
+        RL=np.ascontiguousarray(spec.RL, dtype=np.uint32).reshape(-1) if nr else np.zeros(1, np.uint32),
+    )
+    d = L.ModelDesc()
+    d.number_species, d.number_reactions, d.number_site_types = ns, nr, nst
+    d.reaction_types = _p(keep["rtype"], L.u32p)
+    d.K = _p(keep["K"], L.f64p)
+    d.k_cols = 1
+    d.S = _p(keep["S"], L.i32p)
+    d.D = _p(keep["D"], L.u32p)
+    d.DF = _p(keep["DF"], L.f64p)
+    d.RL = _p(keep["RL"], L.u32p)
+    d.timestep = spec.tau
+    d.lattice_spacing = spec.spacing
+    return d, keep
+
+
+class Server:
+    """Continuous batching of MPD-RDME solves (lmb_server): admitted solves
+    stay resident on the device and advance together, one launch per
+    timestep for all of them; admission is in arrival order under a slot
+    count and a device-memory budget."""
+
+    def __init__(self, ctx, slots=8, bytes_per_slot=1, hbm_budget_bytes=150 << 30, max_active=256,
+                 chunk_timesteps=256):
+        h = L.vp()
+        L.check(L.lib().lmb_server_create(ctx.handle, slots, bytes_per_slot, hbm_budget_bytes, max_active,
+                                          chunk_timesteps, C.byref(h)), "lmb_server_create")
+        self.ctx, self.handle = ctx, h
+        self.words_per_site = slots // 4 if bytes_per_slot == 1 else slots
+
+    def submit(self, request_id, spec, seed, timesteps, lattice=None, sites=None):
+        """Queues a solve of `spec` (ModelSpec-like; its lattice and site types
+        unless given) for `timesteps` timesteps with the composed `seed`."""
+        d, keep = _model_desc(spec)
+        lat = np.ascontiguousarray(spec.lattice if lattice is None else lattice, dtype=np.uint32)
+        st = np.ascontiguousarray(spec.sites if sites is None else sites, dtype=np.uint8)
+        r = L.Request()
+        r.id = request_id
+        r.model = C.pointer(d)
+        r.X, r.Y, r.Z = spec.X, spec.Y, spec.Z
+        r.particles = _p(lat, L.u32p)
+        r.sites = _p(st, L.u8p)
+        r.seed = seed
+        r.timesteps = timesteps
+        L.check(L.lib().lmb_server_submit(self.handle, C.byref(r)), "lmb_server_submit")
+
+    def step(self):
+        a, q = C.c_uint32(), C.c_uint32()
+        L.check(L.lib().lmb_server_step(self.handle, C.byref(a), C.byref(q)), "lmb_server_step")
+        return a.value, q.value
+
+    def status(self):
+        st = L.ServerStatus()
+        L.check(L.lib().lmb_server_status(self.handle, C.byref(st)))
+        return st
+
+    def pop_result(self, with_lattice=True):
+        """(info, native lattice or None, species counts) of the oldest
+        finished solve, or None."""
+        st = self.status()
+        if st.ready == 0:
+            return None
+        info = L.ResultInfo()
+        lat = np.zeros(max(1, st.next_ready_words), dtype=np.uint32) if with_lattice else None
+        counts = np.zeros(4096, dtype=np.uint64)
+        L.check(L.lib().lmb_server_pop_result(self.handle, C.byref(info), _p(lat, L.u32p) if with_lattice else None,
+                                              lat.size if with_lattice else 0, _p(counts, L.u64p), counts.size))
+        n = info.number_species + 1
+        return info, (lat[:st.next_ready_words] if with_lattice else None), counts[:n].copy()
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.lib().lmb_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CMEEnsemble:
+    """Independent replicates of a well-mixed model advanced by the direct
+    method (lmb_cme), the GPU form of running one GillespieDSolver per
+    replicate.  ``spec`` is a configs.CMESpec or any object with ns, rtype,
+    K, S, D, init."""
+
+    def __init__(self, ctx, spec, replicates):
+        self.ctx, self.ns, self.replicates = ctx, spec.ns, replicates
+        nr = len(spec.rtype)
+        self._keep = dict(
+            rtype=np.ascontiguousarray(spec.rtype, dtype=np.uint32),
+            K=np.ascontiguousarray(spec.K, dtype=np.float64).reshape(-1),
+            S=np.ascontiguousarray(spec.S, dtype=np.int32).reshape(-1),
+            D=np.ascontiguousarray(spec.D, dtype=np.uint32).reshape(-1),
+        )
+        kcols = self._keep["K"].size // nr
+        h = L.vp()
+        L.check(L.lib().lmb_cme_create(ctx.handle, spec.ns, nr, _p(self._keep["rtype"], L.u32p),
+                                       _p(self._keep["K"], L.f64p), kcols, _p(self._keep["S"], L.i32p),
+                                       _p(self._keep["D"], L.u32p), replicates, C.byref(h)), "lmb_cme_create")
+        self.handle = h
+        self.set_initial_counts(spec.init)
+
+    def set_initial_counts(self, counts):
+        c = np.ascontiguousarray(counts, dtype=np.uint32)
+        per = 1 if c.ndim == 2 else 0
+        L.check(L.lib().lmb_cme_set_initial_counts(self.handle, _p(c, L.u32p), per))
+
+    def run(self, seed, t_end, write_interval):
+        L.check(L.lib().lmb_cme_run(self.handle, seed, t_end, write_interval), "lmb_cme_run")
+
+    def begin(self, seed, t_end, write_interval):
+        L.check(L.lib().lmb_cme_begin(self.handle, seed, t_end, write_interval))
+
+    def advance_async(self, until):
+        L.check(L.lib().lmb_cme_advance_async(self.handle, until))
+
+    def entries(self):
+        n = C.c_uint32()
+        L.check(L.lib().lmb_cme_entries(self.handle, C.byref(n)))
+        return n.value
+
+    def counts(self):
+        """[replicates, entries, species] uint32."""
+        out = np.zeros((self.replicates, self.entries(), self.ns), dtype=np.uint32)
+        L.check(L.lib().lmb_cme_get_counts(self.handle, _p(out, L.u32p)))
+        return out
+
+    def stats(self):
+        ev = C.c_uint64()
+        fin = C.c_uint32()
+        L.check(L.lib().lmb_cme_stats(self.handle, C.byref(ev), C.byref(fin)))
+        return ev.value, fin.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.lib().lmb_cme_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
