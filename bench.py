@@ -1,11 +1,14 @@
 #!/usr/bin/env python
 """MPD-RDME throughput on the rod-cell oscillator workload (B200).
 
-One bench step = TIMESTEPS_PER_STEP MPD timesteps (x, y, z sweeps, reaction,
-overflow handling) of the 64x64x128 rod-cell model (16 nm, 3 site types,
-5 species, 8 reactions, 4000 D + 1400 E, ByteLattice 8 slots, tau = 25 us),
-a segment of that model's 50,000-timestep trajectory.  Inputs are seeded and
-synthetic (lattice_microbes_b200.configs.config1).
+One bench step = 500 MPD timesteps (x, y, z sweeps, reaction, overflow
+handling) of the 64x64x128 rod-cell model (16 nm, 3 site types, 5 species,
+8 reactions, 4000 D + 1400 E, ByteLattice 8 slots, tau = 25 us), a segment
+of that model's 50,000-timestep trajectory.  Inputs are seeded and synthetic
+(lattice_microbes_b200.configs.config1).  --workload crowded runs the
+128x128x256 IntLattice-16 crowded cell (configs.config2) the same way, 40
+timesteps per bench step; --workload batch / cme / serve run the batched,
+CME-ensemble and serving forms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -34,12 +37,38 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-TIMESTEPS_PER_STEP = 500
-WORKLOAD = "rod-cell 64x64x128 ByteLattice-8, 3 site types, 5 species, 8 reactions, 5400 particles"
 METRIC = "site-steps/s"
-B_SWEEP = 2 * 8 * 1 + 1       # bytes per site per sweep, Byte-8 (read + write 8 slots, read site type)
-B_STEP = 7 * 8 * 1 + 4        # bytes per site-step on the reference schedule
 L2_FLUSH_BYTES = 256 << 20    # larger than the 126 MB L2
+
+# Single-lattice workloads.  S slots of b bytes per site: the reference
+# schedule moves B_sweep = 2 S b + 1 bytes per site per sweep and
+# B_step = 7 S b + 4 per site-step (three sweeps + the reaction read).
+WORKLOADS = {
+    "rodcell": dict(
+        desc="rod-cell 64x64x128 ByteLattice-8, 3 site types, 5 species, 8 reactions, 5400 particles",
+        config="config1", S=8, b=1, tau=25e-6, dtype="u8", timesteps_per_step=500, ref_timesteps=1000,
+        nsm_time=0.04, ref_mpd_timesteps=60,
+        l2="flushed between timed steps (256 MB write); working set 9 MB is L2-resident within a step"),
+    "crowded": dict(
+        desc="crowded cell 128x128x256 IntLattice-16, 8 site types (20% obstacles), 200 species, "
+             "500 reactions, 1M particles",
+        config="config2", S=16, b=4, tau=10e-6, dtype="u32", timesteps_per_step=40, ref_timesteps=100,
+        nsm_time=2e-4, ref_mpd_timesteps=2,
+        l2="inputs larger than L2: 537 MB of particle buffers + 4 MB site types per timestep"),
+}
+
+
+def make_spec(workload, seed):
+    from lattice_microbes_b200 import configs
+    return getattr(configs, WORKLOADS[workload]["config"])(seed=seed)
+
+
+def b_sweep(w):
+    return 2 * w["S"] * w["b"] + 1
+
+
+def b_step(w):
+    return 7 * w["S"] * w["b"] + 4
 
 
 def parse():
@@ -48,7 +77,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--timesteps-per-step", type=int, default=TIMESTEPS_PER_STEP)
+    ap.add_argument("--timesteps-per-step", type=int, default=0, help="0 = the workload's default")
     ap.add_argument("--cpu-sample-timesteps", type=int, default=0,
                     help="timesteps per core of the reference MPD functions on the host (0 = auto)")
     ap.add_argument("--cpu-sample-time", type=float, default=0.0,
@@ -58,8 +87,9 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
-    ap.add_argument("--workload", choices=["rodcell", "batch", "cme", "serve"], default="rodcell",
-                    help="rodcell: one 64x64x128 lattice (default); batch: 256 bimolecular replicates of "
+    ap.add_argument("--workload", choices=["rodcell", "crowded", "batch", "cme", "serve"], default="rodcell",
+                    help="rodcell: one 64x64x128 lattice (default); crowded: one 128x128x256 IntLattice-16; "
+                         "batch: 256 bimolecular replicates of "
                          "uneven size in one launch per timestep; cme: 65,536 two-state gene replicates "
                          "(direct method) to t = 3600 s; serve: a Poisson stream of solve requests")
     ap.add_argument("--replicates", type=int, default=0, help="batch: 256, cme: 65536 (0 = default)")
@@ -73,68 +103,81 @@ def parse():
 
 def _cpu_worker(args):
     """One replicate of the reference MPD device functions on one core (spawned)."""
-    seed, timesteps = args
+    workload, seed, timesteps = args
     sys.path.insert(0, ROOT)
-    from lattice_microbes_b200 import configs
     from tests.cases import oracle_tables
     from tests.oracle_lib import reference_run
-    spec = configs.config1(seed=seed)
+    spec = make_spec(workload, seed)
     t = oracle_tables(spec)
     t0 = time.perf_counter()
     r = reference_run(t, spec.lattice, spec.sites, 1000 + seed, 0, timesteps)
     dt = time.perf_counter() - t0
     if r is None:
         return None
-    return dt, int(r[1])
+    return dt, int(r[1]), spec.nsites
 
 
-def cpu_reference_sample(timesteps, cores):
+def cpu_reference_sample(workload, timesteps, cores):
     """Reference MPD device functions, `cores` replicates in parallel;
     returns (site-steps/s, sample)."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        res = pool.map(_cpu_worker, [(s, timesteps) for s in range(cores)])
+        res = pool.map(_cpu_worker, [(workload, s, timesteps) for s in range(cores)])
     if any(r is None for r in res):
         return None, "reference checker not built (oracle/_ref)"
     wall = max(r[0] for r in res)
-    nsites = 64 * 64 * 128
-    value = nsites * timesteps * cores / wall
-    sample = ("%d replicates x %d timesteps of the rod-cell workload, one per core, reference device "
-              "functions compiled for the host; %.1f s wall" % (cores, timesteps, wall))
+    value = res[0][2] * timesteps * cores / wall
+    sample = ("%d replicates x %d timesteps of the %s workload, one per core, reference device "
+              "functions compiled for the host; %.1f s wall" % (cores, timesteps, workload, wall))
     return value, sample
+
+
+def _byte_lattice(spec):
+    """The spec's particles in a ByteLattice with the same slot count (the
+    reference NextSubvolumeSolver runs ByteLattices only; ids <= 255)."""
+    import numpy as np
+    from lattice_microbes_b200 import configs
+    if spec.bytes_per_slot == 1:
+        return spec
+    N = spec.nsites
+    slots = configs.native_to_slots(spec.lattice, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+    lat = configs.empty_lattice(spec.X, spec.Y, spec.Z, spec.slots, 1)
+    for k in range(spec.slots):
+        lat[(k // 4) * N:(k // 4 + 1) * N] |= slots[:, k].astype(np.uint32) << np.uint32(8 * (k % 4))
+    spec.lattice, spec.bytes_per_slot = lat, 1
+    return spec
 
 
 def _nsm_worker(args):
     """One replicate of the reference NextSubvolumeSolver on one core (spawned)."""
-    seed, sim_time = args
+    workload, seed, sim_time = args
     sys.path.insert(0, ROOT)
-    from lattice_microbes_b200 import configs
     from tests import ref_cpu_lib
     if not ref_cpu_lib.available():
         return None
-    spec = configs.config1(seed=seed)
+    spec = _byte_lattice(make_spec(workload, seed))
     t0 = time.perf_counter()
     ref_cpu_lib.nsm_run(spec, 1000 + seed, seed + 1, sim_time, sim_time / 4)
-    return time.perf_counter() - t0
+    return time.perf_counter() - t0, spec.nsites
 
 
-def cpu_nsm_sample(sim_time, cores):
-    """Reference NextSubvolumeSolver, `cores` replicates of the rod-cell
-    workload in parallel, each to `sim_time` seconds; returns (site-steps/s,
-    sample) with site-steps = sites x sim_time / tau per replicate."""
+def cpu_nsm_sample(workload, sim_time, cores):
+    """Reference NextSubvolumeSolver, `cores` replicates of the workload in
+    parallel, each to `sim_time` seconds; returns (site-steps/s, sample) with
+    site-steps = sites x sim_time / tau per replicate."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        res = pool.map(_nsm_worker, [(s, sim_time) for s in range(cores)])
+        res = pool.map(_nsm_worker, [(workload, s, sim_time) for s in range(cores)])
     if any(r is None for r in res):
         return None, "reference CPU solvers not built (oracle/_ref)"
-    wall = max(res)
-    nsites, tau = 64 * 64 * 128, 25e-6
-    value = nsites * (sim_time / tau) * cores / wall
-    sample = ("%d replicates of the rod-cell workload, one per core, each %.4g s of simulated time (%d "
+    wall = max(r[0] for r in res)
+    tau = WORKLOADS[workload]["tau"]
+    value = res[0][1] * (sim_time / tau) * cores / wall
+    sample = ("%d replicates of the %s workload, one per core, each %.4g s of simulated time (%d "
               "MPD-timestep equivalents), reference NextSubvolumeSolver built from its sources; %.1f s wall"
-              % (cores, sim_time, round(sim_time / tau), wall))
+              % (cores, workload, sim_time, round(sim_time / tau), wall))
     return value, sample
 
 
@@ -210,11 +253,13 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+def ncu_traffic_per_launch(workload, kernel):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summary (profiles/traffic.json), if any."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        return d.get("kernel_dram_bytes_per_launch") if d.get("kernel", "").startswith(kernel) else None
+        e = d.get(workload) or {}
+        return e.get("kernel_dram_bytes_per_launch") if e.get("kernel", "").startswith(kernel) else None
     except Exception:
         return None
 
@@ -238,23 +283,25 @@ def run_ours(a):
     torch.cuda.set_device(device)
 
     # CPU baseline first (spawned workers, before any GPU work on this rank).
+    w = WORKLOADS[a.workload]
     cpu = None
     cpu_mpd = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = host_cores()
-        val, sample = cpu_nsm_sample(a.cpu_sample_time or 0.04, cores)
+        val, sample = cpu_nsm_sample(a.workload, a.cpu_sample_time or w["nsm_time"], cores)
         if val is not None:
             cpu = {"value": val, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample}
-        val, sample = cpu_reference_sample(a.cpu_sample_timesteps or 60, cores)
+        val, sample = cpu_reference_sample(a.workload, a.cpu_sample_timesteps or w["ref_mpd_timesteps"], cores)
         if val is not None:
             cpu_mpd = {"value": val, "unit": METRIC, "cores": cores, "sample": sample}
 
     from lattice_microbes_b200 import configs
     from lattice_microbes_b200.solver import Context, Lattice, Model, compose_seed, kernel_launches
 
-    T = a.timesteps_per_step
-    spec = configs.config1(seed=1 + rank)
+    T = a.timesteps_per_step or w["timesteps_per_step"]
+    spec = make_spec(a.workload, 1 + rank)
     N = spec.nsites
+    B_SWEEP, B_STEP = b_sweep(w), b_step(w)
     ctx = Context(device)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", device))
     model = Model.from_spec(ctx, spec)
@@ -270,9 +317,10 @@ def run_ours(a):
         try:
             from tests.cases import oracle_tables
             from tests.oracle_lib import reference_gpu_time
-            r = reference_gpu_time(oracle_tables(spec), spec.lattice, spec.sites, seed, 0, 1000)
+            nref = w["ref_timesteps"]
+            r = reference_gpu_time(oracle_tables(spec), spec.lattice, spec.sites, seed, 0, nref)
             if r is not None and r[0] == 0:
-                ref_gpu = {"value": N * 1000 / (r[1] / 1e3), "unit": METRIC, "timesteps": 1000,
+                ref_gpu = {"value": N * nref / (r[1] / 1e3), "unit": METRIC, "timesteps": nref,
                            "what": "reference device functions built for sm_100a, reference host loop "
                                    "(4 launches + stream sync + overflow check per timestep)"}
         except Exception as e:  # checker absent: report why
@@ -339,7 +387,7 @@ def run_ours(a):
         kern = "fused_step_kernel (x, y, z sweeps + reaction + overflow, one timestep)"
         launch_ms = float(phase_ms[5]) / int(phase_n[5])
         alg_bytes = N * B_STEP                 # site-steps per launch x per-site-step bytes
-        own_bytes = N * (2 * 8 + 1)            # its own dataflow: read slots + site type, write slots
+        own_bytes = N * B_SWEEP                # its own dataflow: read slots + site type, write slots
     else:
         kern = "sweep_kernel (x/y/z hop sweeps)"
         launch_ms = float(phase_ms[:3].sum()) / max(1, int(phase_n[:3].sum()))
@@ -383,16 +431,16 @@ def run_ours(a):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "u8",
-            "data": "synthetic (seeded rod-cell model, lattice_microbes_b200.configs.config1)",
+            "dtype": w["dtype"],
+            "data": "synthetic (seeded, lattice_microbes_b200.configs.%s)" % w["config"],
             "config": {
-                "workload": WORKLOAD,
+                "workload": w["desc"],
                 "timesteps_per_step": T,
                 "sites": N,
                 "parallelism": "replicas" if world > 1 else "single",
                 "schedule": sched_name,
                 "autotune_ms": None if tuned is None else tuned[3],
-                "l2": "flushed between timed steps (256 MB write); working set 9 MB is L2-resident within a step",
+                "l2": w["l2"],
             },
             "roofline": {
                 "bound": "hbm",
@@ -400,14 +448,18 @@ def run_ours(a):
                 "peak": peak,
                 "unit": "GB/s",
                 "frac": achieved / peak,
-                "traffic": ncu_traffic_per_launch("fused_step_kernel" if phase_n[5] > 0 else "sweep_kernel"),
+                "traffic": ncu_traffic_per_launch(a.workload,
+                                                  "fused_step_kernel" if phase_n[5] > 0 else "sweep_kernel"),
                 "kernel": kern,
                 "ms_per_launch": launch_ms,
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "own_dataflow_bytes_per_launch": own_bytes,
                 "own_dataflow_frac": own_bytes / (launch_ms / 1e3) / 1e9 / peak,
                 "peak_kind": peak_kind,
-                "note": "working set 9 MB is L2-resident; HBM fraction is reference-schedule-equivalent",
+                "note": ("achieved = algorithmic bytes of the reference schedule (B_step per site-step) per "
+                         "launch / launch time; own_dataflow_frac counts the fused kernel's single read and "
+                         "write of the lattice" + ("; working set 9 MB is L2-resident" if a.workload == "rodcell"
+                                                   else "")),
                 "phases": phases,
                 "step_fraction_reference_schedule": value * B_STEP / (peak * 1e9),
             },
@@ -438,20 +490,23 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    wname = a.workload if a.workload in WORKLOADS else "rodcell"
+    w = WORKLOADS[wname]
     cores = host_cores()
-    sim_time = a.cpu_sample_time or 0.01
+    sim_time = a.cpu_sample_time or w["nsm_time"] / 4
     vals, samples = [], []
     for _ in range(min(a.warmup, 1)):
-        cpu_nsm_sample(sim_time / 4, cores)
+        cpu_nsm_sample(wname, sim_time / 4, cores)
     for _ in range(a.steps):
-        v, s = cpu_nsm_sample(sim_time, cores)
+        v, s = cpu_nsm_sample(wname, sim_time, cores)
         if v is None:
             print(json.dumps({"impl": "reference", "unavailable": s}))
             return
         vals.append(v)
         samples.append(s)
     value = statistics.mean(vals)
-    nsites = 64 * 64 * 128
+    spec_sites = {"rodcell": 64 * 64 * 128, "crowded": 128 * 128 * 256}[wname]
+    T = a.timesteps_per_step or w["timesteps_per_step"]
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -460,13 +515,13 @@ def run_reference(a):
         "n_gpus": world,
         "steps": a.steps,
         "warmup": a.warmup,
-        "ms_per_step": nsites * a.timesteps_per_step / value * 1e3,
+        "ms_per_step": spec_sites * T / value * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "u8",
-        "data": "synthetic (seeded rod-cell model)",
-        "config": {"workload": WORKLOAD, "timesteps_per_step": a.timesteps_per_step, "sites": nsites,
+        "dtype": w["dtype"],
+        "data": "synthetic (seeded, lattice_microbes_b200.configs.%s)" % w["config"],
+        "config": {"workload": w["desc"], "timesteps_per_step": T, "sites": spec_sites,
                    "parallelism": "host cores"},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
                          "sample": samples[-1]},
@@ -488,7 +543,7 @@ def run_batch(a):
     from lattice_microbes_b200.solver import Batch, Context, Lattice, Model, compose_seed, kernel_launches
 
     torch.cuda.set_device(0)
-    T = a.timesteps_per_step if a.timesteps_per_step != TIMESTEPS_PER_STEP else 200
+    T = a.timesteps_per_step or 200
     edges = configs.batch_edges(seed=7, count=a.replicates or 256)
     ctx = Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", 0))

@@ -273,15 +273,15 @@ protected:
     /* Hooks (MpdRdmeSolver.cu:789-822).  hookSimulation returns 0 (lattice
      * unchanged), 1 (lattice changed: copied to the device), 2 (sites changed
      * too: copied and written), 3 (stop after writing the sites). */
-    virtual int hookSimulation(double time, HostLattice &lattice) { return 0; }
-    virtual int onBeginTrajectory(HostLattice &lattice) { return 0; }
-    virtual int onEndTrajectory(HostLattice &lattice) { return 0; }
-    virtual int onWriteLattice(double time, HostLattice &lattice) { return 0; }
+    virtual int hookSimulation(double /*time*/, HostLattice &/*lattice*/) { return 0; }
+    virtual int onBeginTrajectory(HostLattice &/*lattice*/) { return 0; }
+    virtual int onEndTrajectory(HostLattice &/*lattice*/) { return 0; }
+    virtual int onWriteLattice(double /*time*/, HostLattice &/*lattice*/) { return 0; }
 
     /* Outputs (the reference's DataOutputQueue data sets). */
-    virtual void writeSpeciesCounts(double time, const std::vector<uint64_t> &counts) {}
-    virtual void writeLattice(double time, const HostLattice &lattice) {}
-    virtual void writeLatticeSites(double time, const HostLattice &lattice) {}
+    virtual void writeSpeciesCounts(double /*time*/, const std::vector<uint64_t> &/*counts*/) {}
+    virtual void writeLattice(double /*time*/, const HostLattice &/*lattice*/) {}
+    virtual void writeLatticeSites(double /*time*/, const HostLattice &/*lattice*/) {}
 
     std::string param(const char *key) const
     {
