@@ -53,7 +53,7 @@ WORKLOADS = {
         desc="crowded cell 128x128x256 IntLattice-16, 8 site types (20% obstacles), 200 species, "
              "500 reactions, 1M particles",
         config="config2", S=16, b=4, tau=10e-6, dtype="u32", timesteps_per_step=40, ref_timesteps=100,
-        nsm_time=2e-4, ref_mpd_timesteps=2,
+        nsm_time=2e-5, ref_mpd_timesteps=2,
         l2="inputs larger than L2: 537 MB of particle buffers + 4 MB site types per timestep"),
 }
 
@@ -150,42 +150,45 @@ def _byte_lattice(spec):
 
 
 def _nsm_worker(args):
-    """One replicate of the reference NextSubvolumeSolver on one core (spawned)."""
+    """One replicate of the reference NextSubvolumeSolver on one core
+    (spawned): a run to a tenth of a timestep (the solver's set-up: lattice,
+    queue, all subvolume propensities) and a run to `sim_time`; the
+    difference is the simulation itself."""
     workload, seed, sim_time = args
     sys.path.insert(0, ROOT)
     from tests import ref_cpu_lib
     if not ref_cpu_lib.available():
         return None
     spec = _byte_lattice(make_spec(workload, seed))
+    short = WORKLOADS[workload]["tau"] / 10
     t0 = time.perf_counter()
+    ref_cpu_lib.nsm_run(spec, 1000 + seed, seed + 1, short, short)
+    t1 = time.perf_counter()
     ref_cpu_lib.nsm_run(spec, 1000 + seed, seed + 1, sim_time, sim_time / 4)
-    return time.perf_counter() - t0, spec.nsites
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1, spec.nsites
 
 
 def cpu_nsm_sample(workload, sim_time, cores):
     """Reference NextSubvolumeSolver, `cores` replicates of the workload in
-    parallel, each to `sim_time` seconds; returns (site-steps/s, sample) with
-    site-steps = sites x sim_time / tau per replicate."""
+    parallel; returns (site-steps/s, sample) with site-steps = sites x
+    simulated time / tau, set-up time excluded."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         res = pool.map(_nsm_worker, [(workload, s, sim_time) for s in range(cores)])
     if any(r is None for r in res):
         return None, "reference CPU solvers not built (oracle/_ref)"
-    wall = max(r[0] for r in res)
     tau = WORKLOADS[workload]["tau"]
-    value = res[0][1] * (sim_time / tau) * cores / wall
+    short = tau / 10
+    wall = max(r[1] - r[0] for r in res)
+    setup = max(r[0] for r in res)
+    value = res[0][2] * ((sim_time - short) / tau) * cores / wall
     sample = ("%d replicates of the %s workload, one per core, each %.4g s of simulated time (%d "
-              "MPD-timestep equivalents), reference NextSubvolumeSolver built from its sources; %.1f s wall"
-              % (cores, workload, sim_time, round(sim_time / tau), wall))
+              "MPD-timestep equivalents), reference NextSubvolumeSolver built from its sources; %.1f s wall "
+              "after the solver's set-up (%.1f s, excluded)" % (cores, workload, sim_time, round(sim_time / tau),
+                                                               wall, setup))
     return value, sample
-
-
-def host_cores():
-    try:
-        return len(os.sched_getaffinity(0))
-    except Exception:
-        return os.cpu_count() or 1
 
 
 # --------------------------------------------------------------------------

@@ -515,7 +515,9 @@ static cudaError_t ensure_smem_limit(size_t smem)
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (smem <= 48 * 1024 || smem <= granted[dev]) return cudaSuccess;
+    // The kernel's static shared memory counts against the default 48 KB
+    // too, so the limit is raised for any size not granted yet.
+    if (smem <= granted[dev]) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(fused_step_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess) granted[dev] = smem;
@@ -580,7 +582,9 @@ static cudaError_t ensure_batch_smem_limit(size_t smem)
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (smem <= 48 * 1024 || smem <= granted[dev]) return cudaSuccess;
+    // The kernel's static shared memory counts against the default 48 KB
+    // too, so the limit is raised for any size not granted yet.
+    if (smem <= granted[dev]) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(fused_batch_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e == cudaSuccess) granted[dev] = smem;

@@ -6,14 +6,15 @@
 // does nothing once a run has failed, so a queued run stops cleanly at the
 // failing timestep.
 //
-// Sweep design: one thread per site.  A thread loads its own site and its two
-// neighbours along the sweep axis (coalesced word-planar loads; the neighbour
-// rows are L1/L2 hits for the neighbouring warps), recomputes the neighbours'
-// hop decisions from the counter hash, and assembles its new site in
-// registers.  Because every decision is a pure function of (seed, step, site,
-// slot, site types), recomputing a neighbour's choice gives the same answer
-// the neighbour's own thread gets, so no shared-memory exchange or barrier is
-// needed.  Empty neighbourhoods take a store-only fast path.
+// Sweep design: one thread per site; a block covers a tile of sites that is
+// long along the sweep axis (x rows for the x sweep, 8 y rows or 8 z planes
+// for the y and z sweeps).  Each thread draws its own site's hop choices once
+// (one hash per particle), publishes the site and its choices in shared
+// memory, and assembles its new site from its own and its two neighbours'
+// entries.  A neighbour outside the tile is loaded and its choices drawn
+// again by the thread that needs it; every decision is a pure function of
+// (seed, step, site, slot, site types), so the copies agree.  Empty
+// neighbourhoods take a store-only path.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -29,43 +30,173 @@ namespace lmb {
 // Diffusion sweep
 // ---------------------------------------------------------------------------
 
-template <int BPS, int S, int DIM>
-__global__ void __launch_bounds__(256) sweep_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
-                                                    const uint8_t *__restrict__ sites, Geometry g, DevTables m,
-                                                    RunState *__restrict__ rs, OverflowEntry *__restrict__ list,
-                                                    uint32_t cap)
+constexpr int SWEEP_THREADS = 256;
+
+// Site coordinates of the thread and its neighbours along axis DIM
+// (periodic), and where a neighbour sits in the block's tile (-1: outside).
+template <int DIM>
+__device__ __forceinline__ void sweep_neighbours(const Geometry &g, uint32_t x, uint32_t y, uint32_t z,
+                                                 uint32_t &i, uint32_t &im, uint32_t &ip, int &lm, int &lp)
 {
+    const uint32_t bx = blockDim.x, by = blockDim.y;
+    const int lid = (int)(threadIdx.x + bx * (threadIdx.y + by * threadIdx.z));
+    i = x + y * g.X + z * g.XY;
+    if (DIM == 0) {
+        const uint32_t xm = x == 0 ? g.X - 1 : x - 1, xp = x == g.X - 1 ? 0 : x + 1;
+        im = i - x + xm;
+        ip = i - x + xp;
+        const uint32_t x0 = blockIdx.x * bx;
+        lm = (xm >= x0 && xm < x0 + bx) ? lid - (int)x + (int)xm : -1;
+        lp = (xp >= x0 && xp < x0 + bx) ? lid - (int)x + (int)xp : -1;
+    } else if (DIM == 1) {
+        const uint32_t ym = y == 0 ? g.Y - 1 : y - 1, yp = y == g.Y - 1 ? 0 : y + 1;
+        im = i - y * g.X + ym * g.X;
+        ip = i - y * g.X + yp * g.X;
+        const uint32_t y0 = blockIdx.y * by;
+        lm = (ym >= y0 && ym < y0 + by) ? lid + ((int)ym - (int)y) * (int)bx : -1;
+        lp = (yp >= y0 && yp < y0 + by) ? lid + ((int)yp - (int)y) * (int)bx : -1;
+    } else {
+        const uint32_t zm = z == 0 ? g.Z - 1 : z - 1, zp = z == g.Z - 1 ? 0 : z + 1;
+        im = i - z * g.XY + zm * g.XY;
+        ip = i - z * g.XY + zp * g.XY;
+        const uint32_t z0 = blockIdx.z * blockDim.z;
+        lm = (zm >= z0 && zm < z0 + blockDim.z) ? lid + ((int)zm - (int)z) * (int)(bx * by) : -1;
+        lp = (zp >= z0 && zp < z0 + blockDim.z) ? lid + ((int)zp - (int)z) * (int)(bx * by) : -1;
+    }
+}
+
+template <int BPS, int S, int DIM>
+__global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__restrict__ src,
+                                                              uint32_t *__restrict__ dst,
+                                                              const uint8_t *__restrict__ sites, Geometry g,
+                                                              DevTables m, RunState *__restrict__ rs,
+                                                              OverflowEntry *__restrict__ list, uint32_t cap)
+{
+    using Code = typename ChoiceCode<S>::type;
+    constexpr int W = SiteWords<BPS, S>::W;
+    __shared__ uint32_t sw[W][SWEEP_THREADS];
+    __shared__ Code sc[SWEEP_THREADS];
+    __shared__ uint8_t st[SWEEP_THREADS];
     if (rs->status != LMB_OK) return;
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
-    const uint32_t z = blockIdx.z;
-    if (x >= g.X || y >= g.Y) return;
-    const uint32_t i = x + y * g.X + z * g.XY;
-    uint32_t im, ip;
-    if (DIM == 0) {
-        im = i - x + (x == 0 ? g.X - 1 : x - 1);
-        ip = i - x + (x == g.X - 1 ? 0 : x + 1);
-    } else if (DIM == 1) {
-        const uint32_t base = i - y * g.X;
-        im = base + (y == 0 ? g.Y - 1 : y - 1) * g.X;
-        ip = base + (y == g.Y - 1 ? 0 : y + 1) * g.X;
-    } else {
-        const uint32_t base = i - z * g.XY;
-        im = base + (z == 0 ? g.Z - 1 : z - 1) * g.XY;
-        ip = base + (z == g.Z - 1 ? 0 : z + 1) * g.XY;
-    }
-    SiteWords<BPS, S> own, mn, pl;
-    own.load(src, g.N, i);
-    mn.load(src, g.N, im);
-    pl.load(src, g.N, ip);
-    if (own.empty() && mn.empty() && pl.empty()) {
-        own.store(dst, g.N, i);
-        return;
-    }
+    const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
+    const bool in = x < g.X && y < g.Y && z < g.Z;
+    const int lid = (int)(threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z));
+    uint32_t i = 0, im = 0, ip = 0;
+    int lm = -1, lp = -1;
+    SiteWords<BPS, S> own;
+    own.clear();
+    uint32_t t = 0, tm = 0, tp = 0;
+    Code c_own = 0;
     const unsigned long long th = timestep_hash(rs->seed, rs->step, DIM);
-    const uint32_t t = __ldg(sites + i), tm = __ldg(sites + im), tp = __ldg(sites + ip);
-    const SiteWords<BPS, S> out =
-        sweep_site<BPS, S>(own, mn, pl, t, tm, tp, i, im, ip, th, m, true, DIM + 1, rs, list, cap);
+    uint32_t occ = 0;
+    if (in) {
+        sweep_neighbours<DIM>(g, x, y, z, i, im, ip, lm, lp);
+        own.load(src, g.N, i);
+        t = __ldg(sites + i);
+        tm = __ldg(sites + im);
+        tp = __ldg(sites + ip);
+        occ = occupied_slots<BPS, S>(own);
+#pragma unroll
+        for (int k = 0; k < W; k++) sw[k][lid] = own.w[k];
+        st[lid] = (uint8_t)t;
+    }
+    sc[lid] = 0;
+    __syncwarp();
+    // The warp's particles drawn together: particle q of the warp (in site,
+    // then slot order) goes to lane q % 32, so every lane hashes about the
+    // same number of particles however unevenly the sites are filled.
+    {
+        constexpr int CB = CountBits<S>::value;
+        const uint32_t lane = threadIdx.x & 31u, wbase = (uint32_t)lid & ~31u;
+        const uint32_t n = __popc(occ);
+        uint32_t incl = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - n;
+        for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t q = base + lane;
+            // Owner lane: the last lane whose first particle index is <= q.
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t step = 16; step >= 1; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xffffffffu, excl, (o + step) & 31u);
+                if (o + step < 32 && e <= q) o += step;
+            }
+            const uint32_t occ_o = __shfl_sync(0xffffffffu, occ, o);
+            const uint32_t j = q - __shfl_sync(0xffffffffu, excl, o);
+            const uint32_t t_o = __shfl_sync(0xffffffffu, t, o), tm_o = __shfl_sync(0xffffffffu, tm, o);
+            const uint32_t tp_o = __shfl_sync(0xffffffffu, tp, o), gi_o = __shfl_sync(0xffffffffu, i, o);
+            if (q < total) {
+                uint32_t mbits = occ_o;
+                for (uint32_t r = 0; r < j; r++) mbits &= mbits - 1;
+                const uint32_t k = __ffs(mbits) - 1;
+                const uint32_t so = wbase + o;
+                const uint32_t p = BPS == 1 ? (sw[k >> 2][so] >> (8 * (k & 3u))) & 0xFFu : sw[k][so];
+                const float rv = hash_float(((unsigned long long)gi_o << CB) | k, th);
+                const float qp = lookup_T(m, p, t_o, tp_o);
+                Code bit = 0;
+                if ((rv >= 0.5f) && (rv < __fadd_rn(qp, 0.5f))) bit = (Code)1 << (S + k);
+                else if (rv < lookup_T(m, p, t_o, tm_o)) bit = (Code)1 << k;
+                if (bit) atomicOr(&sc[so], bit);
+            }
+        }
+    }
+    __syncthreads();
+    if (!in) return;
+    c_own = sc[lid];
+    // The neighbours: from the tile, or loaded with their choices drawn here.
+    SiteWords<BPS, S> mn, pl;
+    Code c_mn = 0, c_pl = 0;
+    if (lm >= 0) {
+#pragma unroll
+        for (int k = 0; k < W; k++) mn.w[k] = sw[k][lm];
+        c_mn = sc[lm];
+    } else {
+        mn.load(src, g.N, im);
+        if (!mn.empty()) {
+            // The minus neighbour's own minus neighbour along the axis.
+            uint32_t imm;
+            if (DIM == 0) {
+                const uint32_t xm = x == 0 ? g.X - 1 : x - 1;
+                imm = i - x + (xm == 0 ? g.X - 1 : xm - 1);
+            } else if (DIM == 1) {
+                const uint32_t ym = y == 0 ? g.Y - 1 : y - 1;
+                imm = i - y * g.X + (ym == 0 ? g.Y - 1 : ym - 1) * g.X;
+            } else {
+                const uint32_t zm = z == 0 ? g.Z - 1 : z - 1;
+                imm = i - z * g.XY + (zm == 0 ? g.Z - 1 : zm - 1) * g.XY;
+            }
+            c_mn = site_choices<BPS, S>(mn, tm, __ldg(sites + imm), t, im, th, m);
+        }
+    }
+    if (lp >= 0) {
+#pragma unroll
+        for (int k = 0; k < W; k++) pl.w[k] = sw[k][lp];
+        c_pl = sc[lp];
+    } else {
+        pl.load(src, g.N, ip);
+        if (!pl.empty()) {
+            uint32_t ipp;
+            if (DIM == 0) {
+                const uint32_t xp = x == g.X - 1 ? 0 : x + 1;
+                ipp = i - x + (xp == g.X - 1 ? 0 : xp + 1);
+            } else if (DIM == 1) {
+                const uint32_t yp = y == g.Y - 1 ? 0 : y + 1;
+                ipp = i - y * g.X + (yp == g.Y - 1 ? 0 : yp + 1) * g.X;
+            } else {
+                const uint32_t zp = z == g.Z - 1 ? 0 : z + 1;
+                ipp = i - z * g.XY + (zp == g.Z - 1 ? 0 : zp + 1) * g.XY;
+            }
+            c_pl = site_choices<BPS, S>(pl, tp, t, __ldg(sites + ipp), ip, th, m);
+        }
+    }
+    const SiteWords<BPS, S> out = assemble_site<BPS, S>(own, c_own, mn, c_mn, pl, c_pl, i, true,
+                                                        (uint32_t)DIM + 1, rs, list, cap);
     out.store(dst, g.N, i);
 }
 
@@ -285,14 +416,30 @@ __global__ void native_to_row_major_kernel(const uint32_t *__restrict__ native, 
 // Launchers
 // ---------------------------------------------------------------------------
 
-static void sweep_shape(const Geometry &g, dim3 &grid, dim3 &block)
+// Tiles long along the sweep axis: whole x rows (up to 256 sites) for x,
+// 32 x 8 sites in the x-y plane for y, 32 x 8 in the x-z plane for z.
+static void sweep_shape(const Geometry &g, int dim, dim3 &grid, dim3 &block)
 {
-    uint32_t bx = ((g.X + 31) / 32) * 32;
-    if (bx > 128) bx = 128;
-    uint32_t by = 256 / bx;
-    if (by > g.Y) by = g.Y;
-    block = dim3(bx, by, 1);
-    grid = dim3((g.X + bx - 1) / bx, (g.Y + by - 1) / by, g.Z);
+    if (dim == 0) {
+        uint32_t bx = ((g.X + 31) / 32) * 32;
+        if (bx > 256) bx = 256;
+        uint32_t by = 256 / bx;
+        if (by > g.Y) by = g.Y;
+        block = dim3(bx, by, 1);
+        grid = dim3((g.X + bx - 1) / bx, (g.Y + by - 1) / by, g.Z);
+    } else if (dim == 1) {
+        const uint32_t by = g.Y < 8 ? g.Y : 8;
+        uint32_t bx = 256 / by;
+        if (bx > ((g.X + 31) / 32) * 32) bx = ((g.X + 31) / 32) * 32;
+        block = dim3(bx, by, 1);
+        grid = dim3((g.X + bx - 1) / bx, (g.Y + by - 1) / by, g.Z);
+    } else {
+        const uint32_t bz = g.Z < 8 ? g.Z : 8;
+        uint32_t bx = 256 / bz;
+        if (bx > ((g.X + 31) / 32) * 32) bx = ((g.X + 31) / 32) * 32;
+        block = dim3(bx, 1, bz);
+        grid = dim3((g.X + bx - 1) / bx, g.Y, (g.Z + bz - 1) / bz);
+    }
 }
 
 #define LMB_DISPATCH(BPS_, S_, ...)                                                   \
@@ -325,7 +472,7 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
                          cudaStream_t stream)
 {
     dim3 grid, block;
-    sweep_shape(g, grid, block);
+    sweep_shape(g, dim, grid, block);
     count_launch();
     LMB_DISPATCH_ALL({
         if (dim == 0) sweep_kernel<BPS, S, 0><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap);

@@ -1,9 +1,11 @@
 // lmb_site.cuh -- the per-site MPD rules, shared by the per-phase kernels and
 // the fused timestep kernel.
 //
-// sweep_site: new content of one site after a 1-D hop sweep, from its own
-// slots and its two neighbours' slots along the sweep axis
-// (byte_diffusion_1d_dev.cu:86-122 choices, :199-269 propagation).
+// site_choices / assemble_site: one 1-D hop sweep, as the reference splits it
+// into choices (byte_diffusion_1d_dev.cu:86-122) and propagation (:199-269):
+// each particle's choice is drawn once, then every output site assembles its
+// new content from its own and its two neighbours' choices.
+// sweep_site: one sweep of one site, drawing its neighbours' choices too.
 // react_site: the precomputed-table reaction step of one site
 // (MpdRdmeSolver.cu:1590-1675 with byte_reaction_dev.cu:121-258).
 #pragma once
@@ -35,6 +37,136 @@ struct SiteBuilder {
     }
 };
 
+// A site's hop choices for one sweep, one bit per slot and direction: bit k
+// of the low half set when the particle in slot k moves to the minus
+// neighbour, bit S + k when it moves to the plus neighbour; neither bit for a
+// stayer or an empty slot.  32 bits cover up to 16 slots, 64 bits 32 slots.
+template <int S>
+struct ChoiceCode {
+    using type = uint32_t;
+};
+template <>
+struct ChoiceCode<32> {
+    using type = unsigned long long;
+};
+
+// Bit k set when slot k holds a particle (slots may have holes in a lattice
+// given by the caller, so every slot is looked at, as the reference does).
+template <int BPS, int S>
+__device__ __forceinline__ uint32_t occupied_slots(const SiteWords<BPS, S> &s)
+{
+    uint32_t m = 0;
+    if (BPS == 1) {
+#pragma unroll
+        for (int k = 0; k < SiteWords<BPS, S>::W; k++) {
+            const uint32_t w = s.w[k];
+            // High bit of each byte set when the byte is nonzero, then the
+            // four bits gathered into bits 28..31 by one multiply.
+            const uint32_t hi = (w | ((w & 0x7F7F7F7Fu) + 0x7F7F7F7Fu)) & 0x80808080u;
+            m |= (((hi >> 7) * 0x10204080u) >> 28) << (4 * k);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < S; k++) m |= (s.w[k] != 0u ? 1u : 0u) << k;
+    }
+    return m;
+}
+
+// The particle in slot k for a slot index known only at run time (no
+// dynamic register indexing: the word is selected, then the byte).
+template <int BPS, int S>
+__device__ __forceinline__ uint32_t slot_at(const SiteWords<BPS, S> &s, uint32_t k)
+{
+    constexpr int W = SiteWords<BPS, S>::W;
+    if (BPS == 1) {
+        uint32_t w = s.w[0];
+#pragma unroll
+        for (int j = 1; j < W; j++)
+            if ((k >> 2) == (uint32_t)j) w = s.w[j];
+        return (w >> (8 * (k & 3u))) & 0xFFu;
+    }
+    uint32_t v = s.w[0];
+#pragma unroll
+    for (int j = 1; j < W; j++)
+        if (k == (uint32_t)j) v = s.w[j];
+    return v;
+}
+
+// Choices of every particle of a site of type t whose minus / plus
+// neighbours have types tm / tp, keyed by the site's lattice index gi
+// (byte_diffusion_1d_dev.cu:86-122, word_diffusion_1d_dev.cu:83-112): draw
+// r; PLUS when 0.5 <= r < q(t->tp) + 0.5, else MINUS when r < q(t->tm),
+// else STAY.  One hash per particle per sweep.
+template <int BPS, int S>
+__device__ __forceinline__ typename ChoiceCode<S>::type site_choices(const SiteWords<BPS, S> &s, uint32_t t,
+                                                                     uint32_t tm, uint32_t tp, uint32_t gi,
+                                                                     unsigned long long th, const DevTables &m)
+{
+    using Code = typename ChoiceCode<S>::type;
+    constexpr int CB = CountBits<S>::value;
+    Code c = 0;
+    uint32_t occ = occupied_slots<BPS, S>(s);
+    while (occ) {
+        const uint32_t k = __ffs(occ) - 1;
+        occ &= occ - 1;
+        const uint32_t p = slot_at<BPS, S>(s, k);
+        const float r = hash_float(((unsigned long long)gi << CB) | k, th);
+        const float qp = lookup_T(m, p, t, tp);
+        if ((r >= 0.5f) && (r < __fadd_rn(qp, 0.5f))) {
+            c |= (Code)1 << (S + k);
+        } else {
+            const float qm = lookup_T(m, p, t, tm);
+            if (r < qm) c |= (Code)1 << k;
+        }
+    }
+    return c;
+}
+
+// New content of a site after a sweep (byte_diffusion_1d_dev.cu:199-269):
+// its stayers in slot order, then the PLUS movers of the minus neighbour,
+// then the MINUS movers of the plus neighbour, each in slot order; the
+// (S+1)-th and later particles overflow (queued with seq = position - S when
+// `record`: only the owner of a site records, halo recomputations do not).
+template <int BPS, int S>
+__device__ __forceinline__ SiteWords<BPS, S> assemble_site(const SiteWords<BPS, S> &own,
+                                                           typename ChoiceCode<S>::type c_own,
+                                                           const SiteWords<BPS, S> &mn,
+                                                           typename ChoiceCode<S>::type c_mn,
+                                                           const SiteWords<BPS, S> &pl,
+                                                           typename ChoiceCode<S>::type c_pl, uint32_t gi,
+                                                           bool record, uint32_t phase, RunState *rs,
+                                                           OverflowEntry *list, uint32_t cap)
+{
+    constexpr uint32_t LOW = S >= 32 ? 0xFFFFFFFFu : ((1u << S) - 1u);
+    SiteBuilder<BPS, S> b;
+    b.init();
+    uint32_t stay = occupied_slots<BPS, S>(own) & ~((uint32_t)c_own | (uint32_t)(c_own >> S)) & LOW;
+    while (stay) {
+        const uint32_t k = __ffs(stay) - 1;
+        stay &= stay - 1;
+        b.push(slot_at<BPS, S>(own, k), record, rs, list, cap, phase, gi);
+    }
+    uint32_t in_m = (uint32_t)(c_mn >> S) & LOW;
+    while (in_m) {
+        const uint32_t k = __ffs(in_m) - 1;
+        in_m &= in_m - 1;
+        b.push(slot_at<BPS, S>(mn, k), record, rs, list, cap, phase, gi);
+    }
+    uint32_t in_p = (uint32_t)c_pl & LOW;
+    while (in_p) {
+        const uint32_t k = __ffs(in_p) - 1;
+        in_p &= in_p - 1;
+        b.push(slot_at<BPS, S>(pl, k), record, rs, list, cap, phase, gi);
+    }
+    return b.out;
+}
+
+// sweep_site: the same sweep for one output site in one call, drawing the
+// choices of its own and its two neighbours' particles itself (three hashes
+// per particle over the sweep, no exchange between threads).  The fused
+// kernel uses it: at the low occupancy it serves, exchanging choices through
+// shared memory costs more (a pass, a barrier and shared memory) than the
+// extra hashes.
 // gi/gim/gip: lattice indices of the site and its minus / plus neighbours
 // (they key the hash); t/tm/tp: their site types.
 template <int BPS, int S>
@@ -134,8 +266,14 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
         }
     }
     if (a == 0.0f) return false;
-    const float prob = (float)(1.0 - exp(-(double)a));
     const float r0 = hash_float(((unsigned long long)gi << 1) | 0ull, th);
+    // prob = (float)(1 - exp(-a)) below never exceeds a: mathematically
+    // 1 - e^-a < a for a > 0, the double evaluation adds at most a few units
+    // of 2^-53, and rounding to float at most one float ulp of a.  A draw
+    // above a * (1 + 2^-20) + 2^-60 therefore cannot react, and the double
+    // exp is evaluated only for draws below that bound.
+    if (r0 > __fadd_ru(__fmul_ru(a, 1.00000095367431640625f), 8.67361738e-19f)) return false;
+    const float prob = (float)(1.0 - exp(-(double)a));
     if (!(prob > 0.0f && r0 <= prob)) return false;
 
     float rp = __fmul_rn(hash_float(((unsigned long long)gi << 1) | 1ull, th), a);
