@@ -806,9 +806,13 @@ def run_serve(a):
 
     # Sequential plain solver: one solve at a time, arrival order.
     solo_s = []
+    from lattice_microbes_b200 import _lib as LL
     for sp, r, sd in zip(specs, stream_reqs, seeds):
         m = Model.from_spec(ctx, sp)
         L2 = Lattice(ctx, sp.X, sp.Y, sp.Z, 16, 1)
+        # The schedule the server gives a large solve (per-phase when dense).
+        if sp.nsites >= (1 << 17) and r.density >= 0.05:
+            L2.set_schedule(LL.LMB_SCHEDULE_PHASES)
         torch.cuda.synchronize(0)
         s0 = time.perf_counter()
         L2.set_native(sp.lattice, sp.sites)

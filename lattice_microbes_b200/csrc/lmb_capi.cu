@@ -43,6 +43,8 @@ struct lmb_model {
     std::vector<uint8_t> RL;
     std::vector<uint32_t> st_off, st_sp;
     std::vector<int32_t> st_d;
+    std::vector<float> qpmax;  // per site type: largest qp1, then largest qp2 entry
+    std::vector<uint32_t> rx_off, rx_list;  // reactions by first reactant (DevTables::rx_off)
     // Device copy.
     void *dev_block;
     size_t dev_bytes;
@@ -227,6 +229,27 @@ static int upload_model(lmb_model *m)
 {
     lmb_ctx *c = m->ctx;
     CK(cudaSetDevice(c->device));
+    // Largest single-particle and pair table entries per site type: they
+    // bound a site's total propensity from its particle count alone.
+    m->qpmax.assign(2 * (size_t)m->nst, 0.0f);
+    for (uint32_t st = 0; st < m->nst; st++) {
+        float a = 0.0f, b = 0.0f;
+        for (uint32_t i = 0; i < m->ns; i++) a = std::max(a, m->qp1[(size_t)st * m->ns + i]);
+        for (size_t i = 0; i < (size_t)m->ns * m->ns; i++) b = std::max(b, m->qp2[(size_t)st * m->ns * m->ns + i]);
+        m->qpmax[st] = a;
+        m->qpmax[m->nst + st] = b;
+    }
+    // Reactions by first reactant (zeroth-order ones first), ascending.
+    m->rx_off.assign((size_t)m->ns + 2, 0);
+    m->rx_list.clear();
+    for (uint32_t sp = 0; sp <= m->ns; sp++) {
+        m->rx_off[sp] = (uint32_t)m->rx_list.size();
+        for (uint32_t r = 0; r < m->nr; r++) {
+            const bool zeroth = m->order[r] == 1;
+            if ((sp == 0 && zeroth) || (sp > 0 && !zeroth && m->D1[r] == sp)) m->rx_list.push_back(r);
+        }
+    }
+    m->rx_off[m->ns + 1] = (uint32_t)m->rx_list.size();
     // One device block holding every table, 256-byte aligned pieces.
     std::vector<std::pair<const void *, size_t>> parts = {
         {m->T.data(), m->T.size() * 4},          {m->qp0.data(), m->qp0.size() * 4},
@@ -234,7 +257,9 @@ static int upload_model(lmb_model *m)
         {m->order.data(), m->order.size() * 4},  {m->D1.data(), m->D1.size() * 4},
         {m->D2.data(), m->D2.size() * 4},        {m->rate.data(), m->rate.size() * 4},
         {m->RL.data(), m->RL.size()},            {m->st_off.data(), m->st_off.size() * 4},
-        {m->st_sp.data(), m->st_sp.size() * 4},  {m->st_d.data(), m->st_d.size() * 4}};
+        {m->st_sp.data(), m->st_sp.size() * 4},  {m->st_d.data(), m->st_d.size() * 4},
+        {m->qpmax.data(), m->qpmax.size() * 4},  {m->rx_off.data(), m->rx_off.size() * 4},
+        {m->rx_list.data(), m->rx_list.size() * 4}};
     std::vector<size_t> off(parts.size());
     size_t total = 0;
     for (size_t i = 0; i < parts.size(); i++) {
@@ -269,6 +294,9 @@ static int upload_model(lmb_model *m)
     m->dev.stoich_off = (const uint32_t *)(b + off[9]);
     m->dev.stoich_sp = (const uint32_t *)(b + off[10]);
     m->dev.stoich_d = (const int32_t *)(b + off[11]);
+    m->dev.qpmax = (const float *)(b + off[12]);
+    m->dev.rx_off = (const uint32_t *)(b + off[13]);
+    m->dev.rx_list = (const uint32_t *)(b + off[14]);
     m->dev.nnz = (uint32_t)m->st_sp.size();
     m->dev.stage_bytes = 0;
     {
@@ -277,7 +305,8 @@ static int upload_model(lmb_model *m)
         size_t bytes = 0;
         const size_t pieces[] = {m->T.size() * 4, m->qp0.size() * 4, m->qp1.size() * 4, m->qp2.size() * 4,
                                  (size_t)m->nr * 4, (size_t)m->nr * 4, (size_t)m->nr * 4, (size_t)m->nr * 4,
-                                 m->RL.size(), ((size_t)m->nr + 1) * 4, m->st_sp.size() * 4, m->st_d.size() * 4};
+                                 m->RL.size(), ((size_t)m->nr + 1) * 4, m->st_sp.size() * 4, m->st_d.size() * 4,
+                                 m->qpmax.size() * 4, m->rx_off.size() * 4, m->rx_list.size() * 4};
         for (size_t p : pieces) bytes += (p + 15) & ~(size_t)15;
         if (bytes <= 8 * 1024) m->dev.stage_bytes = (uint32_t)bytes;
     }

@@ -48,14 +48,14 @@ __device__ __forceinline__ void store_smem(uint32_t *buf, uint32_t R, uint32_t l
 __device__ __forceinline__ DevTables stage_tables(const DevTables &m, uint8_t *dst, uint32_t tid, uint32_t nthr)
 {
     DevTables s = m;
-    const void *srcs[12] = {m.T, m.qp0, m.qp1, m.qp2, m.order, m.D1, m.D2, m.rate, m.RL, m.stoich_off,
-                            m.stoich_sp, m.stoich_d};
-    const uint32_t sizes[12] = {m.nst * m.nst * m.ns * 4, m.nst * 4, m.nst * m.ns * 4, m.nst * m.ns * m.ns * 4,
+    const void *srcs[15] = {m.T, m.qp0, m.qp1, m.qp2, m.order, m.D1, m.D2, m.rate, m.RL, m.stoich_off,
+                            m.stoich_sp, m.stoich_d, m.qpmax, m.rx_off, m.rx_list};
+    const uint32_t sizes[15] = {m.nst * m.nst * m.ns * 4, m.nst * 4, m.nst * m.ns * 4, m.nst * m.ns * m.ns * 4,
                                 m.nr * 4, m.nr * 4, m.nr * 4, m.nr * 4, m.nr * m.nst, (m.nr + 1) * 4, m.nnz * 4,
-                                m.nnz * 4};
-    void *outs[12];
+                                m.nnz * 4, 2 * m.nst * 4, (m.ns + 2) * 4, m.nr * 4};
+    void *outs[15];
     uint32_t off = 0;
-    for (int k = 0; k < 12; k++) {
+    for (int k = 0; k < 15; k++) {
         outs[k] = dst + off;
         const uint8_t *sp = (const uint8_t *)srcs[k];
         for (uint32_t b = tid; b < sizes[k]; b += nthr) dst[off + b] = sp[b];
@@ -73,6 +73,9 @@ __device__ __forceinline__ DevTables stage_tables(const DevTables &m, uint8_t *d
     s.stoich_off = (const uint32_t *)outs[9];
     s.stoich_sp = (const uint32_t *)outs[10];
     s.stoich_d = (const int32_t *)outs[11];
+    s.qpmax = (const float *)outs[12];
+    s.rx_off = (const uint32_t *)outs[13];
+    s.rx_list = (const uint32_t *)outs[14];
     return s;
 }
 
@@ -260,6 +263,12 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     __syncthreads();
 
     uint32_t *src_w = A, *dst_w = B, *src_o = occA, *dst_o = occB;
+    // Models without zeroth-order reactions react only on occupied sites:
+    // the reaction then runs in the z sweep's pass, without a pass of its own.
+    bool zeroth = false;
+    for (uint32_t t = 0; t < mt.nst; t++) zeroth |= mt.qp0[t] != 0.0f;
+    const bool react_inline = with_reaction && !zeroth;
+    const unsigned long long th_rx = timestep_hash(seed, step, 3);
 #pragma unroll 1
     for (int phase = 0; phase < 3; phase++) {
         const unsigned long long th = timestep_hash(seed, step, (uint32_t)phase);
@@ -307,6 +316,10 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
             const bool record = phase == 2 || (rowflag[r] & ROW_OWNED);
             own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], rowbase[r] + x, rowbase[rm] + xm,
                                      rowbase[rp] + xp, th, mt, record, (uint32_t)phase + 1, rs, list, cap);
+            // After the z sweep an owned site reacts right away in
+            // registers, when only occupied sites can react.
+            if (phase == 2 && react_inline && !own.empty())
+                own = react_site_ool<BPS, S>(own, T[l], rowbase[r] + x, th_rx, mt, rs, list, cap);
             if (!own.empty()) {
                 store_smem<BPS, S>(dst_w, R, l, own);
                 atomicOr(&dst_o[r * MW + (x >> 5)], 1u << (x & 31u));
@@ -324,10 +337,8 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
 
     // Reaction on the owned sites that can react: the occupied ones, or every
     // site when the model has zeroth-order reactions.
-    if (with_reaction) {
-        const unsigned long long th = timestep_hash(seed, step, 3);
-        bool zeroth = false;
-        for (uint32_t t = 0; t < mt.nst; t++) zeroth |= mt.qp0[t] != 0.0f;
+    if (with_reaction && !react_inline) {
+        const unsigned long long th = th_rx;
         for (uint32_t i0 = 0; i0 < orows * MW; i0 += nthr) {
             const uint32_t i = i0 + tid;
             uint32_t a = 0, r = 0, w = 0;

@@ -52,6 +52,12 @@ struct DevTables {
     const int32_t *stoich_d;     // stoichiometric change
     uint32_t nnz;                // entries of the sparse stoichiometry
     uint32_t stage_bytes;        // shared-memory copy size of all tables, 0 if too large to stage
+    const float *qpmax;          // [nst] largest qp1 entry, then [nst] largest qp2 entry, per site type
+    // Reactions a site can fire, by first reactant: [rx_off[0], rx_off[1])
+    // lists the zeroth-order reactions, [rx_off[s], rx_off[s+1]) those whose
+    // first reactant is species s (1-based), each list ascending.
+    const uint32_t *rx_off;      // [ns + 2]
+    const uint32_t *rx_list;     // [nr]
 };
 
 // One queued overflow: the sort key orders entries by (phase, site, seq);

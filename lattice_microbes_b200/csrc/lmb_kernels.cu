@@ -149,55 +149,115 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
     __syncthreads();
     if (!in) return;
     c_own = sc[lid];
-    // The neighbours: from the tile, or loaded with their choices drawn here.
-    SiteWords<BPS, S> mn, pl;
-    Code c_mn = 0, c_pl = 0;
-    if (lm >= 0) {
-#pragma unroll
-        for (int k = 0; k < W; k++) mn.w[k] = sw[k][lm];
-        c_mn = sc[lm];
-    } else {
-        mn.load(src, g.N, im);
-        if (!mn.empty()) {
-            // The minus neighbour's own minus neighbour along the axis.
-            uint32_t imm;
-            if (DIM == 0) {
-                const uint32_t xm = x == 0 ? g.X - 1 : x - 1;
-                imm = i - x + (xm == 0 ? g.X - 1 : xm - 1);
-            } else if (DIM == 1) {
-                const uint32_t ym = y == 0 ? g.Y - 1 : y - 1;
-                imm = i - y * g.X + (ym == 0 ? g.Y - 1 : ym - 1) * g.X;
-            } else {
-                const uint32_t zm = z == 0 ? g.Z - 1 : z - 1;
-                imm = i - z * g.XY + (zm == 0 ? g.Z - 1 : zm - 1) * g.XY;
-            }
-            c_mn = site_choices<BPS, S>(mn, tm, __ldg(sites + imm), t, im, th, m);
+    // Lattice index of the neighbour's own outer neighbour along the axis.
+    auto outer_minus = [&]() {
+        if (DIM == 0) {
+            const uint32_t xm = x == 0 ? g.X - 1 : x - 1;
+            return i - x + (xm == 0 ? g.X - 1 : xm - 1);
+        } else if (DIM == 1) {
+            const uint32_t ym = y == 0 ? g.Y - 1 : y - 1;
+            return i - y * g.X + (ym == 0 ? g.Y - 1 : ym - 1) * g.X;
         }
-    }
-    if (lp >= 0) {
-#pragma unroll
-        for (int k = 0; k < W; k++) pl.w[k] = sw[k][lp];
-        c_pl = sc[lp];
-    } else {
-        pl.load(src, g.N, ip);
-        if (!pl.empty()) {
-            uint32_t ipp;
-            if (DIM == 0) {
-                const uint32_t xp = x == g.X - 1 ? 0 : x + 1;
-                ipp = i - x + (xp == g.X - 1 ? 0 : xp + 1);
-            } else if (DIM == 1) {
-                const uint32_t yp = y == g.Y - 1 ? 0 : y + 1;
-                ipp = i - y * g.X + (yp == g.Y - 1 ? 0 : yp + 1) * g.X;
-            } else {
-                const uint32_t zp = z == g.Z - 1 ? 0 : z + 1;
-                ipp = i - z * g.XY + (zp == g.Z - 1 ? 0 : zp + 1) * g.XY;
-            }
-            c_pl = site_choices<BPS, S>(pl, tp, t, __ldg(sites + ipp), ip, th, m);
+        const uint32_t zm = z == 0 ? g.Z - 1 : z - 1;
+        return i - z * g.XY + (zm == 0 ? g.Z - 1 : zm - 1) * g.XY;
+    };
+    auto outer_plus = [&]() {
+        if (DIM == 0) {
+            const uint32_t xp = x == g.X - 1 ? 0 : x + 1;
+            return i - x + (xp == g.X - 1 ? 0 : xp + 1);
+        } else if (DIM == 1) {
+            const uint32_t yp = y == g.Y - 1 ? 0 : y + 1;
+            return i - y * g.X + (yp == g.Y - 1 ? 0 : yp + 1) * g.X;
         }
+        const uint32_t zp = z == g.Z - 1 ? 0 : z + 1;
+        return i - z * g.XY + (zp == g.Z - 1 ? 0 : zp + 1) * g.XY;
+    };
+    if constexpr (BPS == 4) {
+        // IntLattice: a slot is a whole word, read by index from shared or
+        // global memory rather than selected among S registers; the new site
+        // is gathered in shared memory and written plane by plane.
+        __shared__ uint32_t so[S][SWEEP_THREADS];
+        constexpr int CB = CountBits<S>::value;
+        constexpr uint32_t LOW = (1u << S) - 1u;
+        auto choices_mem = [&](uint32_t idx, uint32_t occ_n, uint32_t t_n, uint32_t tm_n, uint32_t tp_n) {
+            Code c = 0;
+            while (occ_n) {
+                const uint32_t k = __ffs(occ_n) - 1;
+                occ_n &= occ_n - 1;
+                const uint32_t p = __ldg(src + (size_t)k * g.N + idx);
+                const float r = hash_float(((unsigned long long)idx << CB) | k, th);
+                if ((r >= 0.5f) && (r < __fadd_rn(lookup_T(m, p, t_n, tp_n), 0.5f))) c |= (Code)1 << (S + k);
+                else if (r < lookup_T(m, p, t_n, tm_n)) c |= (Code)1 << k;
+            }
+            return c;
+        };
+        Code c_mn = 0, c_pl = 0;
+        if (lm >= 0) {
+            c_mn = sc[lm];
+        } else {
+            SiteWords<BPS, S> mn;
+            mn.load(src, g.N, im);
+            const uint32_t o = occupied_slots<BPS, S>(mn);
+            if (o) c_mn = choices_mem(im, o, tm, __ldg(sites + outer_minus()), t);
+        }
+        if (lp >= 0) {
+            c_pl = sc[lp];
+        } else {
+            SiteWords<BPS, S> pl;
+            pl.load(src, g.N, ip);
+            const uint32_t o = occupied_slots<BPS, S>(pl);
+            if (o) c_pl = choices_mem(ip, o, tp, t, __ldg(sites + outer_plus()));
+        }
+        uint32_t n = 0;
+        auto push = [&](uint32_t p) {
+            if (n < (uint32_t)S) so[n][lid] = p;
+            else push_overflow(rs, list, cap, (uint32_t)DIM + 1, i, n - (uint32_t)S, p);
+            n++;
+        };
+        uint32_t stay = occ & ~((uint32_t)c_own | (uint32_t)(c_own >> S)) & LOW;
+        while (stay) {
+            const uint32_t k = __ffs(stay) - 1;
+            stay &= stay - 1;
+            push(sw[k][lid]);
+        }
+        uint32_t in_m = (uint32_t)(c_mn >> S) & LOW;
+        while (in_m) {
+            const uint32_t k = __ffs(in_m) - 1;
+            in_m &= in_m - 1;
+            push(lm >= 0 ? sw[k][lm] : __ldg(src + (size_t)k * g.N + im));
+        }
+        uint32_t in_p = (uint32_t)c_pl & LOW;
+        while (in_p) {
+            const uint32_t k = __ffs(in_p) - 1;
+            in_p &= in_p - 1;
+            push(lp >= 0 ? sw[k][lp] : __ldg(src + (size_t)k * g.N + ip));
+        }
+#pragma unroll
+        for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][lid] : 0u;
+    } else {
+        // The neighbours: from the tile, or loaded with their choices drawn here.
+        SiteWords<BPS, S> mn, pl;
+        Code c_mn = 0, c_pl = 0;
+        if (lm >= 0) {
+#pragma unroll
+            for (int k = 0; k < W; k++) mn.w[k] = sw[k][lm];
+            c_mn = sc[lm];
+        } else {
+            mn.load(src, g.N, im);
+            if (!mn.empty()) c_mn = site_choices<BPS, S>(mn, tm, __ldg(sites + outer_minus()), t, im, th, m);
+        }
+        if (lp >= 0) {
+#pragma unroll
+            for (int k = 0; k < W; k++) pl.w[k] = sw[k][lp];
+            c_pl = sc[lp];
+        } else {
+            pl.load(src, g.N, ip);
+            if (!pl.empty()) c_pl = site_choices<BPS, S>(pl, tp, t, __ldg(sites + outer_plus()), ip, th, m);
+        }
+        const SiteWords<BPS, S> out = assemble_site<BPS, S>(own, c_own, mn, c_mn, pl, c_pl, i, true,
+                                                            (uint32_t)DIM + 1, rs, list, cap);
+        out.store(dst, g.N, i);
     }
-    const SiteWords<BPS, S> out = assemble_site<BPS, S>(own, c_own, mn, c_mn, pl, c_pl, i, true,
-                                                        (uint32_t)DIM + 1, rs, list, cap);
-    out.store(dst, g.N, i);
 }
 
 // ---------------------------------------------------------------------------

@@ -13,6 +13,13 @@
 // as lmb_run on it alone: every decision depends only on (seed, timestep,
 // site, slot) and the lattice's own state.
 //
+// Small solves share the batched launches, where they would otherwise each
+// pay a launch per timestep for little work; a solve of at least
+// SOLO_SITES sites fills the device by itself and runs its chunks on its own
+// (same stream, after the batch), one large solve at a time in arrival
+// order, with the schedule that suits its particle density: the per-phase
+// kernels for dense lattices, the fused kernel for sparse ones.
+//
 // Host code only; it drives the device through the C ABI of lmb_capi.cu.
 #include <chrono>
 #include <cstring>
@@ -51,7 +58,23 @@ struct Active {
     uint32_t done;
     double t_admit;
     lmb_run_stats stats;
+    bool solo;
 };
+
+constexpr uint64_t SOLO_SITES = 1u << 17;      // 128 Ki sites (about 51^3)
+constexpr double DENSE_PARTICLES_PER_SITE = 0.05;
+
+// Particles in a native lattice (nonzero slots).
+uint64_t count_particles(const std::vector<uint32_t> &w, uint32_t bytes_per_particle)
+{
+    uint64_t n = 0;
+    for (uint32_t v : w) {
+        if (!v) continue;
+        if (bytes_per_particle == 4) n++;
+        else n += (v & 0xFFu ? 1 : 0) + (v & 0xFF00u ? 1 : 0) + (v & 0xFF0000u ? 1 : 0) + (v & 0xFF000000u ? 1 : 0);
+    }
+    return n;
+}
 
 struct Result {
     lmb_result_info info;
@@ -216,6 +239,7 @@ static int admit(lmb_server *s)
             a.lat = nullptr;
             a.model = nullptr;
             a.done = 0;
+            a.solo = false;
             a.t_admit = now_s();
             memset(&a.stats, 0, sizeof a.stats);
             a.stats.status = LMB_E_NOMEM;
@@ -230,6 +254,7 @@ static int admit(lmb_server *s)
         a.lat = nullptr;
         a.model = nullptr;
         a.done = 0;
+        a.solo = false;
         memset(&a.stats, 0, sizeof a.stats);
         lmb_model_desc d;
         d.number_species = a.req.ns;
@@ -248,6 +273,12 @@ static int admit(lmb_server *s)
         int rc = lmb_model_create(s->ctx, &d, a.req.X, a.req.Y, a.req.Z, &a.model);
         if (rc == LMB_OK) rc = lmb_lattice_create(s->ctx, a.req.X, a.req.Y, a.req.Z, s->slots, s->bps, &a.lat);
         if (rc == LMB_OK) rc = lmb_lattice_set_native(a.lat, a.req.particles.data(), a.req.sites.data());
+        const uint64_t nsites = (uint64_t)a.req.X * a.req.Y * a.req.Z;
+        a.solo = nsites >= SOLO_SITES;
+        if (rc == LMB_OK && a.solo) {
+            const double density = (double)count_particles(a.req.particles, s->bps) / (double)nsites;
+            if (density >= DENSE_PARTICLES_PER_SITE) rc = lmb_lattice_set_schedule(a.lat, LMB_SCHEDULE_PHASES, 0, 0);
+        }
         a.t_admit = now_s();
         if (rc != LMB_OK) {
             a.stats.status = rc;
@@ -257,8 +288,8 @@ static int admit(lmb_server *s)
         // Host copies are no longer needed once the lattice is on the device.
         std::vector<uint32_t>().swap(a.req.particles);
         std::vector<uint8_t>().swap(a.req.sites);
+        if (!a.solo) s->members_changed = true;
         s->active.push_back(std::move(a));
-        s->members_changed = true;
     }
     if (s->bytes_in_use > s->peak_bytes) s->peak_bytes = s->bytes_in_use;
     if (s->active.size() > s->peak_active) s->peak_active = (uint32_t)s->active.size();
@@ -272,27 +303,53 @@ extern "C" int lmb_server_step(lmb_server *s, uint32_t *active_out, uint32_t *qu
     if (rc) return rc;
     const uint32_t n = (uint32_t)s->active.size();
     if (n > 0) {
-        std::vector<lmb_lattice *> lats(n);
-        std::vector<const lmb_model *> models(n);
-        std::vector<uint32_t> seeds(n), firsts(n), counts(n);
+        std::vector<lmb_run_stats> st(n);
+        // Small solves: one batch, one launch per timestep for all of them.
+        std::vector<uint32_t> small;
+        for (uint32_t j = 0; j < n; j++)
+            if (!s->active[j].solo) small.push_back(j);
+        if (!small.empty()) {
+            const uint32_t nb = (uint32_t)small.size();
+            std::vector<lmb_lattice *> lats(nb);
+            std::vector<const lmb_model *> models(nb);
+            std::vector<uint32_t> seeds(nb), firsts(nb), counts(nb);
+            for (uint32_t q = 0; q < nb; q++) {
+                Active &a = s->active[small[q]];
+                lats[q] = a.lat;
+                models[q] = a.model;
+                seeds[q] = a.req.seed;
+                firsts[q] = a.done;
+                const uint32_t left = a.req.timesteps - a.done;
+                counts[q] = left < s->chunk ? left : s->chunk;
+            }
+            if (!s->batch) rc = lmb_batch_create(s->ctx, nb, lats.data(), models.data(), &s->batch);
+            else if (s->members_changed) rc = lmb_batch_set_lattices(s->batch, nb, lats.data(), models.data());
+            if (rc) return rc;
+            s->members_changed = false;
+            rc = lmb_batch_run_ranges_async(s->batch, seeds.data(), firsts.data(), counts.data(),
+                                            LMB_OVERFLOW_CLASSIC);
+            if (rc) return rc;
+            std::vector<lmb_run_stats> bst(nb);
+            rc = lmb_batch_wait(s->batch, bst.data());
+            if (rc != LMB_OK && rc != LMB_E_OVERFLOW_EXHAUSTED && rc != LMB_E_OVERFLOW_UNRESOLVED) return rc;
+            for (uint32_t q = 0; q < nb; q++) st[small[q]] = bst[q];
+        }
+        // Large solves, each filling the device alone, are served in arrival
+        // order: the oldest one runs its chunk in this step (the others wait
+        // their turn instead of all finishing late), while the small ones
+        // advance in the batch every step.
         for (uint32_t j = 0; j < n; j++) {
             Active &a = s->active[j];
-            lats[j] = a.lat;
-            models[j] = a.model;
-            seeds[j] = a.req.seed;
-            firsts[j] = a.done;
+            if (!a.solo) continue;
             const uint32_t left = a.req.timesteps - a.done;
-            counts[j] = left < s->chunk ? left : s->chunk;
+            rc = lmb_run_async(a.lat, a.model, a.req.seed, a.done, left < s->chunk ? left : s->chunk,
+                               LMB_OVERFLOW_CLASSIC);
+            if (rc) return rc;
+            rc = lmb_run_wait(a.lat, &st[j]);
+            if (rc != LMB_OK && rc != LMB_E_OVERFLOW_EXHAUSTED && rc != LMB_E_OVERFLOW_UNRESOLVED) return rc;
+            break;
         }
-        if (!s->batch) rc = lmb_batch_create(s->ctx, n, lats.data(), models.data(), &s->batch);
-        else if (s->members_changed) rc = lmb_batch_set_lattices(s->batch, n, lats.data(), models.data());
-        if (rc) return rc;
-        s->members_changed = false;
-        rc = lmb_batch_run_ranges_async(s->batch, seeds.data(), firsts.data(), counts.data(), LMB_OVERFLOW_CLASSIC);
-        if (rc) return rc;
-        std::vector<lmb_run_stats> st(n);
-        rc = lmb_batch_wait(s->batch, st.data());
-        if (rc != LMB_OK && rc != LMB_E_OVERFLOW_EXHAUSTED && rc != LMB_E_OVERFLOW_UNRESOLVED) return rc;
+        rc = LMB_OK;
         // Retire finished and failed solves; keep the order of the rest.
         std::vector<Active> keep;
         keep.reserve(n);
@@ -306,8 +363,8 @@ extern "C" int lmb_server_step(lmb_server *s, uint32_t *active_out, uint32_t *qu
                 a.stats.failed_step = st[j].failed_step;
             }
             if (a.stats.status != LMB_OK || a.done >= a.req.timesteps) {
+                if (!a.solo) s->members_changed = true;
                 retire(s, a);
-                s->members_changed = true;
             } else {
                 keep.push_back(std::move(a));
             }

@@ -122,6 +122,58 @@ __device__ __forceinline__ typename ChoiceCode<S>::type site_choices(const SiteW
     return c;
 }
 
+// Byte compaction: the bytes of word w whose bits are set in the 4-bit mask
+// m, moved to the low end in order (one byte permute; the selector of mask m
+// is entry m of a 16-entry table of 16-bit selectors, kept in four 64-bit
+// constants).
+__device__ __forceinline__ uint32_t compact_bytes(uint32_t w, uint32_t m)
+{
+    const unsigned long long q = m < 8u ? (m < 4u ? 0x4410444144404444ull : 0x4210442144204442ull)
+                                        : (m < 12u ? 0x4310443144304443ull : 0x3210432143204432ull);
+    return __byte_perm(w, 0u, (uint32_t)(q >> (16u * (m & 3u))) & 0xFFFFu);
+}
+
+// A site's bytes selected by an S-bit slot mask, packed from the low end of
+// a 128-bit value (lo, hi); n = number of bytes.  S <= 16.
+template <int S>
+__device__ __forceinline__ void compact_site(const uint32_t *w, uint32_t mask, unsigned long long &lo,
+                                             unsigned long long &hi, uint32_t &n)
+{
+    lo = 0;
+    hi = 0;
+    n = 0;
+#pragma unroll
+    for (int k = 0; k < S / 4; k++) {
+        const uint32_t m = (mask >> (4 * k)) & 0xFu;
+        const unsigned long long c = compact_bytes(w[k], m);
+        // Append the (up to 4) bytes at byte offset n (< 16).
+        const uint32_t sh = 8u * n;
+        if (sh < 64u) {
+            lo |= c << sh;
+            if (sh > 32u) hi |= c >> (64u - sh);
+        } else {
+            hi |= c << (sh - 64u);
+        }
+        n += __popc(m);
+    }
+}
+
+// (lo, hi) |= (a_lo, a_hi) << (8 * nb), for nb < 16 and bits beyond 128 dropped.
+__device__ __forceinline__ void or_shifted(unsigned long long &lo, unsigned long long &hi, unsigned long long a_lo,
+                                           unsigned long long a_hi, uint32_t nb)
+{
+    const uint32_t sh = 8u * nb;
+    if (sh == 0u) {
+        lo |= a_lo;
+        hi |= a_hi;
+    } else if (sh < 64u) {
+        lo |= a_lo << sh;
+        hi |= (a_hi << sh) | (a_lo >> (64u - sh));
+    } else {
+        hi |= a_lo << (sh - 64u);
+    }
+}
+
 // New content of a site after a sweep (byte_diffusion_1d_dev.cu:199-269):
 // its stayers in slot order, then the PLUS movers of the minus neighbour,
 // then the MINUS movers of the plus neighbour, each in slot order; the
@@ -138,6 +190,28 @@ __device__ __forceinline__ SiteWords<BPS, S> assemble_site(const SiteWords<BPS, 
                                                            OverflowEntry *list, uint32_t cap)
 {
     constexpr uint32_t LOW = S >= 32 ? 0xFFFFFFFFu : ((1u << S) - 1u);
+    if (BPS == 1 && S <= 16) {
+        // Byte lattices: three byte compactions and two shifts, no loop,
+        // unless the site overflows (then the ordered loop below queues the
+        // extra particles).
+        const uint32_t stay = occupied_slots<BPS, S>(own) & ~((uint32_t)c_own | (uint32_t)(c_own >> S)) & LOW;
+        const uint32_t in_m = (uint32_t)(c_mn >> S) & LOW, in_p = (uint32_t)c_pl & LOW;
+        const uint32_t total = __popc(stay) + __popc(in_m) + __popc(in_p);
+        if (total <= (uint32_t)S) {
+            unsigned long long lo, hi, blo, bhi, clo, chi;
+            uint32_t na, nb, nc;
+            compact_site<S>(own.w, stay, lo, hi, na);
+            compact_site<S>(mn.w, in_m, blo, bhi, nb);
+            compact_site<S>(pl.w, in_p, clo, chi, nc);
+            or_shifted(lo, hi, blo, bhi, na);
+            or_shifted(lo, hi, clo, chi, na + nb);
+            SiteWords<BPS, S> out;
+#pragma unroll
+            for (int k = 0; k < SiteWords<BPS, S>::W; k++)
+                out.w[k] = (uint32_t)((k < 2 ? lo : hi) >> (32 * (k & 1)));
+            return out;
+        }
+    }
     SiteBuilder<BPS, S> b;
     b.init();
     uint32_t stay = occupied_slots<BPS, S>(own) & ~((uint32_t)c_own | (uint32_t)(c_own >> S)) & LOW;
@@ -252,6 +326,22 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
 {
     float a = tload(m.qp0 + t);
     if (s.empty() && a == 0.0f) return false;
+    // The reaction probability below never exceeds the total propensity a
+    // (see the bound before the double exp), and a itself -- a float sum of
+    // qp0, one qp1 entry per particle and one qp2 entry per pair, at most 137
+    // terms -- never exceeds U = qp0 + n max(qp1) + n(n-1)/2 max(qp2) by more
+    // than its rounding, (1 + 2^-24)^136 < 1.0001.  So a draw above
+    // U * 1.0001 * (1 + 2^-20) + 2^-60 cannot react, and the table sums and
+    // the double exp are evaluated only for draws below that bound.
+    const float r0 = hash_float(((unsigned long long)gi << 1) | 0ull, th);
+    {
+        const float n = (float)__popc(occupied_slots<BPS, S>(s));
+        const float pairs = __fmul_rn(n, __fmul_rn(__fsub_rn(n, 1.0f), 0.5f));
+        float u = __fadd_ru(a, __fmul_ru(n, tload(m.qpmax + t)));
+        u = __fadd_ru(u, __fmul_ru(pairs, tload(m.qpmax + m.nst + t)));
+        u = __fmul_ru(u, 1.0001f);
+        if (r0 > __fadd_ru(__fmul_ru(u, 1.00000095367431640625f), 8.67361738e-19f)) return false;
+    }
     const size_t o1 = (size_t)t * m.ns, o2 = (size_t)t * m.ns * m.ns;
 #pragma unroll
     for (int k = 0; k < S; k++) {
@@ -266,7 +356,6 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
         }
     }
     if (a == 0.0f) return false;
-    const float r0 = hash_float(((unsigned long long)gi << 1) | 0ull, th);
     // prob = (float)(1 - exp(-a)) below never exceeds a: mathematically
     // 1 - e^-a < a for a > 0, the double evaluation adds at most a few units
     // of 2^-53, and rounding to float at most one float ulp of a.  A draw
@@ -278,11 +367,62 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
 
     float rp = __fmul_rn(hash_float(((unsigned long long)gi << 1) | 1ull, th), a);
     uint32_t idx = 0;
-    for (uint32_t rx = 0; rx < m.nr; rx++) {
-        const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
-        if (prop > 0.0f) {
-            if (rp > 0.0f) idx = rx;
-            rp = __fsub_rn(rp, prop);
+    // determineReactionIndex (byte_reaction_dev.cu:146-176) visits every
+    // reaction in index order; a reaction whose propensity is 0 changes
+    // nothing, and only the zeroth-order reactions and those whose first
+    // reactant is in the site can have a nonzero one.  So the same steps are
+    // taken over those candidates, merged into index order (the full scan
+    // when there are too many to hold).
+    constexpr int MAX_CAND = 64;
+    uint32_t cand[MAX_CAND];
+    int nc = 0;
+    bool all = false;
+    {
+        const uint32_t z0 = tload(m.rx_off), z1 = tload(m.rx_off + 1);
+        for (uint32_t e = z0; e < z1 && !all; e++) {
+            if (nc < MAX_CAND) cand[nc++] = tload(m.rx_list + e);
+            else all = true;
+        }
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            const uint32_t p = s.slot(k);
+            if (p > 0 && p <= m.ns && !all) {
+                const uint32_t e0 = tload(m.rx_off + p), e1 = tload(m.rx_off + p + 1);
+                for (uint32_t e = e0; e < e1; e++) {
+                    if (nc < MAX_CAND) cand[nc++] = tload(m.rx_list + e);
+                    else all = true;
+                }
+            }
+        }
+    }
+    if (all) {
+        for (uint32_t rx = 0; rx < m.nr; rx++) {
+            const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
+            if (prop > 0.0f) {
+                if (rp > 0.0f) idx = rx;
+                rp = __fsub_rn(rp, prop);
+            }
+        }
+    } else {
+        // Ascending order (insertion sort of a few entries); a species held
+        // twice contributes its list twice, so repeats are skipped.
+        for (int a = 1; a < nc; a++) {
+            const uint32_t v = cand[a];
+            int b = a - 1;
+            while (b >= 0 && cand[b] > v) {
+                cand[b + 1] = cand[b];
+                b--;
+            }
+            cand[b + 1] = v;
+        }
+        for (int q = 0; q < nc; q++) {
+            const uint32_t rx = cand[q];
+            if (q > 0 && rx == cand[q - 1]) continue;
+            const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
+            if (prop > 0.0f) {
+                if (rp > 0.0f) idx = rx;
+                rp = __fsub_rn(rp, prop);
+            }
         }
     }
     atomicAdd(&rs->reactions, 1ull);

@@ -119,18 +119,23 @@ def drain(server, limit=10000):
 def test_server_results_equal_solo_runs(ctx):
     from lattice_microbes_b200.solver import Server
     reqs = small_requests(12)
+    # Two large solves (>= 128 Ki sites) run their chunks on their own: one
+    # dense (per-phase kernels), one sparse (fused kernel).
+    for k, dens in ((12, 1.0), (13, 0.02)):
+        r = configs.ServeRequest(index=k, arrival=0.0, edge=56, ns=5, density=dens, timesteps=150, seed=99 + k)
+        reqs.append((r, _byte16(configs.serve_problem(r)), 4000 + k))
     srv = Server(ctx, slots=16, bytes_per_slot=1, max_active=5, chunk_timesteps=64)
-    for r, spec, seed in reqs[:7]:
+    for r, spec, seed in reqs[:7] + reqs[12:13]:
         srv.submit(r.index, spec, seed, r.timesteps)
     srv.step()
     srv.step()  # the rest arrive while the first ones are on the device
-    for r, spec, seed in reqs[7:]:
+    for r, spec, seed in reqs[7:12] + reqs[13:]:
         srv.submit(r.index, spec, seed, r.timesteps)
     results = drain(srv)
     st = srv.status()
     assert st.peak_active == 5 and st.active == 0 and st.bytes_in_use == 0
     srv.close()
-    assert sorted(results) == list(range(12))
+    assert sorted(results) == list(range(14))
     for r, spec, seed in reqs:
         info, lat, counts = results[r.index]
         assert info.stats.status == 0 and info.stats.steps_done == r.timesteps
