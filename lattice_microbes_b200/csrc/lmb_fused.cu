@@ -43,24 +43,40 @@ __device__ __forceinline__ void store_smem(uint32_t *buf, uint32_t R, uint32_t l
     for (int k = 0; k < SiteWords<BPS, S>::W; k++) buf[(size_t)k * R + l] = s.w[k];
 }
 
-// Copies the model tables into shared memory at `dst` (stage_bytes long,
-// 16-byte aligned pieces) and returns a table set pointing there.
+// Copies the model tables into shared memory at `dst` (16-byte aligned;
+// stage_bytes long, each table at a 16-byte boundary) and returns a table set
+// pointing there.  The device tables sit at 256-byte boundaries of one block
+// (zero padded), so the copy moves whole 16-byte granules, every thread's
+// loads independent of each other.
+constexpr int NTABLES = 15;
 __device__ __forceinline__ DevTables stage_tables(const DevTables &m, uint8_t *dst, uint32_t tid, uint32_t nthr)
 {
     DevTables s = m;
-    const void *srcs[15] = {m.T, m.qp0, m.qp1, m.qp2, m.order, m.D1, m.D2, m.rate, m.RL, m.stoich_off,
-                            m.stoich_sp, m.stoich_d, m.qpmax, m.rx_off, m.rx_list};
-    const uint32_t sizes[15] = {m.nst * m.nst * m.ns * 4, m.nst * 4, m.nst * m.ns * 4, m.nst * m.ns * m.ns * 4,
-                                m.nr * 4, m.nr * 4, m.nr * 4, m.nr * 4, m.nr * m.nst, (m.nr + 1) * 4, m.nnz * 4,
-                                m.nnz * 4, 2 * m.nst * 4, (m.ns + 2) * 4, m.nr * 4};
-    void *outs[15];
-    uint32_t off = 0;
-    for (int k = 0; k < 15; k++) {
-        outs[k] = dst + off;
-        const uint8_t *sp = (const uint8_t *)srcs[k];
-        for (uint32_t b = tid; b < sizes[k]; b += nthr) dst[off + b] = sp[b];
-        off += (sizes[k] + 15u) & ~15u;
+    const void *srcs[NTABLES] = {m.T, m.qp0, m.qp1, m.qp2, m.order, m.D1, m.D2, m.rate, m.RL, m.stoich_off,
+                                 m.stoich_sp, m.stoich_d, m.qpmax, m.rx_off, m.rx_list};
+    const uint32_t sizes[NTABLES] = {m.nst * m.nst * m.ns * 4, m.nst * 4, m.nst * m.ns * 4,
+                                     m.nst * m.ns * m.ns * 4, m.nr * 4, m.nr * 4, m.nr * 4, m.nr * 4,
+                                     m.nr * m.nst, (m.nr + 1) * 4, m.nnz * 4, m.nnz * 4, 2 * m.nst * 4,
+                                     (m.ns + 2) * 4, m.nr * 4};
+    uint32_t first[NTABLES + 1];
+    first[0] = 0;
+#pragma unroll
+    for (int k = 0; k < NTABLES; k++) first[k + 1] = first[k] + (sizes[k] + 15u) / 16u;
+    uint4 *out = (uint4 *)dst;
+    for (uint32_t gr = tid; gr < first[NTABLES]; gr += nthr) {
+        const uint4 *src = (const uint4 *)srcs[0];
+        uint32_t f = 0;
+#pragma unroll
+        for (int j = 1; j < NTABLES; j++)
+            if (gr >= first[j]) {
+                src = (const uint4 *)srcs[j];
+                f = first[j];
+            }
+        out[gr] = __ldg(src + (gr - f));
     }
+    const void *outs[NTABLES];
+#pragma unroll
+    for (int k = 0; k < NTABLES; k++) outs[k] = dst + 16u * first[k];
     s.T = (const float *)outs[0];
     s.qp0 = (const float *)outs[1];
     s.qp1 = (const float *)outs[2];
@@ -169,7 +185,7 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     uint8_t *T = (uint8_t *)(work + R);
     uint32_t *occA = (uint32_t *)(T + ((R + 15u) & ~15u));
     uint32_t *occB = occA + rows * MW;
-    uint8_t *tables = (uint8_t *)(occB + rows * MW);
+    uint8_t *tables = (uint8_t *)(((uintptr_t)(occB + rows * MW) + 15u) & ~(uintptr_t)15u);
     // The model tables, from shared memory when they are small; the table set
     // itself is kept in shared memory so that calls take it by reference
     // without a per-thread copy.
@@ -197,7 +213,7 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
         // into the row's mask word.  Up to four items in flight per thread.
         for (uint32_t i = tid; i < rows * MW; i += nthr) occA[i] = 0u;
         const uint32_t q4 = X / 4, nq = rows * q4;
-        constexpr int U = W >= 4 ? 1 : 4 / W;
+        constexpr int U = W >= 4 ? 2 : 8 / W;
         __syncthreads();
         for (uint32_t i0 = tid; i0 < nq; i0 += U * nthr) {
             uint4 v[U][W];
@@ -461,7 +477,7 @@ static size_t region_bytes(uint32_t X, uint32_t Ty, uint32_t Tz, uint32_t W)
 
 size_t fused_smem_bytes(const TileShape &ts, uint32_t X, uint32_t W, uint32_t cap, uint32_t stage_bytes)
 {
-    const size_t tile = region_bytes(X, ts.Ty, ts.Tz, W) + stage_bytes;
+    const size_t tile = region_bytes(X, ts.Ty, ts.Tz, W) + 16 + stage_bytes;
     const size_t sort = (size_t)pow2_at_least(cap) * sizeof(OverflowEntry);
     return tile > sort ? tile : sort;
 }
