@@ -81,6 +81,22 @@ struct SiteWords {
 #pragma unroll
         for (int k = 0; k < W; k++) lat[(size_t)k * N + i] = w[k];
     }
+    // Loads a packed site (occupied slots first, as every sweep writes them)
+    // touching only the word planes that hold particles: plane k + 1 is read
+    // only when plane k is full (every slot of a byte word, or the one slot
+    // of an int word, occupied); the other planes are zero.
+    __device__ __forceinline__ void load_packed(const uint32_t *lat, uint32_t N, uint32_t i)
+    {
+        clear();
+        bool more = true;
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+            if (more) {
+                w[k] = lat[(size_t)k * N + i];
+                more = BPS == 1 ? (w[k] >> 24) != 0u : w[k] != 0u;
+            }
+        }
+    }
     __device__ __forceinline__ uint32_t slot(int k) const
     {
         if (BPS == 1) return (w[k >> 2] >> (8 * (k & 3))) & 0xFFu;

@@ -274,7 +274,10 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
     if (i >= g.N) return;
     const uint32_t t = __ldg(sites + i);
     SiteWords<BPS, S> s;
-    s.load_plain(lat, g.N, i);
+    // The z sweep wrote this buffer, so its sites are packed (occupied slots
+    // first, whatever the input had): only the planes holding particles are
+    // read.
+    s.load_packed(lat, g.N, i);
     const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
     if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) s.store(lat, g.N, i);
 }

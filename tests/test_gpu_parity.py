@@ -272,3 +272,78 @@ def test_graph_replay_long_run_vs_oracle(ctx, schedule):
     assert sum(s.overflows for s in st) == st_ref.overflows
     assert sum(s.reactions for s in st) == st_ref.reactions
     assert np.array_equal(out, ref)
+
+
+def _busy_problem(seed, promiscuous):
+    """Many species and reactions on a small Int-16 lattice, with fast
+    reactions so that sites react every few timesteps: exercises the
+    candidate-reaction scan (and, when `promiscuous`, its full-scan fallback:
+    one species is the first reactant of 80 reactions) and the propensity
+    bound of the reaction step."""
+    spec = configs.config2(seed=seed, X=32, Y=16, Z=16, ns=60, nr=150, nparticles=12000, nst=4,
+                           obstacle_fraction=0.1)
+    spec.tau = 2e-4  # larger rates per timestep
+    if promiscuous:
+        R = spec.nr
+        for j in range(80):
+            spec.S[:, j] = 0
+            spec.D[:, j] = 0
+            spec.rtype[j] = configs.FIRST
+            spec.K[j] = 50.0
+            spec.S[0, j] = -1
+            spec.D[0, j] = 1
+            spec.S[1 + j % (spec.ns - 1), j] += 1
+        assert R == spec.nr
+    # D limited so that q stays <= 0.5 at the longer timestep.
+    spec.DF = np.minimum(spec.DF, 0.45 * spec.spacing ** 2 / spec.tau)
+    return spec
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
+@pytest.mark.parametrize("promiscuous", [False, True])
+def test_many_reactions_vs_oracle(ctx, schedule, promiscuous):
+    spec = _busy_problem(21, promiscuous)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 4242, 0, 12)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 4242, 0, 12, schedule=schedule)
+    assert rc == rc_ref == 0
+    assert st_ref.reactions > 50  # the reaction step really fires
+    assert st[0].reactions == st_ref.reactions
+    assert np.array_equal(out, ref)
+
+
+def _with_holes(spec, seed=3):
+    """The same particles with holes: in a third of the occupied sites the
+    first particle moves to the last slot (an empty slot now precedes
+    occupied ones).  The reference processes every nonzero slot, holes or
+    not (byte_diffusion_1d_dev.cu:100-118), and keys each draw by its slot."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z, S, b = spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot
+    slots = configs.native_to_slots(spec.lattice, X, Y, Z, S, b).copy()
+    occ = (slots != 0).sum(axis=1)
+    pick = np.nonzero((occ >= 1) & (occ < S) & (rng.random(len(occ)) < 0.33))[0]
+    slots[pick, S - 1] = slots[pick, 0]
+    slots[pick, 0] = 0
+    N = spec.nsites
+    lat = configs.empty_lattice(X, Y, Z, S, b)
+    for k in range(S):
+        v = slots[:, k].astype(np.uint32)
+        if b == 1:
+            lat[(k // 4) * N:(k // 4 + 1) * N] |= v << np.uint32(8 * (k % 4))
+        else:
+            lat[k * N:(k + 1) * N] = v
+    spec.lattice = lat
+    return spec
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
+@pytest.mark.parametrize("slots,bps", [(8, 1), (16, 1), (16, 4)])
+def test_lattice_with_holes_vs_oracle(ctx, schedule, slots, bps):
+    spec = _with_holes(configs.random_problem(31, X=32, Y=8, Z=8, slots=slots, bytes_per_slot=bps, density=1.2,
+                                              nst=2))
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 777, 0, 9)
+    # In pieces: the holes flag must survive a one-timestep run.
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 777, 0, 9, schedule=schedule, chunks=[1, 1, 7])
+    assert rc == rc_ref == 0
+    assert np.array_equal(out, ref)
