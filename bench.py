@@ -101,6 +101,14 @@ def parse():
 # CPU side: the reference's code on the host cores
 # --------------------------------------------------------------------------
 
+def host_cores():
+    """Host threads this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
 def _cpu_worker(args):
     """One replicate of the reference MPD device functions on one core (spawned)."""
     workload, seed, timesteps = args

@@ -8,13 +8,14 @@
 //
 // Sweep design: one thread per site; a block covers a tile of sites that is
 // long along the sweep axis (x rows for the x sweep, 8 y rows or 8 z planes
-// for the y and z sweeps).  Each thread draws its own site's hop choices once
-// (one hash per particle), publishes the site and its choices in shared
-// memory, and assembles its new site from its own and its two neighbours'
-// entries.  A neighbour outside the tile is loaded and its choices drawn
-// again by the thread that needs it; every decision is a pure function of
-// (seed, step, site, slot, site types), so the copies agree.  Empty
-// neighbourhoods take a store-only path.
+// for the y and z sweeps, plus a halo row of threads on either side that
+// only reads).  Each thread draws its own site's hop choices once (one hash
+// per particle, balanced over the warp), publishes the site and its choices
+// in shared memory, and the tile's threads assemble their new sites from
+// their own and their two neighbours' entries.  Halo rows and the ends of x
+// rows longer than 256 sites draw a neighbour's choices a second time; every
+// decision is a pure function of (seed, step, site, slot, site types), so the
+// copies agree.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -30,58 +31,85 @@ namespace lmb {
 // Diffusion sweep
 // ---------------------------------------------------------------------------
 
+// Sites written by one block, and threads of a y or z block: its tile plus
+// one halo row of threads on either side along the sweep axis.
 constexpr int SWEEP_THREADS = 256;
+constexpr int SWEEP_MAX_THREADS = 320;
 
-// Site coordinates of the thread and its neighbours along axis DIM
-// (periodic), and where a neighbour sits in the block's tile (-1: outside).
+// Lattice coordinates of the thread's site.  x tiles are whole x rows (or
+// 256-site pieces of longer rows); y and z tiles carry a halo row on either
+// side, so thread row r of a tile starting at a0 holds axis coordinate
+// a0 - 1 + r, wrapped periodically.  Rows past the wrap point (a0 - 1 + r >
+// extent) hold no site; a row at exactly the extent holds coordinate 0 and is
+// read but not written.
 template <int DIM>
-__device__ __forceinline__ void sweep_neighbours(const Geometry &g, uint32_t x, uint32_t y, uint32_t z,
+__device__ __forceinline__ void sweep_site_of(const Geometry &g, uint32_t &x, uint32_t &y, uint32_t &z, bool &in,
+                                              bool &out)
+{
+    x = blockIdx.x * blockDim.x + threadIdx.x;
+    y = blockIdx.y * blockDim.y + threadIdx.y;
+    z = blockIdx.z * blockDim.z + threadIdx.z;
+    if (DIM == 0) {
+        in = out = x < g.X && y < g.Y && z < g.Z;
+        return;
+    }
+    const uint32_t A = DIM == 1 ? g.Y : g.Z;
+    const uint32_t r = DIM == 1 ? threadIdx.y : threadIdx.z;
+    const uint32_t L = (DIM == 1 ? blockDim.y : blockDim.z) - 2u;
+    const int64_t u = (int64_t)(DIM == 1 ? blockIdx.y : blockIdx.z) * L - 1 + r;
+    const uint32_t a = u < 0 ? A - 1u : (u >= (int64_t)A ? 0u : (uint32_t)u);
+    if (DIM == 1) y = a;
+    else z = a;
+    in = x < g.X && (DIM == 1 ? z < g.Z : y < g.Y) && u <= (int64_t)A;
+    out = in && r >= 1u && r <= L && u < (int64_t)A;
+}
+
+// Lattice indices of the site and its two neighbours along axis DIM
+// (periodic); for the x sweep also where the neighbours sit in the block's
+// tile (-1: outside).  In y and z tiles they are the thread rows either side.
+template <int DIM>
+__device__ __forceinline__ void sweep_neighbours(const Geometry &g, uint32_t x, uint32_t y, uint32_t z, int lid,
                                                  uint32_t &i, uint32_t &im, uint32_t &ip, int &lm, int &lp)
 {
-    const uint32_t bx = blockDim.x, by = blockDim.y;
-    const int lid = (int)(threadIdx.x + bx * (threadIdx.y + by * threadIdx.z));
     i = x + y * g.X + z * g.XY;
     if (DIM == 0) {
         const uint32_t xm = x == 0 ? g.X - 1 : x - 1, xp = x == g.X - 1 ? 0 : x + 1;
         im = i - x + xm;
         ip = i - x + xp;
-        const uint32_t x0 = blockIdx.x * bx;
-        lm = (xm >= x0 && xm < x0 + bx) ? lid - (int)x + (int)xm : -1;
-        lp = (xp >= x0 && xp < x0 + bx) ? lid - (int)x + (int)xp : -1;
+        const uint32_t x0 = blockIdx.x * blockDim.x;
+        lm = (xm >= x0 && xm < x0 + blockDim.x) ? lid - (int)x + (int)xm : -1;
+        lp = (xp >= x0 && xp < x0 + blockDim.x) ? lid - (int)x + (int)xp : -1;
     } else if (DIM == 1) {
         const uint32_t ym = y == 0 ? g.Y - 1 : y - 1, yp = y == g.Y - 1 ? 0 : y + 1;
         im = i - y * g.X + ym * g.X;
         ip = i - y * g.X + yp * g.X;
-        const uint32_t y0 = blockIdx.y * by;
-        lm = (ym >= y0 && ym < y0 + by) ? lid + ((int)ym - (int)y) * (int)bx : -1;
-        lp = (yp >= y0 && yp < y0 + by) ? lid + ((int)yp - (int)y) * (int)bx : -1;
+        lm = lid - (int)blockDim.x;
+        lp = lid + (int)blockDim.x;
     } else {
         const uint32_t zm = z == 0 ? g.Z - 1 : z - 1, zp = z == g.Z - 1 ? 0 : z + 1;
         im = i - z * g.XY + zm * g.XY;
         ip = i - z * g.XY + zp * g.XY;
-        const uint32_t z0 = blockIdx.z * blockDim.z;
-        lm = (zm >= z0 && zm < z0 + blockDim.z) ? lid + ((int)zm - (int)z) * (int)(bx * by) : -1;
-        lp = (zp >= z0 && zp < z0 + blockDim.z) ? lid + ((int)zp - (int)z) * (int)(bx * by) : -1;
+        lm = lid - (int)(blockDim.x * blockDim.y);
+        lp = lid + (int)(blockDim.x * blockDim.y);
     }
 }
 
 template <int BPS, int S, int DIM>
-__global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__restrict__ src,
-                                                              uint32_t *__restrict__ dst,
-                                                              const uint8_t *__restrict__ sites, Geometry g,
-                                                              DevTables m, RunState *__restrict__ rs,
-                                                              OverflowEntry *__restrict__ list, uint32_t cap)
+__global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t *__restrict__ src,
+                                                                  uint32_t *__restrict__ dst,
+                                                                  const uint8_t *__restrict__ sites, Geometry g,
+                                                                  DevTables m, RunState *__restrict__ rs,
+                                                                  OverflowEntry *__restrict__ list, uint32_t cap)
 {
     using Code = typename ChoiceCode<S>::type;
     constexpr int W = SiteWords<BPS, S>::W;
-    __shared__ uint32_t sw[W][SWEEP_THREADS];
-    __shared__ Code sc[SWEEP_THREADS];
-    __shared__ uint8_t st[SWEEP_THREADS];
+    constexpr int NT = DIM == 0 ? SWEEP_THREADS : SWEEP_MAX_THREADS;
+    __shared__ uint32_t sw[W][NT];
+    __shared__ Code sc[NT];
     if (rs->status != LMB_OK) return;
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
-    const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
-    const bool in = x < g.X && y < g.Y && z < g.Z;
+    uint32_t x, y, z;
+    bool in, out;
+    sweep_site_of<DIM>(g, x, y, z, in, out);
     const int lid = (int)(threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z));
     uint32_t i = 0, im = 0, ip = 0;
     int lm = -1, lp = -1;
@@ -92,7 +120,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
     const unsigned long long th = timestep_hash(rs->seed, rs->step, DIM);
     uint32_t occ = 0;
     if (in) {
-        sweep_neighbours<DIM>(g, x, y, z, i, im, ip, lm, lp);
+        sweep_neighbours<DIM>(g, x, y, z, lid, i, im, ip, lm, lp);
         own.load(src, g.N, i);
         t = __ldg(sites + i);
         tm = __ldg(sites + im);
@@ -100,7 +128,6 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
         occ = occupied_slots<BPS, S>(own);
 #pragma unroll
         for (int k = 0; k < W; k++) sw[k][lid] = own.w[k];
-        st[lid] = (uint8_t)t;
     }
     sc[lid] = 0;
     __syncwarp();
@@ -109,7 +136,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
     // same number of particles however unevenly the sites are filled.
     {
         constexpr int CB = CountBits<S>::value;
-        const uint32_t lane = threadIdx.x & 31u, wbase = (uint32_t)lid & ~31u;
+        const uint32_t lane = (uint32_t)lid & 31u, wbase = (uint32_t)lid & ~31u;
         const uint32_t n = __popc(occ);
         uint32_t incl = n;
 #pragma unroll
@@ -147,7 +174,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
         }
     }
     __syncthreads();
-    if (!in) return;
+    if (!out) return;
     c_own = sc[lid];
     // Lattice index of the neighbour's own outer neighbour along the axis.
     auto outer_minus = [&]() {
@@ -177,6 +204,9 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
         // global memory rather than selected among S registers; the new site
         // is gathered in shared memory and written plane by plane.
         __shared__ uint32_t so[S][SWEEP_THREADS];
+        // Index among the block's written sites (the halo row of a y or z
+        // tile comes first).
+        const int oid = DIM == 0 ? lid : lid - (DIM == 1 ? (int)blockDim.x : (int)(blockDim.x * blockDim.y));
         constexpr int CB = CountBits<S>::value;
         constexpr uint32_t LOW = (1u << S) - 1u;
         auto choices_mem = [&](uint32_t idx, uint32_t occ_n, uint32_t t_n, uint32_t tm_n, uint32_t tp_n) {
@@ -192,7 +222,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
             return c;
         };
         Code c_mn = 0, c_pl = 0;
-        if (lm >= 0) {
+        if (DIM != 0 || lm >= 0) {
             c_mn = sc[lm];
         } else {
             SiteWords<BPS, S> mn;
@@ -200,7 +230,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
             const uint32_t o = occupied_slots<BPS, S>(mn);
             if (o) c_mn = choices_mem(im, o, tm, __ldg(sites + outer_minus()), t);
         }
-        if (lp >= 0) {
+        if (DIM != 0 || lp >= 0) {
             c_pl = sc[lp];
         } else {
             SiteWords<BPS, S> pl;
@@ -210,7 +240,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
         }
         uint32_t n = 0;
         auto push = [&](uint32_t p) {
-            if (n < (uint32_t)S) so[n][lid] = p;
+            if (n < (uint32_t)S) so[n][oid] = p;
             else push_overflow(rs, list, cap, (uint32_t)DIM + 1, i, n - (uint32_t)S, p);
             n++;
         };
@@ -224,21 +254,21 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
         while (in_m) {
             const uint32_t k = __ffs(in_m) - 1;
             in_m &= in_m - 1;
-            push(lm >= 0 ? sw[k][lm] : __ldg(src + (size_t)k * g.N + im));
+            push(DIM != 0 || lm >= 0 ? sw[k][lm] : __ldg(src + (size_t)k * g.N + im));
         }
         uint32_t in_p = (uint32_t)c_pl & LOW;
         while (in_p) {
             const uint32_t k = __ffs(in_p) - 1;
             in_p &= in_p - 1;
-            push(lp >= 0 ? sw[k][lp] : __ldg(src + (size_t)k * g.N + ip));
+            push(DIM != 0 || lp >= 0 ? sw[k][lp] : __ldg(src + (size_t)k * g.N + ip));
         }
 #pragma unroll
-        for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][lid] : 0u;
+        for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][oid] : 0u;
     } else {
         // The neighbours: from the tile, or loaded with their choices drawn here.
         SiteWords<BPS, S> mn, pl;
         Code c_mn = 0, c_pl = 0;
-        if (lm >= 0) {
+        if (DIM != 0 || lm >= 0) {
 #pragma unroll
             for (int k = 0; k < W; k++) mn.w[k] = sw[k][lm];
             c_mn = sc[lm];
@@ -246,7 +276,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS) sweep_kernel(const uint32_t *__
             mn.load(src, g.N, im);
             if (!mn.empty()) c_mn = site_choices<BPS, S>(mn, tm, __ldg(sites + outer_minus()), t, im, th, m);
         }
-        if (lp >= 0) {
+        if (DIM != 0 || lp >= 0) {
 #pragma unroll
             for (int k = 0; k < W; k++) pl.w[k] = sw[k][lp];
             c_pl = sc[lp];
@@ -479,29 +509,31 @@ __global__ void native_to_row_major_kernel(const uint32_t *__restrict__ native, 
 // Launchers
 // ---------------------------------------------------------------------------
 
-// Tiles long along the sweep axis: whole x rows (up to 256 sites) for x,
-// 32 x 8 sites in the x-y plane for y, 32 x 8 in the x-z plane for z.
+// Tiles long along the sweep axis: whole x rows (up to 256 sites) for x; for
+// y and z, 32 x 8 sites in the x-y or x-z plane (wider when the axis is
+// shorter than 8) launched with one halo row of threads on either side.
+// Every block is a whole number of warps.
 static void sweep_shape(const Geometry &g, int dim, dim3 &grid, dim3 &block)
 {
+    const uint32_t xw = ((g.X + 31) / 32) * 32;
     if (dim == 0) {
-        uint32_t bx = ((g.X + 31) / 32) * 32;
-        if (bx > 256) bx = 256;
+        const uint32_t bx = xw > 256 ? 256 : xw;
         uint32_t by = 256 / bx;
         if (by > g.Y) by = g.Y;
         block = dim3(bx, by, 1);
         grid = dim3((g.X + bx - 1) / bx, (g.Y + by - 1) / by, g.Z);
-    } else if (dim == 1) {
-        const uint32_t by = g.Y < 8 ? g.Y : 8;
-        uint32_t bx = 256 / by;
-        if (bx > ((g.X + 31) / 32) * 32) bx = ((g.X + 31) / 32) * 32;
-        block = dim3(bx, by, 1);
-        grid = dim3((g.X + bx - 1) / bx, (g.Y + by - 1) / by, g.Z);
+        return;
+    }
+    const uint32_t A = dim == 1 ? g.Y : g.Z;
+    const uint32_t L = A < 8 ? A : 8;
+    uint32_t bx = (SWEEP_MAX_THREADS / (L + 2)) & ~31u;
+    if (bx > xw) bx = xw;
+    if (dim == 1) {
+        block = dim3(bx, L + 2, 1);
+        grid = dim3((g.X + bx - 1) / bx, (g.Y + L - 1) / L, g.Z);
     } else {
-        const uint32_t bz = g.Z < 8 ? g.Z : 8;
-        uint32_t bx = 256 / bz;
-        if (bx > ((g.X + 31) / 32) * 32) bx = ((g.X + 31) / 32) * 32;
-        block = dim3(bx, 1, bz);
-        grid = dim3((g.X + bx - 1) / bx, g.Y, (g.Z + bz - 1) / bz);
+        block = dim3(bx, 1, L + 2);
+        grid = dim3((g.X + bx - 1) / bx, g.Y, (g.Z + L - 1) / L);
     }
 }
 

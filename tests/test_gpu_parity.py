@@ -97,6 +97,21 @@ def test_odd_shapes_vs_oracle(ctx, shape, schedule):
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("slots,bps", [(8, 1), (16, 1), (16, 4), (4, 4)])
+@pytest.mark.parametrize("shape", [(96, 3, 5), (300, 4, 12), (40, 12, 9), (33, 1, 2), (64, 2, 17)])
+def test_sweep_tiles_vs_oracle(ctx, shape, slots, bps):
+    """Per-phase sweeps on shapes that exercise every tile form: x rows longer
+    than one block, y and z axes shorter than a tile, tiles cut off by the
+    end of the axis, blocks wider than the lattice, dense sites."""
+    X, Y, Z = shape
+    spec = configs.random_problem(11, X=X, Y=Y, Z=Z, slots=slots, bytes_per_slot=bps, density=0.4 * slots, nst=3)
+    t = oracle_tables(spec)
+    ref, rc_ref, _ = oracle_run(t, spec.lattice, spec.sites, 7, 3, 6)
+    out, rc, _ = _gpu_run(ctx, t, spec.lattice, spec.sites, 7, 3, 6, schedule="phases")
+    assert rc == rc_ref
+    assert np.array_equal(out, ref)
+
+
 @pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("slots,bps,dens", [(8, 1, 5.0), (16, 4, 12.0), (8, 4, 6.0)])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
