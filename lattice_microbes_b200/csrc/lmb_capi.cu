@@ -63,6 +63,10 @@ struct lmb_lattice {
     RunState *rs_host;  // pinned
     OverflowEntry *list;
     uint32_t cap;
+    // Per-phase schedule: sites the z sweep lists for the reaction step
+    // (allocated when the schedule is first chosen).
+    uint32_t *rx_sites;
+    uint32_t rx_cap;
     unsigned long long *counts_dev;
     uint32_t counts_len;
     bool validated;
@@ -594,15 +598,32 @@ extern "C" int lmb_lattice_create(lmb_ctx *c, uint32_t X, uint32_t Y, uint32_t Z
         return cuda_status(e);
     }
     l->validated = false;
-    l->schedule = fused_default_shape(l->g, (int)bps, (int)slots, l->tile) ? LMB_SCHEDULE_FUSED : LMB_SCHEDULE_PHASES;
+    l->schedule = LMB_SCHEDULE_FUSED;
+    if (!fused_default_shape(l->g, (int)bps, (int)slots, l->tile)) {
+        const int rc = lmb_lattice_set_schedule(l, LMB_SCHEDULE_PHASES, 0, 0);
+        if (rc != LMB_OK) {
+            lmb_lattice_destroy(l);
+            return rc;
+        }
+    }
     *out = l;
     return LMB_OK;
 }
+
+// Room for one eighth of the sites plus 4096: sparse lattices list a small
+// fraction of their sites; denser ones overflow it and react over every site.
+static uint32_t reaction_list_capacity(const Geometry &g) { return g.N / 8 + 4096; }
 
 extern "C" int lmb_lattice_set_schedule(lmb_lattice *l, int schedule, uint32_t Ty, uint32_t Tz)
 {
     if (!l) return LMB_E_ARG;
     if (schedule == LMB_SCHEDULE_PHASES) {
+        if (!l->rx_sites) {
+            CK(cudaSetDevice(l->ctx->device));
+            const uint32_t cap = reaction_list_capacity(l->g);
+            CK(cudaMalloc(&l->rx_sites, (size_t)cap * sizeof(uint32_t)));
+            l->rx_cap = cap;
+        }
         l->schedule = schedule;
         return LMB_OK;
     }
@@ -635,6 +656,7 @@ extern "C" int lmb_lattice_destroy(lmb_lattice *l)
     if (l->sites) cudaFree(l->sites);
     if (l->rs) cudaFree(l->rs);
     if (l->list) cudaFree(l->list);
+    if (l->rx_sites) cudaFree(l->rx_sites);
     if (l->counts_dev) cudaFree(l->counts_dev);
     if (l->rs_host) cudaFreeHost(l->rs_host);
     for (auto &gr : l->graph)
@@ -785,12 +807,19 @@ static cudaError_t enqueue_step(lmb_lattice *l, lmb_model *m, cudaStream_t st)
         l->cur ^= 1;
         return e;
     }
-    if ((e = launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess) return e;
-    if ((e = launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess) return e;
-    if ((e = launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess) return e;
+    uint32_t *rx = m->nr > 0 ? l->rx_sites : nullptr;
+    if ((e = launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, st)) !=
+        cudaSuccess)
+        return e;
+    if ((e = launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, st)) !=
+        cudaSuccess)
+        return e;
+    if ((e = launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap, st)) !=
+        cudaSuccess)
+        return e;
     l->cur ^= 1;
-    if (m->nr > 0 &&
-        (e = launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, st)) != cudaSuccess)
+    if (m->nr > 0 && (e = launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap,
+                                          rx, l->rx_cap, st)) != cudaSuccess)
         return e;
     return launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, st);
 }
@@ -964,18 +993,20 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
             continue;
         }
         CK(cudaEventRecord(E[0], c->stream));
-        CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        uint32_t *rx = m->nr > 0 ? l->rx_sites : nullptr;
+        CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, c->stream));
         CK(cudaEventRecord(E[1], c->stream));
         CK(cudaEventRecord(E[2], c->stream));
-        CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, c->stream));
         CK(cudaEventRecord(E[3], c->stream));
         CK(cudaEventRecord(E[4], c->stream));
-        CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap, c->stream));
         CK(cudaEventRecord(E[5], c->stream));
         l->cur ^= 1;
         CK(cudaEventRecord(E[6], c->stream));
         if (m->nr > 0)
-            CK(launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+            CK(launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap,
+                               c->stream));
         CK(cudaEventRecord(E[7], c->stream));
         CK(cudaEventRecord(E[8], c->stream));
         CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, c->stream));

@@ -86,16 +86,20 @@ struct RunState {
     uint32_t max_species; // validation scratch
     uint32_t max_site_type;
     uint32_t tiles_done;  // fused kernel: blocks finished in this launch
-    uint32_t pad_;
+    uint32_t rx_count;    // per-phase schedule: sites the z sweep listed for the reaction step
 };
 
 // Kernel launchers (lmb_kernels.cu).  Each returns a cudaError_t.
+// The z sweep (dim 2) lists in rx_sites the sites whose reaction step could
+// change them, when rx_sites is given; launch_reaction then visits only
+// those (every site when the list is absent or overflowed rx_cap).
 cudaError_t launch_sweep(int bytes_per_slot, int slots, int dim, const uint32_t *src, uint32_t *dst,
                          const uint8_t *sites, const Geometry &g, const DevTables &m, RunState *rs,
-                         OverflowEntry *list, uint32_t cap, cudaStream_t stream);
+                         OverflowEntry *list, uint32_t cap, uint32_t *rx_sites, uint32_t rx_cap,
+                         cudaStream_t stream);
 cudaError_t launch_reaction(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
                             const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list,
-                            uint32_t cap, cudaStream_t stream);
+                            uint32_t cap, const uint32_t *rx_sites, uint32_t rx_cap, cudaStream_t stream);
 cudaError_t launch_resolve(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
                            const Geometry &g, RunState *rs, OverflowEntry *list, uint32_t cap,
                            cudaStream_t stream);

@@ -94,12 +94,37 @@ __device__ __forceinline__ void sweep_neighbours(const Geometry &g, uint32_t x, 
     }
 }
 
+// Appends site i (type t, n particles after the z sweep) to the reaction
+// list when its reaction step could change it (reaction_may_fire), one
+// atomic per group of converged lanes.  Entries past rx_cap are dropped but
+// counted, which sends the reaction step over every site.
+__device__ __forceinline__ void list_for_reaction(uint32_t n, uint32_t t, uint32_t i, int lid, const DevTables &m,
+                                                  RunState *rs, uint32_t *rx_sites, uint32_t rx_cap)
+{
+    const float a0 = tload(m.qp0 + t);
+    bool need = false;
+    if (n != 0 || a0 != 0.0f) {
+        const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
+        need = reaction_may_fire(n, a0, t, hash_float((unsigned long long)i << 1, th), m);
+    }
+    const uint32_t act = __activemask();
+    const uint32_t want = __ballot_sync(act, need);
+    if (!need) return;
+    const uint32_t lane = (uint32_t)lid & 31u, leader = __ffs(want) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&rs->rx_count, (uint32_t)__popc(want));
+    base = __shfl_sync(want, base, leader);
+    const uint32_t idx = base + __popc(want & ((1u << lane) - 1u));
+    if (idx < rx_cap) rx_sites[idx] = i;
+}
+
 template <int BPS, int S, int DIM>
 __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t *__restrict__ src,
                                                                   uint32_t *__restrict__ dst,
                                                                   const uint8_t *__restrict__ sites, Geometry g,
                                                                   DevTables m, RunState *__restrict__ rs,
-                                                                  OverflowEntry *__restrict__ list, uint32_t cap)
+                                                                  OverflowEntry *__restrict__ list, uint32_t cap,
+                                                                  uint32_t *__restrict__ rx_sites, uint32_t rx_cap)
 {
     using Code = typename ChoiceCode<S>::type;
     constexpr int W = SiteWords<BPS, S>::W;
@@ -264,6 +289,8 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
         }
 #pragma unroll
         for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][oid] : 0u;
+        if (DIM == 2 && rx_sites)
+            list_for_reaction(n < (uint32_t)S ? n : (uint32_t)S, t, i, lid, m, rs, rx_sites, rx_cap);
     } else {
         // The neighbours: from the tile, or loaded with their choices drawn here.
         SiteWords<BPS, S> mn, pl;
@@ -287,6 +314,8 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
         const SiteWords<BPS, S> out = assemble_site<BPS, S>(own, c_own, mn, c_mn, pl, c_pl, i, true,
                                                             (uint32_t)DIM + 1, rs, list, cap);
         out.store(dst, g.N, i);
+        if (DIM == 2 && rx_sites)
+            list_for_reaction((uint32_t)__popc(occupied_slots<BPS, S>(out)), t, i, lid, m, rs, rx_sites, rx_cap);
     }
 }
 
@@ -297,19 +326,26 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
 template <int BPS, int S>
 __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ lat, const uint8_t *__restrict__ sites,
                                                        Geometry g, DevTables m, RunState *__restrict__ rs,
-                                                       OverflowEntry *__restrict__ list, uint32_t cap)
+                                                       OverflowEntry *__restrict__ list, uint32_t cap,
+                                                       const uint32_t *__restrict__ rx_sites, uint32_t rx_cap)
 {
     if (rs->status != LMB_OK) return;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.N) return;
-    const uint32_t t = __ldg(sites + i);
-    SiteWords<BPS, S> s;
-    // The z sweep wrote this buffer, so its sites are packed (occupied slots
-    // first, whatever the input had): only the planes holding particles are
-    // read.
-    s.load_packed(lat, g.N, i);
+    // The sites the z sweep listed, or every site when it listed none or
+    // more than the list holds.
+    const uint32_t listed = rx_sites ? rs->rx_count : 0xFFFFFFFFu;
+    const bool all = listed > rx_cap;
+    const uint32_t n = all ? g.N : listed;
     const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
-    if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) s.store(lat, g.N, i);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t i = all ? j : rx_sites[j];
+        const uint32_t t = __ldg(sites + i);
+        SiteWords<BPS, S> s;
+        // The z sweep wrote this buffer, so its sites are packed (occupied
+        // slots first, whatever the input had): only the planes holding
+        // particles are read.
+        s.load_packed(lat, g.N, i);
+        if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) s.store(lat, g.N, i);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -326,6 +362,8 @@ __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__re
 {
     extern __shared__ OverflowEntry sh[];
     if (rs->status != LMB_OK) return;
+    // The reaction step of this timestep has read its site list.
+    if (threadIdx.x == 0) rs->rx_count = 0;
     resolve_block<BPS, S>(lat, sites, g, rs, list, cap, sh);
 }
 
@@ -342,6 +380,7 @@ __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, ui
     rs->overflows = 0;
     rs->reactions = 0;
     rs->tiles_done = 0;
+    rs->rx_count = 0;
     if (mode == LMB_OVERFLOW_CLASSIC) {
         rs->ovf_count = 0;
         rs->carried = 0;
@@ -367,6 +406,7 @@ __global__ void begin_batch_kernel(RunState *const *rs_ptrs, const uint32_t *see
     rs->overflows = 0;
     rs->reactions = 0;
     rs->tiles_done = 0;
+    rs->rx_count = 0;
     if (mode == LMB_OVERFLOW_CLASSIC) {
         rs->ovf_count = 0;
         rs->carried = 0;
@@ -564,24 +604,35 @@ bool slots_supported(int bps, int slots)
 
 cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint32_t *dst, const uint8_t *sites,
                          const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
-                         cudaStream_t stream)
+                         uint32_t *rx_sites, uint32_t rx_cap, cudaStream_t stream)
 {
     dim3 grid, block;
     sweep_shape(g, dim, grid, block);
     count_launch();
     LMB_DISPATCH_ALL({
-        if (dim == 0) sweep_kernel<BPS, S, 0><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap);
-        else if (dim == 1) sweep_kernel<BPS, S, 1><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap);
-        else sweep_kernel<BPS, S, 2><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap);
+        if (dim == 0)
+            sweep_kernel<BPS, S, 0><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0);
+        else if (dim == 1)
+            sweep_kernel<BPS, S, 1><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0);
+        else
+            sweep_kernel<BPS, S, 2><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, rx_sites,
+                                                                rx_cap);
     })
 }
 
+// A grid of at most 8 blocks per SM strides over the listed sites (or every
+// site); the full pass keeps as many threads resident as one thread per site
+// would.
 cudaError_t launch_reaction(int bps, int slots, uint32_t *lat, const uint8_t *sites, const Geometry &g,
-                            const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap, cudaStream_t stream)
+                            const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
+                            const uint32_t *rx_sites, uint32_t rx_cap, cudaStream_t stream)
 {
-    const uint32_t threads = 256, blocks = (g.N + threads - 1) / threads;
+    const uint32_t threads = 256;
+    uint32_t blocks = (g.N + threads - 1) / threads;
+    if (blocks > 148 * 8) blocks = 148 * 8;
     count_launch();
-    LMB_DISPATCH_ALL(reaction_kernel<BPS, S><<<blocks, threads, 0, stream>>>(lat, sites, g, m, rs, list, cap))
+    LMB_DISPATCH_ALL(reaction_kernel<BPS, S><<<blocks, threads, 0, stream>>>(lat, sites, g, m, rs, list, cap,
+                                                                             rx_sites, rx_cap))
 }
 
 cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sites, const Geometry &g, RunState *rs,

@@ -318,6 +318,28 @@ __device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_
 
 constexpr int MAX_STOICH = 32;
 
+// The first two exits of react_site, for a site of type t holding n
+// particles whose zeroth-order propensity is a0 and whose reaction draw is
+// r0: false when the reaction step cannot change the site.  The reaction
+// probability never exceeds the total propensity a (see the bound before
+// the double exp in react_site), and a itself -- a float sum of qp0, one qp1
+// entry per particle and one qp2 entry per pair, at most 137 terms -- never
+// exceeds U = qp0 + n max(qp1) + n(n-1)/2 max(qp2) by more than its rounding,
+// (1 + 2^-24)^136 < 1.0001.  So a draw above U * 1.0001 * (1 + 2^-20) + 2^-60
+// cannot react.  The z sweep evaluates the same function on the site it has
+// just assembled, so the sites it leaves out are exactly those react_site
+// would leave unchanged.
+__device__ __forceinline__ bool reaction_may_fire(uint32_t n, float a0, uint32_t t, float r0, const DevTables &m)
+{
+    if (n == 0 && a0 == 0.0f) return false;
+    const float nf = (float)n;
+    const float pairs = __fmul_rn(nf, __fmul_rn(__fsub_rn(nf, 1.0f), 0.5f));
+    float u = __fadd_ru(a0, __fmul_ru(nf, tload(m.qpmax + t)));
+    u = __fadd_ru(u, __fmul_ru(pairs, tload(m.qpmax + m.nst + t)));
+    u = __fmul_ru(u, 1.0001f);
+    return !(r0 > __fadd_ru(__fmul_ru(u, 1.00000095367431640625f), 8.67361738e-19f));
+}
+
 // Table propensity sum in slot order, double precision probability, at most
 // one reaction; returns true when the site changed (s updated in place).
 template <int BPS, int S>
@@ -326,22 +348,10 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
 {
     float a = tload(m.qp0 + t);
     if (s.empty() && a == 0.0f) return false;
-    // The reaction probability below never exceeds the total propensity a
-    // (see the bound before the double exp), and a itself -- a float sum of
-    // qp0, one qp1 entry per particle and one qp2 entry per pair, at most 137
-    // terms -- never exceeds U = qp0 + n max(qp1) + n(n-1)/2 max(qp2) by more
-    // than its rounding, (1 + 2^-24)^136 < 1.0001.  So a draw above
-    // U * 1.0001 * (1 + 2^-20) + 2^-60 cannot react, and the table sums and
-    // the double exp are evaluated only for draws below that bound.
+    // The table sums and the double exp are evaluated only for draws below
+    // the bound of reaction_may_fire.
     const float r0 = hash_float(((unsigned long long)gi << 1) | 0ull, th);
-    {
-        const float n = (float)__popc(occupied_slots<BPS, S>(s));
-        const float pairs = __fmul_rn(n, __fmul_rn(__fsub_rn(n, 1.0f), 0.5f));
-        float u = __fadd_ru(a, __fmul_ru(n, tload(m.qpmax + t)));
-        u = __fadd_ru(u, __fmul_ru(pairs, tload(m.qpmax + m.nst + t)));
-        u = __fmul_ru(u, 1.0001f);
-        if (r0 > __fadd_ru(__fmul_ru(u, 1.00000095367431640625f), 8.67361738e-19f)) return false;
-    }
+    if (!reaction_may_fire((uint32_t)__popc(occupied_slots<BPS, S>(s)), a, t, r0, m)) return false;
     const size_t o1 = (size_t)t * m.ns, o2 = (size_t)t * m.ns * m.ns;
 #pragma unroll
     for (int k = 0; k < S; k++) {

@@ -112,6 +112,25 @@ def test_sweep_tiles_vs_oracle(ctx, shape, slots, bps):
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("slots,bps", [(8, 1), (16, 4)])
+@pytest.mark.parametrize("shape,per_slot", [((64, 32, 32), 0.03), ((64, 32, 32), 0.15), ((64, 64, 32), 0.3)])
+def test_reaction_site_list_vs_oracle(ctx, shape, per_slot, slots, bps):
+    """Per-phase schedule: the z sweep lists the sites whose reaction step
+    could change them.  Sparse lattices react over the list; the dense one
+    lists more sites than the list holds (N / 8 + 4096) and reacts over every
+    site.  Zeroth-order reactions list empty sites too."""
+    X, Y, Z = shape
+    spec = configs.random_problem(21, X=X, Y=Y, Z=Z, slots=slots, bytes_per_slot=bps, density=per_slot * slots,
+                                  nst=3, qmax=0.3)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 5, 0, 3)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 5, 0, 3, schedule="phases")
+    assert rc == rc_ref
+    if rc == 0:
+        assert st[0].reactions == st_ref.reactions
+    assert np.array_equal(out, ref)
+
+
 @pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("slots,bps,dens", [(8, 1, 5.0), (16, 4, 12.0), (8, 4, 6.0)])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
