@@ -344,6 +344,13 @@ int lmb_cme_get_counts(lmb_cme *cme, uint32_t *counts);
 int lmb_cme_device_counts(lmb_cme *cme, void **counts);
 /* Waits; total events applied and replicates that reached t_end. */
 int lmb_cme_stats(lmb_cme *cme, uint64_t *events, uint32_t *finished);
+/* Kernel form: LMB_CME_KERNEL_AUTO (default) runs models of up to 8 species
+ * and 16 reactions whose stoichiometric changes lie in -8..7 with the rates
+ * and reactant codes in registers; LMB_CME_KERNEL_GENERIC runs every model
+ * from shared-memory tables.  Both give the same trajectories bit for bit. */
+#define LMB_CME_KERNEL_AUTO 0
+#define LMB_CME_KERNEL_GENERIC 1
+int lmb_cme_set_kernel(lmb_cme *cme, int kernel);
 
 /* Launch counters for the bench's kernel accounting. */
 uint64_t lmb_kernel_launches(void);

@@ -27,6 +27,8 @@ LMB_NOALLOC_MAX_SPECIES = 4095
 
 LMB_SCHEDULE_FUSED = 0
 LMB_SCHEDULE_PHASES = 1
+LMB_CME_KERNEL_AUTO = 0
+LMB_CME_KERNEL_GENERIC = 1
 
 u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
@@ -150,6 +152,7 @@ PROTOTYPES = {
     "lmb_cme_get_counts": (C.c_int, [vp, u32p]),
     "lmb_cme_device_counts": (C.c_int, [vp, C.POINTER(vp)]),
     "lmb_cme_stats": (C.c_int, [vp, u64p, u32p]),
+    "lmb_cme_set_kernel": (C.c_int, [vp, C.c_int]),
     "lmb_kernel_launches": (C.c_uint64, []),
 }
 

@@ -48,6 +48,12 @@ struct CmeModel {
     uint32_t off[CME_MAX_REACTIONS + 1];
     uint8_t sp[CME_MAX_REACTIONS * CME_MAX_SPECIES];
     int32_t d[CME_MAX_REACTIONS * CME_MAX_SPECIES];
+    // Compact form (models of up to 8 species and 16 reactions whose
+    // changes lie in -8..7): reaction r's type | s1 << 2 | s2 << 7, and its
+    // change of species s in bits 4s..4s+3 (two's complement).
+    uint32_t code[CME_MAX_REACTIONS];
+    uint32_t delta4[CME_MAX_REACTIONS];
+    uint32_t compact;
 };
 
 // Per-replicate state, structure of arrays.
@@ -208,6 +214,121 @@ __global__ void __launch_bounds__(CME_THREADS) cme_segment_kernel(const CmeModel
     if (finished) st.done[rep] = 1;
 }
 
+// The segment kernel for compact models: each reaction's rate and reactant
+// code live in registers, its change vector is one shared word, and the
+// total propensity is carried from one event to the next.  The arithmetic
+// is the generic kernel's, operation for operation, so the trajectories are
+// the same bit for bit.
+template <int NS, int NR>
+__global__ void __launch_bounds__(CME_THREADS) cme_compact_kernel(const CmeModel *__restrict__ gm, CmeState st,
+                                                                  int32_t *__restrict__ out, uint32_t reps,
+                                                                  uint32_t entries, uint32_t seed, double seg_end,
+                                                                  double t_end, double write_interval)
+{
+    static_assert(NS <= 8 && NR <= 32, "compact models have at most 8 species");
+    __shared__ uint32_t s_delta[NR];
+    __shared__ unsigned long long s_dep[NR];
+    const uint32_t nr = gm->nr, ns = gm->ns;
+    float kq[NR];
+    uint32_t code[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) {
+        kq[q] = (uint32_t)q < nr ? gm->k[q] : 0.0f;
+        code[q] = (uint32_t)q < nr ? gm->code[q] : 0u;
+    }
+    for (uint32_t q = threadIdx.x; q < NR; q += blockDim.x) {
+        s_delta[q] = q < nr ? gm->delta4[q] : 0u;
+        s_dep[q] = q < nr ? gm->dep[q] : 0ull;
+    }
+    __syncthreads();
+    const uint32_t rep = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rep >= reps || st.done[rep]) return;
+
+    int32_t x[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) x[s] = (uint32_t)s < ns ? st.counts[(size_t)s * reps + rep] : 0;
+    // Propensity of reaction q (CMESolver.cpp:797-822), as propensity().
+    auto prop = [&](int q) {
+        const uint32_t c = code[q], type = c & 3u;
+        const float k = kq[q];
+        const int32_t n1 = getx(x, (c >> 2) & 31u);
+        if (type == LMB_REACTION_ZEROTH) return k;
+        if (type == LMB_REACTION_FIRST) return __fmul_rn(k, (float)n1);
+        if (type == LMB_REACTION_SECOND) return __fmul_rn(__fmul_rn(k, (float)n1), (float)getx(x, (c >> 7) & 31u));
+        if (n1 < 2) return 0.0f;
+        return __fmul_rn(__fmul_rn(__fmul_rn(0.5f, k), (float)n1), (float)(n1 - 1));
+    };
+    float a[NR];
+#pragma unroll
+    for (int q = 0; q < NR; q++) a[q] = (uint32_t)q < nr ? prop(q) : 0.0f;
+    float atot = total(a, nr);
+
+    const unsigned long long th = timestep_hash(seed, rep, 0);
+    double t = st.t[rep];
+    double t_next = st.t_next[rep];
+    double next_write = st.next_write[rep];
+    uint32_t next_entry = st.next_entry[rep];
+    unsigned long long ev = st.events[rep];
+    bool finished = false;
+
+    auto record_until = [&](double limit) {
+        while (next_entry < entries && next_write <= limit) {
+#pragma unroll
+            for (int s = 0; s < NS; s++)
+                if ((uint32_t)s < ns) out[((size_t)next_entry * ns + s) * reps + rep] = x[s];
+            next_entry++;
+            next_write += write_interval;
+        }
+    };
+
+    for (;;) {
+        if (t_next >= t_end) {
+            t = t_end;
+            record_until(t_end + 1e-9);
+            finished = true;
+            break;
+        }
+        if (t_next >= seg_end) break;
+        record_until(t_next + 1e-9);
+        const float u = __fmul_rn(__uint2float_rn(mix_hash((ev << 1) | 1ull, th)), 2.32830643654e-10f);
+        float rv = __fmul_rn(u, atot);
+        uint32_t pick = nr - 1;
+        bool found = false;
+#pragma unroll
+        for (int q = 0; q < NR; q++) {
+            if ((uint32_t)q + 1 < nr && !found) {
+                if (rv < a[q]) {
+                    pick = q;
+                    found = true;
+                } else {
+                    rv = __fsub_rn(rv, a[q]);
+                }
+            }
+        }
+        const uint32_t dv = s_delta[pick];
+#pragma unroll
+        for (int s = 0; s < NS; s++) x[s] += (int32_t)(dv << (28 - 4 * s)) >> 28;
+        const unsigned long long dep = s_dep[pick];
+#pragma unroll
+        for (int q = 0; q < NR; q++)
+            if ((uint32_t)q < nr && ((dep >> q) & 1ull)) a[q] = prop(q);
+        t = t_next;
+        ev++;
+        atot = total(a, nr);
+        t_next = atot > 0.0f ? t + (double)exp_draw(ev, th) / (double)atot : INFINITY;
+    }
+
+#pragma unroll
+    for (int s = 0; s < NS; s++)
+        if ((uint32_t)s < ns) st.counts[(size_t)s * reps + rep] = x[s];
+    st.t[rep] = t;
+    st.t_next[rep] = t_next;
+    st.next_write[rep] = next_write;
+    st.next_entry[rep] = next_entry;
+    st.events[rep] = ev;
+    if (finished) st.done[rep] = 1;
+}
+
 // Sets up every replicate at t = 0: counts and the first event's time; the
 // first segment records entry 0.
 template <int NS, int NR>
@@ -257,6 +378,7 @@ struct lmb_cme {
     uint32_t seed;
     double t_done;
     bool begun;
+    int kernel;  // LMB_CME_KERNEL_*
 };
 
 #define CKC(call)                                                                    \
@@ -330,6 +452,16 @@ extern "C" int lmb_cme_create(lmb_ctx *ctx, uint32_t ns, uint32_t nr, const uint
         }
     }
     h.off[nr] = nnz;
+    h.compact = ns <= 8 && nr <= 16;
+    for (uint32_t r = 0; r < nr; r++) {
+        h.code[r] = h.type[r] | (h.s1[r] << 2) | (h.s2[r] << 7);
+        uint32_t packed = 0;
+        for (uint32_t j = h.off[r]; j < h.off[r + 1]; j++) {
+            if (h.d[j] < -8 || h.d[j] > 7) h.compact = 0;
+            packed |= ((uint32_t)h.d[j] & 0xFu) << (4 * h.sp[j]);
+        }
+        h.delta4[r] = packed;
+    }
     for (uint32_t r = 0; r < nr; r++) {
         unsigned long long dep = 0;
         for (uint32_t j = h.off[r]; j < h.off[r + 1]; j++) {
@@ -440,6 +572,16 @@ static cudaError_t launch_segment(lmb_cme *c, double seg_end)
     return cudaGetLastError();
 }
 
+template <int NS, int NR>
+static cudaError_t launch_compact(lmb_cme *c, double seg_end)
+{
+    const uint32_t blocks = (c->reps + CME_THREADS - 1) / CME_THREADS;
+    cme_compact_kernel<NS, NR><<<blocks, CME_THREADS, 0, c->ctx->stream>>>(
+        c->dev_model, c->st, c->out, c->reps, c->entries, c->seed, seg_end, c->t_end, c->write_interval);
+    count_launch();
+    return cudaGetLastError();
+}
+
 // Register-resident variants: (species, reactions) up to (4, 8), (8, 16) and
 // (32, 64).
 static cudaError_t dispatch_begin(lmb_cme *c)
@@ -451,9 +593,20 @@ static cudaError_t dispatch_begin(lmb_cme *c)
 
 static cudaError_t dispatch_segment(lmb_cme *c, double seg_end)
 {
+    if (c->host.compact && c->kernel == LMB_CME_KERNEL_AUTO) {
+        if (c->ns <= 4 && c->nr <= 8) return launch_compact<4, 8>(c, seg_end);
+        return launch_compact<8, 16>(c, seg_end);
+    }
     if (c->ns <= 4 && c->nr <= 8) return launch_segment<4, 8>(c, seg_end);
     if (c->ns <= 8 && c->nr <= 16) return launch_segment<8, 16>(c, seg_end);
     return launch_segment<CME_MAX_SPECIES, CME_MAX_REACTIONS>(c, seg_end);
+}
+
+extern "C" int lmb_cme_set_kernel(lmb_cme *c, int kernel)
+{
+    if (!c || (kernel != LMB_CME_KERNEL_AUTO && kernel != LMB_CME_KERNEL_GENERIC)) return LMB_E_ARG;
+    c->kernel = kernel;
+    return LMB_OK;
 }
 
 extern "C" int lmb_cme_begin(lmb_cme *c, uint32_t seed, double t_end, double write_interval)

@@ -147,71 +147,89 @@ __device__ __forceinline__ void warp_append(uint32_t b, uint32_t r, uint32_t w, 
     }
 }
 
-// One timestep of one tile (`tile` of the lattice's `ntiles`), run by the
-// whole block.  The block is flat (FUSED_THREADS threads); the tile's
-// logical bx x by layout (bx a multiple of 32, so a warp is 32 consecutive x
-// of one row) comes from the tile shape.
-template <int BPS, int S>
-__device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
-                                           const uint8_t *__restrict__ sites, const Geometry &g, const DevTables &m,
-                                           RunState *__restrict__ rs, OverflowEntry *__restrict__ list, uint32_t cap,
-                                           const TileShape &ts, int with_reaction, uint32_t tile, uint32_t ntiles)
-{
-    extern __shared__ __align__(16) uint32_t smem[];
-    __shared__ uint32_t s_last;
-    __shared__ uint32_t s_cnt[4];
-    // Per region row: lattice index of its x = 0 site and its flags, and the
-    // region rows the y and z sweeps produce.  Filled once: no sweep divides.
-    __shared__ uint32_t rowbase[FUSED_MAX_ROWS];
-    __shared__ uint16_t yrow[FUSED_MAX_ROWS], zrow[FUSED_MAX_ROWS];
-    __shared__ uint8_t rowflag[FUSED_MAX_ROWS];
-    constexpr int W = SiteWords<BPS, S>::W;
-    // A failed run stops; in a batch, a lattice whose own timestep range is
-    // done sits out the remaining launches.
-    if (rs->status != LMB_OK || rs->step >= rs->end_step) return;
-    const uint32_t X = g.X, R = ts.R, Ry = ts.Ry, Ty = ts.Ty, Tz = ts.Tz, MW = ts.MW;
-    const uint32_t tyi = tile % ts.tiles_y, tzi = tile / ts.tiles_y;
-    const uint32_t y0 = tyi * Ty, z0 = tzi * Tz;
-    const uint32_t seed = rs->seed, step = rs->step;
-    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
-    const uint32_t bx = ts.bx, by = nthr / bx, tx = tid % bx, ty = tid / bx;
-    const uint32_t rows = Ry * ts.Rz, yrows = Ty * ts.Rz, orows = Ty * Tz;
-    // Shared layout: A[W][R], B[W][R] particle words (valid where the
-    // occupancy bit is set), work[R] site list, T[R] site types, then
-    // occA / occB [rows * MW] occupancy bit masks.
-    uint32_t *A = smem;
-    uint32_t *B = A + W * R;
-    uint32_t *work = B + W * R;
-    uint8_t *T = (uint8_t *)(work + R);
-    uint32_t *occA = (uint32_t *)(T + ((R + 15u) & ~15u));
-    uint32_t *occB = occA + rows * MW;
-    uint8_t *tables = (uint8_t *)(((uintptr_t)(occB + rows * MW) + 15u) & ~(uintptr_t)15u);
-    // The model tables, from shared memory when they are small; the table set
-    // itself is kept in shared memory so that calls take it by reference
-    // without a per-thread copy.
-    __shared__ DevTables s_mt;
-    {
-        const DevTables staged = m.stage_bytes ? stage_tables(m, tables, tid, nthr) : m;
-        if (tid == 0) s_mt = staged;
-    }
-    const DevTables &mt = s_mt;
+// Shared-memory layout of a tile: A[W][R], B[W][R] particle words (valid
+// where the occupancy bit is set), work[R] site list, T[R] site types, then
+// occA / occB [rows * MW] occupancy bit masks and the staged model tables;
+// per region row its lattice index of x = 0 and flags, and the region rows
+// the y and z sweeps produce.  Filled once: no sweep divides.
+struct TileSmem {
+    uint32_t *A, *B, *work;
+    uint8_t *T;
+    uint32_t *occA, *occB;
+    uint8_t *tables;
+    uint32_t *rowbase;
+    uint16_t *yrow, *zrow;
+    uint8_t *rowflag;
+    uint32_t *cnt;
+};
 
+template <int BPS, int S>
+__device__ __forceinline__ TileSmem tile_smem(uint32_t *smem, const TileShape &ts, uint32_t *rowbase, uint16_t *yrow,
+                                              uint16_t *zrow, uint8_t *rowflag, uint32_t *cnt)
+{
+    constexpr int W = SiteWords<BPS, S>::W;
+    const uint32_t R = ts.R, rows = ts.Ry * ts.Rz, MW = ts.MW;
+    TileSmem t;
+    t.A = smem;
+    t.B = t.A + W * R;
+    t.work = t.B + W * R;
+    t.T = (uint8_t *)(t.work + R);
+    t.occA = (uint32_t *)(t.T + ((R + 15u) & ~15u));
+    t.occB = t.occA + rows * MW;
+    t.tables = (uint8_t *)(((uintptr_t)(t.occB + rows * MW) + 15u) & ~(uintptr_t)15u);
+    t.rowbase = rowbase;
+    t.yrow = yrow;
+    t.zrow = zrow;
+    t.rowflag = rowflag;
+    t.cnt = cnt;
+    return t;
+}
+
+// Row tables of tile `tile` (no barrier).
+__device__ __forceinline__ void tile_rows(const Geometry &g, const TileShape &ts, uint32_t tile, const TileSmem &t)
+{
+    const uint32_t X = g.X, Ry = ts.Ry, Ty = ts.Ty, Tz = ts.Tz, tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t y0 = (tile % ts.tiles_y) * Ty, z0 = (tile / ts.tiles_y) * Tz;
+    const uint32_t rows = Ry * ts.Rz, yrows = Ty * ts.Rz, orows = Ty * Tz;
     for (uint32_t r = tid; r < rows; r += nthr) {
         const uint32_t ly = r % Ry, lz = r / Ry;
-        rowbase[r] = ((y0 + ly + g.Y - 1) % g.Y) * X + ((z0 + lz + g.Z - 1) % g.Z) * g.XY;
-        rowflag[r] = ly >= 1 && ly <= Ty && lz >= 1 && lz <= Tz ? ROW_OWNED : 0;
+        t.rowbase[r] = ((y0 + ly + g.Y - 1) % g.Y) * X + ((z0 + lz + g.Z - 1) % g.Z) * g.XY;
+        t.rowflag[r] = ly >= 1 && ly <= Ty && lz >= 1 && lz <= Tz ? ROW_OWNED : 0;
     }
-    for (uint32_t q = tid; q < yrows; q += nthr) yrow[q] = (uint16_t)((q / Ty) * Ry + 1 + q % Ty);
-    for (uint32_t q = tid; q < orows; q += nthr) zrow[q] = (uint16_t)((1 + q / Ty) * Ry + 1 + q % Ty);
-    if (tid < 4) s_cnt[tid] = 0;
-    __syncthreads();
+    for (uint32_t q = tid; q < yrows; q += nthr) t.yrow[q] = (uint16_t)((q / Ty) * Ry + 1 + q % Ty);
+    for (uint32_t q = tid; q < orows; q += nthr) t.zrow[q] = (uint16_t)((1 + q / Ty) * Ry + 1 + q % Ty);
+    if (tid < 4) t.cnt[tid] = 0;
+}
 
-    // ---- load the region ----
+template <bool CG>
+__device__ __forceinline__ uint4 load16(const uint32_t *p)
+{
+    return CG ? __ldcg((const uint4 *)p) : __ldg((const uint4 *)p);
+}
+
+template <bool CG>
+__device__ __forceinline__ uint32_t load4(const uint32_t *p)
+{
+    return CG ? __ldcg(p) : __ldg(p);
+}
+
+// Loads region rows of `src` into `w` with their occupancy masks in `occ`:
+// every row, or (halo_only) the rows the tile does not own; the site types
+// too when `types`.  CG: read through L2 (the rows were written by other
+// blocks of the same launch).  Ends with a block barrier.
+template <int BPS, int S, bool CG>
+__device__ __forceinline__ void tile_load(const uint32_t *__restrict__ src, const uint8_t *__restrict__ sites,
+                                          const Geometry &g, const TileShape &ts, const TileSmem &t, uint32_t *w,
+                                          uint32_t *occ, bool halo_only, bool types)
+{
+    constexpr int W = SiteWords<BPS, S>::W;
+    const uint32_t X = g.X, R = ts.R, MW = ts.MW, rows = ts.Ry * ts.Rz, tid = threadIdx.x, nthr = blockDim.x;
     if (ts.vec) {
         // 16-byte loads: an item is 4 consecutive sites of one row, read from
         // every word plane (W 16-byte loads), with its 4 occupancy bits OR-ed
         // into the row's mask word.  Up to four items in flight per thread.
-        for (uint32_t i = tid; i < rows * MW; i += nthr) occA[i] = 0u;
+        for (uint32_t i = tid; i < rows * MW; i += nthr)
+            if (!halo_only || !(t.rowflag[i / MW] & ROW_OWNED)) occ[i] = 0u;
         const uint32_t q4 = X / 4, nq = rows * q4;
         constexpr int U = W >= 4 ? 2 : 8 / W;
         __syncthreads();
@@ -224,10 +242,11 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
                 rr[u] = ~0u;
                 if (i < nq) {
                     const uint32_t r = i / q4, c = i - r * q4;
+                    if (halo_only && (t.rowflag[r] & ROW_OWNED)) continue;
                     rr[u] = r;
                     cc[u] = c;
 #pragma unroll
-                    for (int k = 0; k < W; k++) v[u][k] = __ldg((const uint4 *)(src + (size_t)k * g.N + rowbase[r]) + c);
+                    for (int k = 0; k < W; k++) v[u][k] = load16<CG>(src + (size_t)k * g.N + t.rowbase[r] + 4 * c);
                 }
             }
 #pragma unroll
@@ -237,61 +256,84 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
                 uint4 o = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
                 for (int k = 0; k < W; k++) {
-                    *(uint4 *)(A + k * R + r * X + x) = v[u][k];
+                    *(uint4 *)(w + k * R + r * X + x) = v[u][k];
                     o.x |= v[u][k].x;
                     o.y |= v[u][k].y;
                     o.z |= v[u][k].z;
                     o.w |= v[u][k].w;
                 }
                 const uint32_t bits = (o.x ? 1u : 0u) | (o.y ? 2u : 0u) | (o.z ? 4u : 0u) | (o.w ? 8u : 0u);
-                if (bits) atomicOr(&occA[r * MW + (x >> 5)], bits << (x & 31u));
+                if (bits) atomicOr(&occ[r * MW + (x >> 5)], bits << (x & 31u));
             }
         }
-        const uint32_t q16 = X / 16, nt = rows * q16;
-        for (uint32_t i = tid; i < nt; i += nthr) {
-            const uint32_t r = i / q16, c = i - r * q16;
-            *((uint4 *)(T + r * X) + c) = __ldg((const uint4 *)(sites + rowbase[r]) + c);
+        if (types) {
+            const uint32_t q16 = X / 16, nt = rows * q16;
+            for (uint32_t i = tid; i < nt; i += nthr) {
+                const uint32_t r = i / q16, c = i - r * q16;
+                *((uint4 *)(t.T + r * X) + c) = __ldg((const uint4 *)(sites + t.rowbase[r]) + c);
+            }
         }
     } else {
         // Rows not 16-byte aligned: one word per thread.
+        const uint32_t bx = ts.bx, by = nthr / bx, tx = tid % bx, ty = tid / bx;
         for (uint32_t r = ty; r < rows; r += by) {
-            const uint32_t gbase = rowbase[r];
+            if (halo_only && (t.rowflag[r] & ROW_OWNED)) continue;
+            const uint32_t gbase = t.rowbase[r];
             for (uint32_t xb = 0; xb < X; xb += bx) {
                 const uint32_t x = xb + tx;
-                bool occ = false;
+                bool o_site = false;
                 if (x < X) {
                     const uint32_t l = r * X + x, gi = gbase + x;
                     uint32_t o = 0;
 #pragma unroll
                     for (int k = 0; k < W; k++) {
-                        const uint32_t v = __ldg(src + (size_t)k * g.N + gi);
-                        A[k * R + l] = v;
+                        const uint32_t v = load4<CG>(src + (size_t)k * g.N + gi);
+                        w[k * R + l] = v;
                         o |= v;
                     }
-                    T[l] = __ldg(sites + gi);
-                    occ = o != 0;
+                    if (types) t.T[l] = __ldg(sites + gi);
+                    o_site = o != 0;
                 }
-                const uint32_t mask = __ballot_sync(0xffffffffu, occ);
-                if ((tx & 31u) == 0 && (x >> 5) < MW) occA[r * MW + (x >> 5)] = mask;
+                const uint32_t mask = __ballot_sync(0xffffffffu, o_site);
+                if ((tx & 31u) == 0 && (x >> 5) < MW) occ[r * MW + (x >> 5)] = mask;
             }
         }
     }
     __syncthreads();
+}
 
-    uint32_t *src_w = A, *dst_w = B, *src_o = occA, *dst_o = occB;
+// One timestep of the tile in shared memory, from (w, o) = the region at the
+// start of the timestep; on return (w, o) hold the owned rows after the x,
+// y and z sweeps and the reaction (the other rows are stale).  Ends with a
+// block barrier.
+template <int BPS, int S>
+__device__ __forceinline__ void tile_timestep(const Geometry &g, const DevTables &mt, RunState *__restrict__ rs,
+                                              OverflowEntry *__restrict__ list, uint32_t cap, const TileShape &ts,
+                                              const TileSmem &t, uint32_t *&src_w, uint32_t *&dst_w,
+                                              uint32_t *&src_o, uint32_t *&dst_o, uint32_t seed, uint32_t step,
+                                              int with_reaction)
+{
+    const uint32_t X = g.X, R = ts.R, Ry = ts.Ry, Ty = ts.Ty, Tz = ts.Tz, MW = ts.MW;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t rows = Ry * ts.Rz, yrows = Ty * ts.Rz, orows = Ty * Tz;
+    uint32_t *work = t.work;
+    const uint8_t *T = t.T;
+    const uint32_t *rowbase = t.rowbase;
     // Models without zeroth-order reactions react only on occupied sites:
     // the reaction then runs in the z sweep's pass, without a pass of its own.
     bool zeroth = false;
-    for (uint32_t t = 0; t < mt.nst; t++) zeroth |= mt.qp0[t] != 0.0f;
+    for (uint32_t q = 0; q < mt.nst; q++) zeroth |= mt.qp0[q] != 0.0f;
     const bool react_inline = with_reaction && !zeroth;
     const unsigned long long th_rx = timestep_hash(seed, step, 3);
+    if (tid < 4) t.cnt[tid] = 0;
+    __syncthreads();
 #pragma unroll 1
     for (int phase = 0; phase < 3; phase++) {
         const unsigned long long th = timestep_hash(seed, step, (uint32_t)phase);
-        const uint16_t *orow = phase == 0 ? nullptr : (phase == 1 ? yrow : zrow);
+        const uint16_t *orow = phase == 0 ? nullptr : (phase == 1 ? t.yrow : t.zrow);
         const uint32_t nout = phase == 0 ? rows : (phase == 1 ? yrows : orows);
         const uint32_t d = phase == 1 ? 1u : Ry;  // row step of the y / z neighbours
-        uint32_t *cnt = &s_cnt[phase];
+        uint32_t *cnt = &t.cnt[phase];
 
         // 1. Active outputs: occupied or next to an occupied site on the axis.
         for (uint32_t i0 = 0; i0 < nout * MW; i0 += nthr) {
@@ -329,7 +371,7 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
             if ((src_o[r * MW + (x >> 5)] >> (x & 31u)) & 1u) load_smem<BPS, S>(src_w, R, l, own);
             if ((src_o[rm * MW + (xm >> 5)] >> (xm & 31u)) & 1u) load_smem<BPS, S>(src_w, R, lm, mn);
             if ((src_o[rp * MW + (xp >> 5)] >> (xp & 31u)) & 1u) load_smem<BPS, S>(src_w, R, lp, pl);
-            const bool record = phase == 2 || (rowflag[r] & ROW_OWNED);
+            const bool record = phase == 2 || (t.rowflag[r] & ROW_OWNED);
             own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], rowbase[r] + x, rowbase[rm] + xm,
                                      rowbase[rp] + xp, th, mt, record, (uint32_t)phase + 1, rs, list, cap);
             // After the z sweep an owned site reacts right away in
@@ -361,14 +403,14 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
             if (i < orows * MW) {
                 const uint32_t q = i / MW;
                 w = i - q * MW;
-                r = zrow[q];
+                r = t.zrow[q];
                 const uint32_t all = (w + 1 < MW || !(X & 31u)) ? 0xffffffffu : ((1u << (X & 31u)) - 1u);
                 a = zeroth ? all : src_o[r * MW + w];
             }
-            warp_append(a, r, w, work, &s_cnt[3]);
+            warp_append(a, r, w, work, &t.cnt[3]);
         }
         __syncthreads();
-        const uint32_t n = s_cnt[3];
+        const uint32_t n = t.cnt[3];
         for (uint32_t j = tid; j < n; j += nthr) {
             const uint32_t e = work[j], r = e >> 16, x = e & 0xFFFFu, l = r * X + x;
             const bool occ = (src_o[r * MW + (x >> 5)] >> (x & 31u)) & 1u;
@@ -383,38 +425,86 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
         }
         __syncthreads();
     }
+}
 
-    // Dense write of the owned rows (empty sites as zeros).
+// Dense write of the owned rows (empty sites as zeros) from (w, o).
+template <int BPS, int S>
+__device__ __forceinline__ void tile_store(uint32_t *__restrict__ dst, const Geometry &g, const TileShape &ts,
+                                           const TileSmem &t, const uint32_t *w, const uint32_t *o)
+{
+    constexpr int W = SiteWords<BPS, S>::W;
+    const uint32_t X = g.X, R = ts.R, MW = ts.MW, orows = ts.Ty * ts.Tz, tid = threadIdx.x, nthr = blockDim.x;
     if (ts.vec) {
         // Four sites per thread: a 16-byte store per word plane.
         const uint32_t q4 = X / 4, n4 = orows * q4;
         for (uint32_t i = tid; i < n4; i += nthr) {
-            const uint32_t q = i / q4, c = i - q * q4, r = zrow[q], x = 4 * c;
-            const uint32_t bits = (src_o[r * MW + (x >> 5)] >> (x & 31u)) & 0xFu;
+            const uint32_t q = i / q4, c = i - q * q4, r = t.zrow[q], x = 4 * c;
+            const uint32_t bits = (o[r * MW + (x >> 5)] >> (x & 31u)) & 0xFu;
 #pragma unroll
             for (int k = 0; k < W; k++) {
                 uint4 v = make_uint4(0u, 0u, 0u, 0u);
                 if (bits) {
-                    const uint32_t *a = src_w + k * R + r * X + x;
+                    const uint32_t *a = w + k * R + r * X + x;
                     v.x = (bits & 1u) ? a[0] : 0u;
                     v.y = (bits & 2u) ? a[1] : 0u;
                     v.z = (bits & 4u) ? a[2] : 0u;
                     v.w = (bits & 8u) ? a[3] : 0u;
                 }
-                *((uint4 *)(dst + (size_t)k * g.N + rowbase[r]) + c) = v;
+                *((uint4 *)(dst + (size_t)k * g.N + t.rowbase[r]) + c) = v;
             }
         }
-    } else
-    for (uint32_t q = ty; q < orows; q += by) {
-        const uint32_t r = zrow[q];
-        const uint32_t gb = rowbase[r];
-        for (uint32_t x = tx; x < X; x += bx) {
-            SiteWords<BPS, S> s;
-            s.clear();
-            if ((src_o[r * MW + (x >> 5)] >> (x & 31u)) & 1u) load_smem<BPS, S>(src_w, R, r * X + x, s);
-            s.store(dst, g.N, gb + x);
+    } else {
+        const uint32_t bx = ts.bx, by = nthr / bx, tx = tid % bx, ty = tid / bx;
+        for (uint32_t q = ty; q < orows; q += by) {
+            const uint32_t r = t.zrow[q];
+            const uint32_t gb = t.rowbase[r];
+            for (uint32_t x = tx; x < X; x += bx) {
+                SiteWords<BPS, S> s;
+                s.clear();
+                if ((o[r * MW + (x >> 5)] >> (x & 31u)) & 1u) load_smem<BPS, S>(w, R, r * X + x, s);
+                s.store(dst, g.N, gb + x);
+            }
         }
     }
+}
+
+// One timestep of one tile (`tile` of the lattice's `ntiles`), run by the
+// whole block.  The block is flat (FUSED_THREADS threads); the tile's
+// logical bx x by layout (bx a multiple of 32, so a warp is 32 consecutive x
+// of one row) comes from the tile shape.
+template <int BPS, int S>
+__device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
+                                           const uint8_t *__restrict__ sites, const Geometry &g, const DevTables &m,
+                                           RunState *__restrict__ rs, OverflowEntry *__restrict__ list, uint32_t cap,
+                                           const TileShape &ts, int with_reaction, uint32_t tile, uint32_t ntiles)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ uint32_t s_last;
+    __shared__ uint32_t s_cnt[4];
+    __shared__ uint32_t rowbase[FUSED_MAX_ROWS];
+    __shared__ uint16_t yrow[FUSED_MAX_ROWS], zrow[FUSED_MAX_ROWS];
+    __shared__ uint8_t rowflag[FUSED_MAX_ROWS];
+    // A failed run stops; in a batch, a lattice whose own timestep range is
+    // done sits out the remaining launches.
+    if (rs->status != LMB_OK || rs->step >= rs->end_step) return;
+    const uint32_t seed = rs->seed, step = rs->step;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const TileSmem t = tile_smem<BPS, S>(smem, ts, rowbase, yrow, zrow, rowflag, s_cnt);
+    // The model tables, from shared memory when they are small; the table set
+    // itself is kept in shared memory so that calls take it by reference
+    // without a per-thread copy.
+    __shared__ DevTables s_mt;
+    {
+        const DevTables staged = m.stage_bytes ? stage_tables(m, t.tables, tid, nthr) : m;
+        if (tid == 0) s_mt = staged;
+    }
+    tile_rows(g, ts, tile, t);
+    __syncthreads();
+    tile_load<BPS, S, false>(src, sites, g, ts, t, t.A, t.occA, false, true);
+
+    uint32_t *src_w = t.A, *dst_w = t.B, *src_o = t.occA, *dst_o = t.occB;
+    tile_timestep<BPS, S>(g, s_mt, rs, list, cap, ts, t, src_w, dst_w, src_o, dst_o, seed, step, with_reaction);
+    tile_store<BPS, S>(dst, g, ts, t, src_w, src_o);
 
     // The last block to finish resolves the overflow queue and advances the
     // step counter.

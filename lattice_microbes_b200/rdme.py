@@ -1,0 +1,373 @@
+"""lm::rdme::MpdRdmeSolver / IntMpdRdmeSolver for Python callers.
+
+pyLM's RDMESimulation and jLM's runSolver drive the reference's SWIG class
+(src/swig/lm.i:949-1015) with initialize / buildModel / buildDiffusionModel /
+generateTrajectory and subclass it to override hookSimulation and the other
+callbacks.  This module gives the same calls, argument meaning and callback
+contract on top of the C ABI, so such a script switches by changing the class
+it instantiates:
+
+    class Solver(MpdRdmeSolver):
+        def hookSimulation(self, time, lattice):
+            ...                      # lattice: HostLattice, reference accessors
+            return 0                 # 0 / 1 / 2 / 3 as in MpdRdmeSolver
+
+    s = Solver()
+    s.initialize(replicate, {"seed": "1234", "timestep": "5e-05", "maxTime": "1.0",
+                             "writeInterval": "1000", "latticeWriteInterval": "10000"})
+    s.buildModel(ns, nr, init, types, K, S, D)
+    s.buildDiffusionModel(nst, DF, RL, X, Y, Z, 8, 1, spacing, lattice_xyzp, sites_xyz)
+    s.generateTrajectory()
+
+Outputs go to writeSpeciesCounts / writeLattice / writeLatticeSites, which by
+default keep the records in memory (speciesCounts, latticeFrames); the
+reference sends the same records to its HDF5 output queue.
+"""
+import time as _time
+
+import numpy as np
+
+from . import _lib as L
+from .solver import Context, Lattice, Model, compose_seed
+
+
+def trajectory_events(total, counts_interval, lattice_interval, hook_interval=None):
+    """The timesteps after which MpdRdmeSolver::generateTrajectory
+    (MpdRdmeSolver.cu:485-668) does something, with what it does there:
+    yields (step, hook, lattice, counts) for each such step, in order, for a
+    run of `total` timesteps.  Intervals are in timesteps; an interval of 0
+    fires after every timestep, as in the reference; hook_interval None means
+    no hook."""
+    next_counts, next_lattice = counts_interval, lattice_interval
+    next_hook = hook_interval if hook_interval is not None else None
+    step = 0
+    while step < total:
+        ev = total
+        ev = min(ev, next_counts if next_counts > step else step + 1)
+        ev = min(ev, next_lattice if next_lattice > step else step + 1)
+        if next_hook is not None:
+            ev = min(ev, next_hook if next_hook > step else step + 1)
+        step = ev
+        hook = next_hook is not None and step >= next_hook
+        lat = step >= next_lattice
+        cnt = step >= next_counts
+        if hook:
+            next_hook += hook_interval
+        if lat:
+            next_lattice += lattice_interval
+        if cnt:
+            next_counts += counts_interval
+        if hook or lat or cnt:
+            yield step, hook, lat, cnt
+
+
+def timesteps_for(max_time, tau):
+    """Timesteps the reference runs: it loops while timestep * tau < maxTime."""
+    if tau <= 0.0:
+        return 0
+    n = int(np.floor(max_time / tau))
+    while n * tau < max_time:
+        n += 1
+    while n > 0 and (n - 1) * tau >= max_time:
+        n -= 1
+    return n
+
+
+class HostLattice:
+    """Host copy of a lattice in the native layout, with the reference
+    lattice's accessors (rdme/Lattice.h:131-259, ByteLattice / IntLattice
+    views of lm.i:854-915).  `particles` is the native word-planar array
+    (word w of site i = x + y X + z X Y at particles[w N + i]; a ByteLattice
+    word holds 4 slots), `sites` the [z][y][x] site types."""
+
+    def __init__(self, X, Y, Z, slots, bytes_per_particle, spacing=0.0):
+        self.X, self.Y, self.Z, self.slots = X, Y, Z, slots
+        self.bytes_per_particle = bytes_per_particle
+        self.spacing = spacing
+        self.words = slots // 4 if bytes_per_particle == 1 else slots
+        self.particles = np.zeros(self.words * X * Y * Z, dtype=np.uint32)
+        self.sites = np.zeros(X * Y * Z, dtype=np.uint8)
+
+    # Lattice (rdme/Lattice.h)
+    def getXSize(self):
+        return self.X
+
+    def getYSize(self):
+        return self.Y
+
+    def getZSize(self):
+        return self.Z
+
+    def getSize(self):
+        return (self.X, self.Y, self.Z)
+
+    def getNumberSites(self):
+        return self.X * self.Y * self.Z
+
+    def getSpacing(self):
+        return self.spacing
+
+    def getMaxOccupancy(self):
+        return self.slots
+
+    def _index(self, x, y, z):
+        if not (0 <= x < self.X and 0 <= y < self.Y and 0 <= z < self.Z):
+            raise IndexError("site (%d, %d, %d) outside the lattice" % (x, y, z))
+        return x + y * self.X + z * self.X * self.Y
+
+    def getSiteType(self, x, y, z):
+        return int(self.sites[self._index(x, y, z)])
+
+    def setSiteType(self, x, y, z, site_type):
+        self.sites[self._index(x, y, z)] = site_type
+
+    def getParticle(self, x, y, z, index):
+        if not 0 <= index < self.slots:
+            raise IndexError("particle index %d" % index)
+        i, N = self._index(x, y, z), self.getNumberSites()
+        if self.bytes_per_particle == 1:
+            return int((self.particles[(index // 4) * N + i] >> np.uint32(8 * (index % 4))) & np.uint32(0xFF))
+        return int(self.particles[index * N + i])
+
+    def getOccupancy(self, x, y, z):
+        n = 0
+        while n < self.slots and self.getParticle(x, y, z, n) != 0:
+            n += 1
+        return n
+
+    def _set_slot(self, i, index, value):
+        N = self.getNumberSites()
+        if self.bytes_per_particle == 1:
+            k, sh = (index // 4) * N + i, np.uint32(8 * (index % 4))
+            w = self.particles[k] & ~(np.uint32(0xFF) << sh)
+            self.particles[k] = w | (np.uint32(value & 0xFF) << sh)
+        else:
+            self.particles[index * N + i] = value
+
+    def addParticle(self, x, y, z, particle):
+        """ByteLattice::addParticle: the first free slot; raises when full
+        (InvalidParticleException in the reference)."""
+        n = self.getOccupancy(x, y, z)
+        if n >= self.slots:
+            raise ValueError("site (%d, %d, %d) is full" % (x, y, z))
+        self._set_slot(self._index(x, y, z), n, particle)
+
+    def removeParticles(self, x, y, z):
+        i = self._index(x, y, z)
+        for k in range(self.slots):
+            self._set_slot(i, k, 0)
+
+    def getParticleCounts(self):
+        """{species: count} over the lattice (ByteLattice.cpp:495-520)."""
+        if self.bytes_per_particle == 1:
+            v = self.particles.view(np.uint8)
+        else:
+            v = self.particles
+        ids, counts = np.unique(v[v != 0], return_counts=True)
+        return {int(s): int(c) for s, c in zip(ids, counts)}
+
+    # Views (lm.i:894-895, 913-914)
+    def getSiteLatticeView(self):
+        """Site types, shape (Z, Y, X), sharing memory with the lattice."""
+        return self.sites.reshape(self.Z, self.Y, self.X)
+
+    def getParticleLatticeView(self):
+        """Particles, shape (words, Z, Y, X, per-word slots): uint8 with 4
+        slots per word for ByteLattices, uint32 with 1 for IntLattices;
+        shares memory with the lattice."""
+        if self.bytes_per_particle == 1:
+            return self.particles.view(np.uint8).reshape(self.words, self.Z, self.Y, self.X, 4)
+        return self.particles.reshape(self.words, self.Z, self.Y, self.X, 1)
+
+
+class MpdRdmeSolver:
+    """lm::rdme::MpdRdmeSolver (ByteLattice); IntMpdRdmeSolver below."""
+
+    bytes_per_particle = 1
+
+    def __init__(self, device=0):
+        self.ctx = Context(device)
+        self.model = None
+        self.lat = None
+        self.parameters = {}
+        self.replicate = 0
+        self.seed = 0
+        self.overflow_mode = L.LMB_OVERFLOW_CLASSIC
+        self.lattice = None
+        self.speciesCounts = []       # (time, counts of species 1..ns)
+        self.latticeFrames = []       # (time, particles copy, sites copy)
+        self.lastRunStats = None
+        self._stop = False
+
+    def needsReactionModel(self):
+        return True
+
+    def needsDiffusionModel(self):
+        return True
+
+    # ---- set-up (MpdRdmeSolver.cu:107-162, CMESolver.h:200-201, RDMESolver.cpp:97-189)
+    def initialize(self, replicate, parameters):
+        """seed = (seedTop << 16) | (replicate & 0xFFFF), seedTop from the
+        "seed" parameter (the clock's nanoseconds when 0);
+        "rdme.mpd.overflowhandler" classic (default) or relaxed."""
+        self.replicate = replicate
+        self.parameters = {k: str(v) for k, v in dict(parameters).items()}
+        seed_top = int(float(self.parameters.get("seed", "0") or 0))
+        if seed_top == 0:
+            seed_top = _time.time_ns() % 1000000000
+        self.seed = compose_seed(seed_top, replicate)
+        handler = self.parameters.get("rdme.mpd.overflowhandler", "classic")
+        self.overflow_mode = L.LMB_OVERFLOW_RELAXED if handler == "relaxed" else L.LMB_OVERFLOW_CLASSIC
+
+    def buildModel(self, numberSpecies, numberReactions, initialSpeciesCounts, reactionTypes, K, S, D, kCols=1):
+        """Reaction types 0..3; K [R * kCols] (column 0 used); S and D
+        species-major [NS * R]."""
+        self._ns, self._nr = int(numberSpecies), int(numberReactions)
+        K = np.asarray(K, dtype=np.float64).reshape(-1)
+        self._rtype = np.asarray(reactionTypes, dtype=np.uint32).reshape(-1)
+        self._K = K[::int(kCols)][:self._nr] if self._nr else np.zeros(0)
+        self._S = np.asarray(S, dtype=np.int32).reshape(-1)
+        self._D = np.asarray(D, dtype=np.uint32).reshape(-1)
+        self._initial = np.asarray(initialSpeciesCounts, dtype=np.uint32).reshape(-1)
+
+    def buildDiffusionModel(self, numberSiteTypes, DF, RL, X, Y, Z, particlesPerSite, bytesPerParticle,
+                            latticeSpacing, latticeData, latticeSitesData, rowMajorData=True):
+        """DF [NST * NST * NS] m^2/s, RL [R * NST]; lattice [x][y][z][p] and
+        site types [x][y][z] row-major; "timestep" from the parameters."""
+        if not rowMajorData:
+            raise ValueError("columns major lattice data is not currently supported")
+        if bytesPerParticle != self.bytes_per_particle:
+            raise ValueError("bytes_per_particle does not match the solver's lattice type")
+        self._nst = int(numberSiteTypes)
+        self.tau = float(self.parameters.get("timestep", "0"))
+        spec = _ModelInputs(self._ns, self._nst, self._nr, self._rtype, self._K, self._S, self._D,
+                            np.asarray(DF, dtype=np.float64).reshape(-1),
+                            np.asarray(RL, dtype=np.uint32).reshape(-1), self.tau, float(latticeSpacing), X, Y, Z)
+        for h in (self.lat, self.model):
+            if h is not None:
+                h.close()
+        self.model = Model.from_spec(self.ctx, spec)
+        self.lat = Lattice(self.ctx, X, Y, Z, particlesPerSite, bytesPerParticle)
+        self.lat.set_row_major(latticeData, latticeSitesData, self._ns, self._nst)
+        self.lattice = HostLattice(X, Y, Z, particlesPerSite, bytesPerParticle, float(latticeSpacing))
+
+    def setReactionRate(self, rxid, rate):
+        """MpdRdmeSolver::setReactionRate: used from the next timestep on."""
+        self.model.set_reaction_rate(rxid, rate)
+
+    # ---- callbacks (MpdRdmeSolver.cu:789-822); override in a subclass
+    def hookSimulation(self, time, lattice):
+        return 0
+
+    def onBeginTrajectory(self, lattice):
+        return 0
+
+    def onEndTrajectory(self, lattice):
+        return 0
+
+    def onWriteLattice(self, time, lattice):
+        return 0
+
+    # ---- outputs (the reference's output-queue data sets)
+    def writeSpeciesCounts(self, time, counts):
+        self.speciesCounts.append((time, counts))
+
+    def writeLattice(self, time, lattice):
+        self.latticeFrames.append((time, lattice.particles.copy(), lattice.sites.copy()))
+
+    def writeLatticeSites(self, time, lattice):
+        pass
+
+    # ---- the trajectory
+    def _download(self):
+        p, s = self.lat.get_native()
+        self.lattice.particles[:] = p
+        self.lattice.sites[:] = s
+
+    def _upload(self, with_sites):
+        self.lat.set_native(self.lattice.particles, self.lattice.sites if with_sites else None)
+
+    def _record_counts(self, time):
+        c = self.lat.species_counts(self._ns)
+        self.writeSpeciesCounts(time, np.asarray(c[1:], dtype=np.uint64))
+
+    def _hook(self, time):
+        r = self.hookSimulation(time, self.lattice)
+        if r == 0:
+            return
+        if r == 1:
+            self._upload(False)
+        elif r == 2:
+            self._upload(True)
+            self.writeLatticeSites(time, self.lattice)
+        elif r == 3:
+            self.writeLatticeSites(time, self.lattice)
+            self._stop = True
+        else:
+            raise RuntimeError("Unknown hook return value")
+
+    def generateTrajectory(self):
+        """MpdRdmeSolver::generateTrajectory (MpdRdmeSolver.cu:485-668): runs
+        timesteps while timestep * tau < maxTime; after a timestep that
+        reaches the next hook, lattice-write or species-write step, calls the
+        hook, writes the lattice, records the counts, in that order.  Counts
+        and lattice are also written at t = 0.  Timesteps between two such
+        steps run as one call."""
+        p = self.parameters
+        counts_interval = int(float(p.get("writeInterval", "0") or 0))
+        lattice_interval = int(float(p.get("latticeWriteInterval", "0") or 0))
+        hook_interval = int(float(p["hookInterval"])) if p.get("hookInterval", "") != "" else None
+        max_time = float(p.get("maxTime", "0") or 0)
+        self._stop = False
+        self._download()
+        self.onBeginTrajectory(self.lattice)
+        self._upload(True)
+        t = 0.0
+        self._record_counts(t)
+        self.writeLattice(t, self.lattice)
+        self._hook(t)
+        total = timesteps_for(max_time, self.tau)
+        done = 0
+        for step, hook, lat, cnt in trajectory_events(total, counts_interval, lattice_interval, hook_interval):
+            if self._stop:
+                break
+            _, self.lastRunStats = self.lat.run(self.model, self.seed, done, step - done, self.overflow_mode)
+            done = step
+            t = step * self.tau
+            if hook:
+                self._download()
+                self._hook(t)
+            if lat:
+                self._download()
+                if self.onWriteLattice(t, self.lattice):
+                    self._upload(True)
+                self.writeLattice(t, self.lattice)
+            if cnt:
+                self._record_counts(t)
+        if not self._stop and done < total:
+            _, self.lastRunStats = self.lat.run(self.model, self.seed, done, total - done, self.overflow_mode)
+        self._download()
+        self.onEndTrajectory(self.lattice)
+
+    def close(self):
+        for h in (self.lat, self.model):
+            if h is not None:
+                h.close()
+        self.lat = self.model = None
+        self.ctx.close()
+
+
+class IntMpdRdmeSolver(MpdRdmeSolver):
+    """lm::rdme::IntMpdRdmeSolver: the same solver on an IntLattice."""
+
+    bytes_per_particle = 4
+
+
+class _ModelInputs:
+    """The fields Model.from_spec reads."""
+
+    def __init__(self, ns, nst, nr, rtype, K, S, D, DF, RL, tau, spacing, X, Y, Z):
+        self.ns, self.nst, self.nr = ns, nst, nr
+        self.rtype, self.K, self.S, self.D, self.DF, self.RL = rtype, K, S, D, DF, RL
+        self.tau, self.spacing = tau, spacing
+        self.X, self.Y, self.Z = X, Y, Z

@@ -426,6 +426,11 @@ class CMEEnsemble:
         per = 1 if c.ndim == 2 else 0
         L.check(L.lib().lmb_cme_set_initial_counts(self.handle, _p(c, L.u32p), per))
 
+    def set_kernel(self, kernel):
+        """L.LMB_CME_KERNEL_AUTO (register-resident form for small models) or
+        L.LMB_CME_KERNEL_GENERIC; both give the same trajectories."""
+        L.check(L.lib().lmb_cme_set_kernel(self.handle, kernel), "lmb_cme_set_kernel")
+
     def run(self, seed, t_end, write_interval):
         L.check(L.lib().lmb_cme_run(self.handle, seed, t_end, write_interval), "lmb_cme_run")
 

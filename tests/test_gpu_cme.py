@@ -110,3 +110,39 @@ def test_second_order_and_zeroth_order_reactions(ctx):
     z = stats.norm.ppf(1 - 0.025 / len(pairs))
     for e, s in pairs:
         compare(out[:, e, s], ref[:, e, s], 0.01 / len(pairs), z, (e, s))
+
+
+def _ensemble_with_kernel(ctx, spec, reps, seed, kernel, segments=1):
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import CMEEnsemble
+    ens = CMEEnsemble(ctx, spec, reps)
+    ens.set_kernel(kernel)
+    ens.begin(seed, spec.max_time, spec.write_interval)
+    for k in range(1, segments + 1):
+        ens.advance_async(spec.max_time * k / segments)
+    out = ens.counts()
+    ev, fin = ens.stats()
+    ens.close()
+    return out, ev, fin
+
+
+@pytest.mark.parametrize("model", ["two_state_gene", "dimer", "wide"])
+def test_compact_kernel_equals_generic(ctx, model):
+    """The register-resident kernel for small models against the generic one:
+    the same trajectories, event counts and records, also when the run is cut
+    into segments.  'wide' has a stoichiometric change of 9, outside the
+    compact form, so both settings run the generic kernel."""
+    from lattice_microbes_b200 import _lib as L
+    if model == "two_state_gene":
+        spec = configs.two_state_gene(max_time=600.0, write_interval=120.0)
+    else:
+        d = 9 if model == "wide" else 2
+        S = np.array([[-d, d, 1, -1], [1, -1, 0, 0]], dtype=np.int32)
+        D = np.array([[1, 0, 0, 1], [0, 1, 0, 0]], dtype=np.uint32)
+        spec = configs.CMESpec(model, 2, np.array([3, 1, 0, 1], np.uint32), np.array([0.02, 0.5, 5.0, 0.1]), S, D,
+                               np.array([20, 0], np.uint32), 50.0, 10.0)
+    gen, ev_g, fin_g = _ensemble_with_kernel(ctx, spec, 3000, 21, L.LMB_CME_KERNEL_GENERIC)
+    auto, ev_a, fin_a = _ensemble_with_kernel(ctx, spec, 3000, 21, L.LMB_CME_KERNEL_AUTO, segments=3)
+    assert fin_g == fin_a == 3000
+    assert ev_g == ev_a and ev_g > 3000
+    assert np.array_equal(gen, auto)

@@ -1,0 +1,80 @@
+"""The pyLM-style solver classes (lattice_microbes_b200.rdme) driven as pyLM
+and jLM drive lm::rdme::MpdRdmeSolver: parameter map, buildModel,
+buildDiffusionModel with row-major lattice data, generateTrajectory with a
+hookSimulation override.  Every record and the final lattice must equal the
+same trajectory replayed range by range through the C ABI."""
+import numpy as np
+import pytest
+
+from lattice_microbes_b200 import configs
+from tests import ref_cpu_lib
+from tests.test_gpu_cpp_solver import _row_major_int, clear_left, replay
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(kind, spec, hook, params):
+    from lattice_microbes_b200.rdme import IntMpdRdmeSolver, MpdRdmeSolver
+    base = MpdRdmeSolver if kind == "byte" else IntMpdRdmeSolver
+
+    class Solver(base):
+        calls = 0
+
+        def hookSimulation(self, time, lattice):
+            Solver.calls += 1
+            if hook.startswith("clear_left:"):
+                lattice.particles[:] = clear_left(spec, lattice.particles, int(hook.split(":")[1]))
+                return 1
+            if hook.startswith("stop_after:") and Solver.calls >= int(hook.split(":")[1]):
+                return 3
+            return 0
+
+    s = Solver(0)
+    s.initialize(3, params)
+    init = configs.species_counts(spec.lattice, spec.nsites, spec.slots, spec.bytes_per_slot, spec.ns)[1:]
+    s.buildModel(spec.ns, spec.nr, init, spec.rtype, spec.K, np.asarray(spec.S).reshape(-1),
+                 np.asarray(spec.D).reshape(-1))
+    lat_rm, sites_rm = ref_cpu_lib.row_major(spec) if kind == "byte" else _row_major_int(spec)
+    s.buildDiffusionModel(spec.nst, np.asarray(spec.DF).reshape(-1), np.asarray(spec.RL).reshape(-1), spec.X,
+                          spec.Y, spec.Z, spec.slots, spec.bytes_per_slot, spec.spacing, lat_rm, sites_rm)
+    return s, Solver
+
+
+@pytest.mark.parametrize("kind", ["byte", "int"])
+def test_python_solver_matches_replay(gpu, kind):
+    if kind == "byte":
+        spec = configs.config0(seed=5, edge=16, nA=600, nB=600)
+        spec.K = spec.K * np.array([300.0, 30.0])
+    else:
+        spec = configs.random_problem(8, X=16, Y=8, Z=8, slots=16, bytes_per_slot=4, density=1.5, nst=2)
+    steps, ce, le, he = 301, 50, 100, 70
+    params = {"seed": "9", "timestep": repr(spec.tau), "maxTime": repr((steps - 0.5) * spec.tau),
+              "writeInterval": str(ce), "latticeWriteInterval": str(le), "hookInterval": str(he)}
+    s, cls = _solver(kind, spec, "clear_left:1", params)
+    s.generateTrajectory()
+    ref_c, ref_f, ref_final = replay(spec, s.seed, steps, ce, le, he, "clear_left:1")
+    assert s.seed == (9 << 16) | 3
+    assert len(s.speciesCounts) == len(ref_c) == 1 + steps // ce
+    for (ta, a), (tb, b) in zip(s.speciesCounts, ref_c):
+        assert ta == tb and np.array_equal(a, b)
+    assert len(s.latticeFrames) == len(ref_f)
+    for (_, a, _), b in zip(s.latticeFrames, ref_f):
+        assert np.array_equal(a, b)
+    assert np.array_equal(s.lattice.particles, ref_final)
+    assert cls.calls == 1 + steps // he
+    s.close()
+
+
+def test_python_solver_hook_3_stops(gpu):
+    spec = configs.config0(seed=6, edge=16, nA=300, nB=300)
+    steps, ce, le, he = 200, 20, 1000, 30
+    params = {"seed": "9", "timestep": repr(spec.tau), "maxTime": repr((steps - 0.5) * spec.tau),
+              "writeInterval": str(ce), "latticeWriteInterval": str(le), "hookInterval": str(he)}
+    s, _ = _solver("byte", spec, "stop_after:3", params)
+    s.generateTrajectory()
+    ref_c, _, ref_final = replay(spec, s.seed, steps, ce, le, he, "stop_after:3")
+    assert np.array_equal(s.lattice.particles, ref_final)
+    assert len(s.speciesCounts) == len(ref_c)
+    assert all(np.array_equal(a[1], b[1]) for a, b in zip(s.speciesCounts, ref_c))
+    assert s.speciesCounts[-1][0] == 60 * spec.tau
+    s.close()
