@@ -282,16 +282,13 @@ def ncu_traffic_per_launch(workload, kernel):
 def run_ours(a):
     import numpy as np
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from lattice_microbes_b200.replicas import Ranks, aggregate_rate
+    ranks = Ranks()
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     device = local if world > 1 else 0
     torch.cuda.set_device(device)
+    ranks.init("nccl")
 
     # CPU baseline first (spawned workers, before any GPU work on this rank).
     w = WORKLOADS[a.workload]
@@ -307,7 +304,7 @@ def run_ours(a):
             cpu_mpd = {"value": val, "unit": METRIC, "cores": cores, "sample": sample}
 
     from lattice_microbes_b200 import configs
-    from lattice_microbes_b200.solver import Context, Lattice, Model, compose_seed, kernel_launches
+    from lattice_microbes_b200.solver import Context, Lattice, Model, kernel_launches
 
     T = a.timesteps_per_step or w["timesteps_per_step"]
     spec = make_spec(a.workload, 1 + rank)
@@ -318,7 +315,7 @@ def run_ours(a):
     model = Model.from_spec(ctx, spec)
     lat = Lattice(ctx, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
     lat.set_native(spec.lattice, spec.sites)
-    seed = compose_seed(2024, rank)
+    seed = ranks.seed(2024)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
 
     # The reference's own kernels (compiled for sm_100a from its sources) on
@@ -356,8 +353,7 @@ def run_ours(a):
     # ---- device-timed throughput (inputs resident in HBM) ----
     clocks = ClockSampler(device)
     times = []
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize(device)
     launches0 = kernel_launches()
     clocks.start()
@@ -374,16 +370,10 @@ def run_ours(a):
             step += T
     torch.cuda.synchronize(device)
     clock_info = clocks.stop()
-    launches = kernel_launches() - launches0 - 0
-    if world > 1:
-        dist.barrier()
-    my_ms = sum(times)
-    ms_total = my_ms
-    if world > 1:
-        t = torch.tensor([my_ms], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
-    value = N * T * a.steps * world / (ms_total / 1e3)
+    launches = kernel_launches() - launches0
+    ranks.barrier()
+    ms_total = ranks.max(sum(times), device)
+    value = aggregate_rate(N * T * a.steps, ms_total, world)
 
     # ---- per-kernel device times (roofline of the dominant kernel) ----
     st, phase_ms, phase_n = lat.run_profiled(model, seed, step, T)
@@ -413,8 +403,7 @@ def run_ours(a):
     import ctypes as C
     from lattice_microbes_b200 import _lib as L
     e2e_ms = []
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     for _ in range(a.steps):
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
@@ -423,12 +412,8 @@ def run_ours(a):
         lat.run(model, seed, 0, T)
         L.check(L.lib().lmb_lattice_get_native(lat.handle, C.cast(h_out.data_ptr(), L.u32p), None))
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = N * T * a.steps * world / (e2e_total / 1e3)
+    e2e_total = ranks.max(sum(e2e_ms), device)
+    e2e_value = aggregate_rate(N * T * a.steps, e2e_total, world)
 
     if rank == 0:
         line = {
@@ -491,9 +476,7 @@ def run_ours(a):
     lat.close()
     model.close()
     ctx.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.finish()
 
 
 def run_reference(a):
