@@ -136,6 +136,22 @@ __device__ __forceinline__ float lookup_T(const DevTables &m, uint32_t p, uint32
     return tload(m.T + ((size_t)src * m.nst + dst) * m.ns + (p - 1u));
 }
 
+// One row T[src][dst][*] of the transition table, held in registers: the
+// lookups of a site's particles need no access to the table set itself.
+struct TRow {
+    const float *row;  // null when src or dst is out of range
+    uint32_t ns;
+    __device__ __forceinline__ TRow(const float *T, uint32_t ns_, uint32_t nst, uint32_t src, uint32_t dst)
+        : row(src < nst && dst < nst ? T + ((size_t)src * nst + dst) * ns_ : nullptr), ns(ns_)
+    {
+    }
+    // lookup_T for particle p, the same value.
+    __device__ __forceinline__ float operator()(uint32_t p) const
+    {
+        return (row && (uint32_t)(p - 1u) < ns) ? tload(row + (p - 1u)) : 0.0f;
+    }
+};
+
 // Queues one overflowed particle; the list index comes from an atomic, the
 // sort key restores a deterministic order later.
 __device__ __forceinline__ void push_overflow(RunState *rs, OverflowEntry *list, uint32_t cap,

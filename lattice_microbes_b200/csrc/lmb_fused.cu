@@ -325,6 +325,9 @@ __device__ __forceinline__ void tile_timestep(const Geometry &g, const DevTables
     for (uint32_t q = 0; q < mt.nst; q++) zeroth |= mt.qp0[q] != 0.0f;
     const bool react_inline = with_reaction && !zeroth;
     const unsigned long long th_rx = timestep_hash(seed, step, 3);
+    // The transition table's base and sizes, in registers for the sweeps.
+    const float *Tq = mt.T;
+    const uint32_t ns = mt.ns, nst = mt.nst;
     if (tid < 4) t.cnt[tid] = 0;
     __syncthreads();
 #pragma unroll 1
@@ -373,11 +376,18 @@ __device__ __forceinline__ void tile_timestep(const Geometry &g, const DevTables
             if ((src_o[rp * MW + (xp >> 5)] >> (xp & 31u)) & 1u) load_smem<BPS, S>(src_w, R, lp, pl);
             const bool record = phase == 2 || (t.rowflag[r] & ROW_OWNED);
             own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], rowbase[r] + x, rowbase[rm] + xm,
-                                     rowbase[rp] + xp, th, mt, record, (uint32_t)phase + 1, rs, list, cap);
+                                     rowbase[rp] + xp, th, Tq, ns, nst, record, (uint32_t)phase + 1, rs, list,
+                                     cap);
             // After the z sweep an owned site reacts right away in
-            // registers, when only occupied sites can react.
-            if (phase == 2 && react_inline && !own.empty())
-                own = react_site_ool<BPS, S>(own, T[l], rowbase[r] + x, th_rx, mt, rs, list, cap);
+            // registers, when only occupied sites can react.  Its exact
+            // early exit is taken here; only a site whose draw may react
+            // makes the call.
+            if (phase == 2 && react_inline && !own.empty()) {
+                const uint32_t gi = rowbase[r] + x, ts = T[l];
+                const float r0 = hash_float((unsigned long long)gi << 1, th_rx);
+                if (reaction_may_fire((uint32_t)__popc(occupied_slots<BPS, S>(own)), tload(mt.qp0 + ts), ts, r0, mt))
+                    own = react_site_ool<BPS, S>(own, ts, gi, th_rx, mt, rs, list, cap);
+            }
             if (!own.empty()) {
                 store_smem<BPS, S>(dst_w, R, l, own);
                 atomicOr(&dst_o[r * MW + (x >> 5)], 1u << (x & 31u));

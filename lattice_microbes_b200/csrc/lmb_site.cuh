@@ -247,21 +247,23 @@ template <int BPS, int S>
 __device__ __forceinline__ SiteWords<BPS, S> sweep_site(const SiteWords<BPS, S> &own, const SiteWords<BPS, S> &mn,
                                                         const SiteWords<BPS, S> &pl, uint32_t t, uint32_t tm,
                                                         uint32_t tp, uint32_t gi, uint32_t gim, uint32_t gip,
-                                                        unsigned long long th, const DevTables &m, bool record,
-                                                        uint32_t phase, RunState *rs, OverflowEntry *list,
-                                                        uint32_t cap)
+                                                        unsigned long long th, const float *T, uint32_t ns,
+                                                        uint32_t nst, bool record, uint32_t phase, RunState *rs,
+                                                        OverflowEntry *list, uint32_t cap)
 {
     SiteBuilder<BPS, S> b;
     b.init();
     constexpr int CB = CountBits<S>::value;
+    // The four rows of T the site's particles use.
+    const TRow own_m(T, ns, nst, t, tm), own_p(T, ns, nst, t, tp), mn_p(T, ns, nst, tm, t), pl_m(T, ns, nst, tp, t);
     // Stayers of this site, slot order.
 #pragma unroll
     for (int k = 0; k < S; k++) {
         const uint32_t p = own.slot(k);
         if (p) {
             const float r = hash_float(((unsigned long long)gi << CB) | (unsigned)k, th);
-            const float qm = lookup_T(m, p, t, tm);
-            const float qp = lookup_T(m, p, t, tp);
+            const float qm = own_m(p);
+            const float qp = own_p(p);
             const bool plus = (r >= 0.5f) && (r < __fadd_rn(qp, 0.5f));
             if (!plus && !(r < qm)) b.push(p, record, rs, list, cap, phase, gi);
         }
@@ -272,7 +274,7 @@ __device__ __forceinline__ SiteWords<BPS, S> sweep_site(const SiteWords<BPS, S> 
         const uint32_t p = mn.slot(k);
         if (p) {
             const float r = hash_float(((unsigned long long)gim << CB) | (unsigned)k, th);
-            const float qp = lookup_T(m, p, tm, t);
+            const float qp = mn_p(p);
             if ((r >= 0.5f) && (r < __fadd_rn(qp, 0.5f))) b.push(p, record, rs, list, cap, phase, gi);
         }
     }
@@ -282,7 +284,7 @@ __device__ __forceinline__ SiteWords<BPS, S> sweep_site(const SiteWords<BPS, S> 
         const uint32_t p = pl.slot(k);
         if (p) {
             const float r = hash_float(((unsigned long long)gip << CB) | (unsigned)k, th);
-            const float qm = lookup_T(m, p, tp, t);
+            const float qm = pl_m(p);
             if (r < qm) b.push(p, record, rs, list, cap, phase, gi);
         }
     }
