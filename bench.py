@@ -204,16 +204,59 @@ def cpu_nsm_sample(workload, sim_time, cores):
 # --------------------------------------------------------------------------
 
 class ClockSampler:
+    """SM clocks, power and clock-event reasons of `device` during a timed
+    region: read through NVML every 20 ms on a background thread (reads
+    only; no setting is touched), or from nvidia-smi's 200 ms log when NVML
+    is not available."""
+
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device):
         self.device = device
         self.proc = None
         self.path = None
+        self.thread = None
+        self.samples = []
+
+    def _nvml_start(self):
+        import threading
+        import pynvml as nv
+        nv.nvmlInit()
+        try:
+            import torch
+            index = torch.cuda._get_nvml_device_index(self.device)
+        except Exception:
+            index = self.device
+        h = nv.nvmlDeviceGetHandleByIndex(index)
+        self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        self.stop_flag = threading.Event()
+
+        def run():
+            while not self.stop_flag.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, [k for k, v in bits.items() if r & v]))
+                except Exception:
+                    pass
+                self.stop_flag.wait(0.02)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def start(self):
+        try:
+            self._nvml_start()
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -225,6 +268,17 @@ class ClockSampler:
 
     def stop(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            sm = [float(v) for v, _ in self.samples]
+            if sm:
+                out["sm_mhz"] = statistics.median(sm)
+            out["sm_max_mhz"] = float(self.max_mhz)
+            out["reasons"] = sorted({k for _, ks in self.samples for k in ks})
+            out["samples"] = len(sm)
+            out["source"] = "nvml, 20 ms"
+            return out
         if self.proc is None:
             return out
         self.proc.terminate()
@@ -239,12 +293,11 @@ class ClockSampler:
             return out
         sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
         for r in rows:
             if len(r) < 9:
                 continue
-            for k, nm in enumerate(names):
+            for k, nm in enumerate(self.REASONS):
                 if r[5 + k].strip() == "Active":
                     reasons.add(nm)
         if sm:
@@ -253,6 +306,7 @@ class ClockSampler:
             out["sm_max_mhz"] = max(mx)
         out["reasons"] = sorted(reasons)
         out["samples"] = len(sm)
+        out["source"] = "nvidia-smi, 200 ms"
         return out
 
 
