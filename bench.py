@@ -720,7 +720,7 @@ def run_cme(a):
     cores = host_cores()
     cpu = None
     if not a.no_cpu_baseline:
-        v, sample = cpu_gillespie_sample(64, cores)
+        v, sample = cpu_gillespie_sample(1500, cores)
         if v is not None:
             cpu = {"value": v, "unit": "replicates/s", "cores": cores, "kind": "reference", "sample": sample}
     torch.cuda.set_device(0)
