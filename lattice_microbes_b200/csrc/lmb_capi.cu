@@ -63,8 +63,9 @@ struct lmb_lattice {
     RunState *rs_host;  // pinned
     OverflowEntry *list;
     uint32_t cap;
-    // Per-phase schedule: sites the z sweep lists for the reaction step
-    // (allocated when the schedule is first chosen).
+    // Per-phase schedule: sites the z sweep lists for the reaction step,
+    // rx_cap entries of two words (allocated when the schedule is first
+    // chosen).
     uint32_t *rx_sites;
     uint32_t rx_cap;
     unsigned long long *counts_dev;
@@ -621,7 +622,7 @@ extern "C" int lmb_lattice_set_schedule(lmb_lattice *l, int schedule, uint32_t T
         if (!l->rx_sites) {
             CK(cudaSetDevice(l->ctx->device));
             const uint32_t cap = reaction_list_capacity(l->g);
-            CK(cudaMalloc(&l->rx_sites, (size_t)cap * sizeof(uint32_t)));
+            CK(cudaMalloc(&l->rx_sites, (size_t)cap * 2 * sizeof(uint32_t)));
             l->rx_cap = cap;
         }
         l->schedule = schedule;

@@ -71,11 +71,6 @@ struct SiteWords {
 #pragma unroll
         for (int k = 0; k < W; k++) w[k] = __ldg(lat + (size_t)k * N + i);
     }
-    __device__ __forceinline__ void load_plain(const uint32_t *lat, uint32_t N, uint32_t i)
-    {
-#pragma unroll
-        for (int k = 0; k < W; k++) w[k] = lat[(size_t)k * N + i];
-    }
     __device__ __forceinline__ void store(uint32_t *lat, uint32_t N, uint32_t i) const
     {
 #pragma unroll
@@ -96,6 +91,13 @@ struct SiteWords {
                 more = BPS == 1 ? (w[k] >> 24) != 0u : w[k] != 0u;
             }
         }
+    }
+    // Loads words 0 .. nw - 1 (independent loads) and clears the rest: a
+    // packed site whose particle count is known.
+    __device__ __forceinline__ void load_first(const uint32_t *lat, uint32_t N, uint32_t i, uint32_t nw)
+    {
+#pragma unroll
+        for (int k = 0; k < W; k++) w[k] = (uint32_t)k < nw ? lat[(size_t)k * N + i] : 0u;
     }
     __device__ __forceinline__ uint32_t slot(int k) const
     {

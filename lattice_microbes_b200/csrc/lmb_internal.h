@@ -91,7 +91,8 @@ struct RunState {
 
 // Kernel launchers (lmb_kernels.cu).  Each returns a cudaError_t.
 // The z sweep (dim 2) lists in rx_sites the sites whose reaction step could
-// change them, when rx_sites is given; launch_reaction then visits only
+// change them, when rx_sites is given (rx_cap entries of two words: the site
+// and its type << 8 | particle count); launch_reaction then visits only
 // those (every site when the list is absent or overflowed rx_cap).
 cudaError_t launch_sweep(int bytes_per_slot, int slots, int dim, const uint32_t *src, uint32_t *dst,
                          const uint8_t *sites, const Geometry &g, const DevTables &m, RunState *rs,

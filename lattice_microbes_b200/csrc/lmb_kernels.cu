@@ -96,8 +96,9 @@ __device__ __forceinline__ void sweep_neighbours(const Geometry &g, uint32_t x, 
 
 // Appends site i (type t, n particles after the z sweep) to the reaction
 // list when its reaction step could change it (reaction_may_fire), one
-// atomic per group of converged lanes.  Entries past rx_cap are dropped but
-// counted, which sends the reaction step over every site.
+// atomic per group of converged lanes.  An entry is the pair (i, t << 8 |
+// n).  Entries past rx_cap are dropped but counted, which sends the reaction
+// step over every site.
 __device__ __forceinline__ void list_for_reaction(uint32_t n, uint32_t t, uint32_t i, int lid, const DevTables &m,
                                                   RunState *rs, uint32_t *rx_sites, uint32_t rx_cap)
 {
@@ -115,7 +116,7 @@ __device__ __forceinline__ void list_for_reaction(uint32_t n, uint32_t t, uint32
     if (lane == leader) base = atomicAdd(&rs->rx_count, (uint32_t)__popc(want));
     base = __shfl_sync(want, base, leader);
     const uint32_t idx = base + __popc(want & ((1u << lane) - 1u));
-    if (idx < rx_cap) rx_sites[idx] = i;
+    if (idx < rx_cap) reinterpret_cast<uint2 *>(rx_sites)[idx] = make_uint2(i, (t << 8) | n);
 }
 
 template <int BPS, int S, int DIM>
@@ -151,8 +152,16 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
         tm = __ldg(sites + im);
         tp = __ldg(sites + ip);
         occ = occupied_slots<BPS, S>(own);
+        if constexpr (BPS == 4) {
+            // Only a site's occupied slots are ever read from the tile (by
+            // the hashing, its own stayers and its neighbours' arrivals).
 #pragma unroll
-        for (int k = 0; k < W; k++) sw[k][lid] = own.w[k];
+            for (int k = 0; k < W; k++)
+                if ((occ >> k) & 1u) sw[k][lid] = own.w[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < W; k++) sw[k][lid] = own.w[k];
+        }
     }
     sc[lid] = 0;
     __syncwarp();
@@ -337,13 +346,22 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
     const uint32_t n = all ? g.N : listed;
     const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        const uint32_t i = all ? j : rx_sites[j];
-        const uint32_t t = __ldg(sites + i);
-        SiteWords<BPS, S> s;
         // The z sweep wrote this buffer, so its sites are packed (occupied
         // slots first, whatever the input had): only the planes holding
         // particles are read.
-        s.load_packed(lat, g.N, i);
+        uint32_t i, t;
+        SiteWords<BPS, S> s;
+        if (all) {
+            i = j;
+            t = __ldg(sites + i);
+            s.load_packed(lat, g.N, i);
+        } else {
+            const uint2 e = reinterpret_cast<const uint2 *>(rx_sites)[j];
+            const uint32_t np = e.y & 0xFFu;
+            i = e.x;
+            t = e.y >> 8;
+            s.load_first(lat, g.N, i, BPS == 1 ? (np + 3u) / 4u : np);
+        }
         if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) s.store(lat, g.N, i);
     }
 }

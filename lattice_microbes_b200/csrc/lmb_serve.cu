@@ -102,12 +102,12 @@ struct lmb_server {
 
 // Device bytes a resident solve holds: two particle buffers, site types, the
 // overflow queue and run state (lmb_lattice_create), the reaction site list
-// of the per-phase schedule (N / 8 + 4096 entries), and the model tables
+// of the per-phase schedule (N / 8 + 4096 entries of 8 bytes), and the model tables
 // (lmb_model_create).
 static uint64_t request_bytes(const lmb_server *s, const Request &r)
 {
     const uint64_t N = (uint64_t)r.X * r.Y * r.Z;
-    const uint64_t lattice = 2ull * s->words * N * 4 + N + 2048ull * 16 + 256 + 4ull * (N / 8 + 4096);
+    const uint64_t lattice = 2ull * s->words * N * 4 + N + 2048ull * 16 + 256 + 8ull * (N / 8 + 4096);
     const uint64_t tables = 4ull * ((uint64_t)r.nst * r.nst * r.ns + r.nst + (uint64_t)r.nst * r.ns +
                                     (uint64_t)r.nst * r.ns * r.ns + 8ull * r.nr) +
                             (uint64_t)r.nr * (r.ns + r.nst) + 4096;
