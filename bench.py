@@ -794,8 +794,10 @@ def run_serve(a):
     1k..20k timesteps; configs.serve_stream) replayed at their arrival times
     into the solve server (continuous batching, 150 GB budget, ByteLattice
     16 slots).  Compared with sequential plain runs: the same requests solved
-    one at a time in arrival order (lmb_run each), their latencies computed
-    from the same arrival times."""
+    one at a time in arrival order (lmb_run each), each timed over the same
+    per-request work as a served solve (set-up, upload, run, counts and
+    lattice back, release), their latencies computed from the same arrival
+    times."""
     import numpy as np
     import torch
 
@@ -853,19 +855,23 @@ def run_serve(a):
     solo_s = []
     from lattice_microbes_b200 import _lib as LL
     for sp, r, sd in zip(specs, stream_reqs, seeds):
-        m = Model.from_spec(ctx, sp)
-        L2 = Lattice(ctx, sp.X, sp.Y, sp.Z, 16, 1)
-        # The schedule the server gives a large solve (per-phase when dense).
-        if sp.nsites >= (1 << 17) and r.density >= 0.05:
-            L2.set_schedule(LL.LMB_SCHEDULE_PHASES)
+        # The same work per request as the server does for a solve: model
+        # and lattice set-up (per-phase schedule for a large dense solve, as
+        # the server gives it), upload, the run, the species counts and the
+        # lattice copied back, device memory freed.
         torch.cuda.synchronize(0)
         s0 = time.perf_counter()
+        m = Model.from_spec(ctx, sp)
+        L2 = Lattice(ctx, sp.X, sp.Y, sp.Z, 16, 1)
+        if sp.nsites >= (1 << 17) and r.density >= 0.05:
+            L2.set_schedule(LL.LMB_SCHEDULE_PHASES)
         L2.set_native(sp.lattice, sp.sites)
         L2.run(m, sd, 0, r.timesteps)
         L2.species_counts(sp.ns)
-        solo_s.append(time.perf_counter() - s0)
+        L2.get_native()
         L2.close()
         m.close()
+        solo_s.append(time.perf_counter() - s0)
     finish, seq_lat = 0.0, []
     for r, d in zip(stream_reqs, solo_s):
         finish = max(finish, r.arrival) + d

@@ -86,6 +86,8 @@ struct Result {
 
 struct lmb_server {
     lmb_ctx *ctx;
+    // Large solves run on their own stream, beside the small solves' batch.
+    lmb_ctx *solo_ctx;
     uint32_t slots, bps, words;
     uint64_t budget;
     uint32_t max_active, chunk;
@@ -125,6 +127,13 @@ extern "C" int lmb_server_create(lmb_ctx *ctx, uint32_t particles_per_site, uint
     if (!s) return LMB_E_NOMEM;
     s->ctx = ctx;
     ctx_retain(ctx);
+    s->solo_ctx = nullptr;
+    const int rc = lmb_ctx_create(ctx->device, &s->solo_ctx);
+    if (rc != LMB_OK) {
+        ctx_release(ctx);
+        delete s;
+        return rc;
+    }
     s->slots = particles_per_site;
     s->bps = bytes_per_particle;
     s->words = bytes_per_particle == 1 ? particles_per_site / 4 : particles_per_site;
@@ -156,6 +165,7 @@ extern "C" int lmb_server_destroy(lmb_server *s)
     if (s->batch) lmb_batch_destroy(s->batch);
     for (Active &a : s->active) release_active(s, a);
     lmb_ctx *c = s->ctx;
+    if (s->solo_ctx) lmb_ctx_destroy(s->solo_ctx);
     delete s;
     ctx_release(c);
     return LMB_OK;
@@ -271,11 +281,12 @@ static int admit(lmb_server *s)
         d.timestep = a.req.timestep;
         d.lattice_spacing = a.req.spacing;
         s->bytes_in_use += a.req.bytes;
-        int rc = lmb_model_create(s->ctx, &d, a.req.X, a.req.Y, a.req.Z, &a.model);
-        if (rc == LMB_OK) rc = lmb_lattice_create(s->ctx, a.req.X, a.req.Y, a.req.Z, s->slots, s->bps, &a.lat);
-        if (rc == LMB_OK) rc = lmb_lattice_set_native(a.lat, a.req.particles.data(), a.req.sites.data());
         const uint64_t nsites = (uint64_t)a.req.X * a.req.Y * a.req.Z;
         a.solo = nsites >= SOLO_SITES;
+        lmb_ctx *c = a.solo ? s->solo_ctx : s->ctx;
+        int rc = lmb_model_create(c, &d, a.req.X, a.req.Y, a.req.Z, &a.model);
+        if (rc == LMB_OK) rc = lmb_lattice_create(c, a.req.X, a.req.Y, a.req.Z, s->slots, s->bps, &a.lat);
+        if (rc == LMB_OK) rc = lmb_lattice_set_native(a.lat, a.req.particles.data(), a.req.sites.data());
         if (rc == LMB_OK && a.solo) {
             const double density = (double)count_particles(a.req.particles, s->bps) / (double)nsites;
             if (density >= DENSE_PARTICLES_PER_SITE) rc = lmb_lattice_set_schedule(a.lat, LMB_SCHEDULE_PHASES, 0, 0);
@@ -330,26 +341,33 @@ extern "C" int lmb_server_step(lmb_server *s, uint32_t *active_out, uint32_t *qu
             rc = lmb_batch_run_ranges_async(s->batch, seeds.data(), firsts.data(), counts.data(),
                                             LMB_OVERFLOW_CLASSIC);
             if (rc) return rc;
-            std::vector<lmb_run_stats> bst(nb);
-            rc = lmb_batch_wait(s->batch, bst.data());
-            if (rc != LMB_OK && rc != LMB_E_OVERFLOW_EXHAUSTED && rc != LMB_E_OVERFLOW_UNRESOLVED) return rc;
-            for (uint32_t q = 0; q < nb; q++) st[small[q]] = bst[q];
         }
         // Large solves, each filling the device alone, are served in arrival
-        // order: the oldest one runs its chunk in this step (the others wait
-        // their turn instead of all finishing late), while the small ones
-        // advance in the batch every step.
+        // order: the oldest one runs its chunk in this step, on its own
+        // stream beside the batch (the others wait their turn instead of all
+        // finishing late), while the small ones advance in the batch every
+        // step.
+        int solo = -1;
         for (uint32_t j = 0; j < n; j++) {
             Active &a = s->active[j];
             if (!a.solo) continue;
             const uint32_t left = a.req.timesteps - a.done;
             rc = lmb_run_async(a.lat, a.model, a.req.seed, a.done, left < s->chunk ? left : s->chunk,
                                LMB_OVERFLOW_CLASSIC);
-            if (rc) return rc;
-            rc = lmb_run_wait(a.lat, &st[j]);
-            if (rc != LMB_OK && rc != LMB_E_OVERFLOW_EXHAUSTED && rc != LMB_E_OVERFLOW_UNRESOLVED) return rc;
+            if (rc) break;
+            solo = (int)j;
             break;
         }
+        int rc_batch = LMB_OK;
+        if (!small.empty()) {
+            std::vector<lmb_run_stats> bst(small.size());
+            rc_batch = lmb_batch_wait(s->batch, bst.data());
+            for (size_t q = 0; q < small.size(); q++) st[small[q]] = bst[q];
+        }
+        if (solo >= 0) rc = lmb_run_wait(s->active[solo].lat, &st[solo]);
+        if (rc != LMB_OK && rc != LMB_E_OVERFLOW_EXHAUSTED && rc != LMB_E_OVERFLOW_UNRESOLVED) return rc;
+        if (rc_batch != LMB_OK && rc_batch != LMB_E_OVERFLOW_EXHAUSTED && rc_batch != LMB_E_OVERFLOW_UNRESOLVED)
+            return rc_batch;
         rc = LMB_OK;
         // Retire finished and failed solves; keep the order of the rest.
         std::vector<Active> keep;

@@ -142,8 +142,12 @@ __device__ __forceinline__ void compact_site(const uint32_t *w, uint32_t mask, u
     lo = 0;
     hi = 0;
     n = 0;
+    // Words past the mask's highest bit contribute nothing (a packed site's
+    // particles sit in its first words).
+    const uint32_t top = 32u - __clz(mask);
 #pragma unroll
     for (int k = 0; k < S / 4; k++) {
+        if (4u * k >= top) break;
         const uint32_t m = (mask >> (4 * k)) & 0xFu;
         const unsigned long long c = compact_bytes(w[k], m);
         // Append the (up to 4) bytes at byte offset n (< 16).
