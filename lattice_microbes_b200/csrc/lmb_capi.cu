@@ -822,7 +822,7 @@ static cudaError_t enqueue_step(lmb_lattice *l, lmb_model *m, cudaStream_t st)
     if (m->nr > 0 && (e = launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap,
                                           rx, l->rx_cap, st)) != cudaSuccess)
         return e;
-    return launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, st);
+    return launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, rx ? l->rx_cap : 0, st);
 }
 
 // Captures GRAPH_STEPS timesteps starting at the current buffer parity, or
@@ -1010,7 +1010,8 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
                                c->stream));
         CK(cudaEventRecord(E[7], c->stream));
         CK(cudaEventRecord(E[8], c->stream));
-        CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, c->stream));
+        CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, rx ? l->rx_cap : 0,
+                          c->stream));
         CK(cudaEventRecord(E[9], c->stream));
     }
     CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));

@@ -87,6 +87,7 @@ struct RunState {
     uint32_t max_site_type;
     uint32_t tiles_done;  // fused kernel: blocks finished in this launch
     uint32_t rx_count;    // per-phase schedule: sites the z sweep listed for the reaction step
+    uint32_t rx_skip;     // timesteps left to run without the list (it overflowed recently)
 };
 
 // Kernel launchers (lmb_kernels.cu).  Each returns a cudaError_t.
@@ -101,8 +102,10 @@ cudaError_t launch_sweep(int bytes_per_slot, int slots, int dim, const uint32_t 
 cudaError_t launch_reaction(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
                             const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list,
                             uint32_t cap, const uint32_t *rx_sites, uint32_t rx_cap, cudaStream_t stream);
+// Also closes the timestep's reaction list (rx_cap: its capacity, 0 when
+// there is none).
 cudaError_t launch_resolve(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
-                           const Geometry &g, RunState *rs, OverflowEntry *list, uint32_t cap,
+                           const Geometry &g, RunState *rs, OverflowEntry *list, uint32_t cap, uint32_t rx_cap,
                            cudaStream_t stream);
 cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
                              cudaStream_t stream);

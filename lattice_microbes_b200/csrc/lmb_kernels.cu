@@ -133,6 +133,8 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
     __shared__ uint32_t sw[W][NT];
     __shared__ Code sc[NT];
     if (rs->status != LMB_OK) return;
+    // The z sweep lists reaction sites unless the list overflowed recently.
+    const bool listing = DIM == 2 && rs->rx_skip == 0;
     uint32_t x, y, z;
     bool in, out;
     sweep_site_of<DIM>(g, x, y, z, in, out);
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
         }
 #pragma unroll
         for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][oid] : 0u;
-        if (DIM == 2 && rx_sites)
+        if (DIM == 2 && rx_sites && listing)
             list_for_reaction(n < (uint32_t)S ? n : (uint32_t)S, t, i, lid, m, rs, rx_sites, rx_cap);
     } else {
         // The neighbours: from the tile, or loaded with their choices drawn here.
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
         const SiteWords<BPS, S> out = assemble_site<BPS, S>(own, c_own, mn, c_mn, pl, c_pl, i, true,
                                                             (uint32_t)DIM + 1, rs, list, cap);
         out.store(dst, g.N, i);
-        if (DIM == 2 && rx_sites)
+        if (DIM == 2 && rx_sites && listing)
             list_for_reaction((uint32_t)__popc(occupied_slots<BPS, S>(out)), t, i, lid, m, rs, rx_sites, rx_cap);
     }
 }
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
     if (rs->status != LMB_OK) return;
     // The sites the z sweep listed, or every site when it listed none or
     // more than the list holds.
-    const uint32_t listed = rx_sites ? rs->rx_count : 0xFFFFFFFFu;
+    const uint32_t listed = rx_sites && rs->rx_skip == 0 ? rs->rx_count : 0xFFFFFFFFu;
     const bool all = listed > rx_cap;
     const uint32_t n = all ? g.N : listed;
     const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
@@ -376,12 +378,19 @@ template <int BPS, int S>
 __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__restrict__ lat,
                                                                   const uint8_t *__restrict__ sites, Geometry g,
                                                                   RunState *__restrict__ rs,
-                                                                  OverflowEntry *__restrict__ list, uint32_t cap)
+                                                                  OverflowEntry *__restrict__ list, uint32_t cap,
+                                                                  uint32_t rx_cap)
 {
     extern __shared__ OverflowEntry sh[];
     if (rs->status != LMB_OK) return;
-    // The reaction step of this timestep has read its site list.
-    if (threadIdx.x == 0) rs->rx_count = 0;
+    // The reaction step of this timestep has read its site list.  A list
+    // that overflowed is not built for the next 31 timesteps (the reaction
+    // step visits every site meanwhile; either way the result is the same).
+    if (threadIdx.x == 0) {
+        if (rs->rx_skip) rs->rx_skip--;
+        else if (rs->rx_count > rx_cap) rs->rx_skip = 31;
+        rs->rx_count = 0;
+    }
     resolve_block<BPS, S>(lat, sites, g, rs, list, cap, sh);
 }
 
@@ -399,6 +408,7 @@ __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, ui
     rs->reactions = 0;
     rs->tiles_done = 0;
     rs->rx_count = 0;
+    rs->rx_skip = 0;
     if (mode == LMB_OVERFLOW_CLASSIC) {
         rs->ovf_count = 0;
         rs->carried = 0;
@@ -425,6 +435,7 @@ __global__ void begin_batch_kernel(RunState *const *rs_ptrs, const uint32_t *see
     rs->reactions = 0;
     rs->tiles_done = 0;
     rs->rx_count = 0;
+    rs->rx_skip = 0;
     if (mode == LMB_OVERFLOW_CLASSIC) {
         rs->ovf_count = 0;
         rs->carried = 0;
@@ -654,7 +665,7 @@ cudaError_t launch_reaction(int bps, int slots, uint32_t *lat, const uint8_t *si
 }
 
 cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sites, const Geometry &g, RunState *rs,
-                           OverflowEntry *list, uint32_t cap, cudaStream_t stream)
+                           OverflowEntry *list, uint32_t cap, uint32_t rx_cap, cudaStream_t stream)
 {
     uint32_t pow2 = 1;
     while (pow2 < cap) pow2 <<= 1;
@@ -668,7 +679,7 @@ cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sit
             cudaFuncSetAttribute(resolve_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             raised[dev] = true;
         }
-        resolve_kernel<BPS, S><<<1, RESOLVE_THREADS, smem, stream>>>(lat, sites, g, rs, list, cap);
+        resolve_kernel<BPS, S><<<1, RESOLVE_THREADS, smem, stream>>>(lat, sites, g, rs, list, cap, rx_cap);
     })
 }
 

@@ -131,6 +131,24 @@ def test_reaction_site_list_vs_oracle(ctx, shape, per_slot, slots, bps):
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("slots,bps,zeroth", [(8, 1, False), (16, 1, True), (16, 4, True)])
+def test_reaction_list_skip_window_vs_oracle(ctx, slots, bps, zeroth):
+    """A dense lattice whose reaction list overflows: the next 31 timesteps
+    react over every site without building the list, then the list is
+    tried again; 40 timesteps cross that window, in graph replays and in
+    single launches."""
+    spec = configs.random_problem(22, X=64, Y=32, Z=32, slots=slots, bytes_per_slot=bps, density=0.2 * slots,
+                                  nst=3, qmax=0.3, zeroth=zeroth)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 8, 0, 40)
+    assert rc_ref == 0
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 8, 0, 40, schedule="phases", chunks=[33, 7])
+    assert rc == rc_ref
+    if rc == 0:
+        assert sum(x.reactions for x in st) == st_ref.reactions
+    assert np.array_equal(out, ref)
+
+
 @pytest.mark.parametrize("schedule", SCHEDULES)
 @pytest.mark.parametrize("slots,bps,dens", [(8, 1, 5.0), (16, 4, 12.0), (8, 4, 6.0)])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
