@@ -266,9 +266,9 @@ int lmb_batch_destroy(lmb_batch *batch);
  * and their device bytes fit hbm_budget_bytes, runs chunk_timesteps
  * timesteps of every resident solve (fewer for a solve near its end), and
  * retires the solves that are done.  Solves of at least 131,072 sites
- * (which fill the device alone) run their chunks on their own instead, one
- * such solve at a time in arrival order, on a second stream beside the
- * small solves' batch, with the per-phase schedule when they hold 0.05
+ * (which fill the device alone) run their chunks on their own instead, on
+ * two streams beside the small solves' batch (each stream one solve at a
+ * time, in arrival order), with the per-phase schedule when they hold 0.05
  * particles per site or more.  A solve's result is lmb_run's result for it
  * alone, bit for bit.  Replaces the reference's one-solver-per-thread
  * replicate runner (core/ReplicateRunner.cpp:84-166) for many independent

@@ -16,9 +16,12 @@
 // Small solves share the batched launches, where they would otherwise each
 // pay a launch per timestep for little work; a solve of at least
 // SOLO_SITES sites fills the device by itself and runs its chunks on its own
-// (same stream, after the batch), one large solve at a time in arrival
-// order, with the schedule that suits its particle density: the per-phase
-// kernels for dense lattices, the fused kernel for sparse ones.
+// stream, beside the batch.  There are SOLO_STREAMS such streams; a large
+// solve is given one at admission (in turn), and each stream advances its
+// oldest solve in every step, so that large solves finish in arrival order
+// per stream instead of all finishing late.  A large solve takes the
+// schedule that suits its particle density: the per-phase kernels for dense
+// lattices, the fused kernel for sparse ones.
 //
 // Host code only; it drives the device through the C ABI of lmb_capi.cu.
 #include <chrono>
@@ -59,9 +62,11 @@ struct Active {
     double t_admit;
     lmb_run_stats stats;
     bool solo;
+    uint32_t stream;  // large solves: which solo stream
 };
 
 constexpr uint64_t SOLO_SITES = 1u << 17;      // 128 Ki sites (about 51^3)
+constexpr uint32_t SOLO_STREAMS = 2;
 constexpr double DENSE_PARTICLES_PER_SITE = 0.05;
 
 // Particles in a native lattice (nonzero slots).
@@ -86,8 +91,9 @@ struct Result {
 
 struct lmb_server {
     lmb_ctx *ctx;
-    // Large solves run on their own stream, beside the small solves' batch.
-    lmb_ctx *solo_ctx;
+    // Large solves run on their own streams, beside the small solves' batch.
+    lmb_ctx *solo_ctx[SOLO_STREAMS];
+    uint32_t next_stream;
     uint32_t slots, bps, words;
     uint64_t budget;
     uint32_t max_active, chunk;
@@ -127,12 +133,16 @@ extern "C" int lmb_server_create(lmb_ctx *ctx, uint32_t particles_per_site, uint
     if (!s) return LMB_E_NOMEM;
     s->ctx = ctx;
     ctx_retain(ctx);
-    s->solo_ctx = nullptr;
-    const int rc = lmb_ctx_create(ctx->device, &s->solo_ctx);
-    if (rc != LMB_OK) {
-        ctx_release(ctx);
-        delete s;
-        return rc;
+    s->next_stream = 0;
+    for (uint32_t k = 0; k < SOLO_STREAMS; k++) s->solo_ctx[k] = nullptr;
+    for (uint32_t k = 0; k < SOLO_STREAMS; k++) {
+        const int rc = lmb_ctx_create(ctx->device, &s->solo_ctx[k]);
+        if (rc != LMB_OK) {
+            for (uint32_t q = 0; q < k; q++) lmb_ctx_destroy(s->solo_ctx[q]);
+            ctx_release(ctx);
+            delete s;
+            return rc;
+        }
     }
     s->slots = particles_per_site;
     s->bps = bytes_per_particle;
@@ -165,7 +175,8 @@ extern "C" int lmb_server_destroy(lmb_server *s)
     if (s->batch) lmb_batch_destroy(s->batch);
     for (Active &a : s->active) release_active(s, a);
     lmb_ctx *c = s->ctx;
-    if (s->solo_ctx) lmb_ctx_destroy(s->solo_ctx);
+    for (uint32_t k = 0; k < SOLO_STREAMS; k++)
+        if (s->solo_ctx[k]) lmb_ctx_destroy(s->solo_ctx[k]);
     delete s;
     ctx_release(c);
     return LMB_OK;
@@ -283,7 +294,12 @@ static int admit(lmb_server *s)
         s->bytes_in_use += a.req.bytes;
         const uint64_t nsites = (uint64_t)a.req.X * a.req.Y * a.req.Z;
         a.solo = nsites >= SOLO_SITES;
-        lmb_ctx *c = a.solo ? s->solo_ctx : s->ctx;
+        a.stream = 0;
+        if (a.solo) {
+            a.stream = s->next_stream;
+            s->next_stream = (s->next_stream + 1) % SOLO_STREAMS;
+        }
+        lmb_ctx *c = a.solo ? s->solo_ctx[a.stream] : s->ctx;
         int rc = lmb_model_create(c, &d, a.req.X, a.req.Y, a.req.Z, &a.model);
         if (rc == LMB_OK) rc = lmb_lattice_create(c, a.req.X, a.req.Y, a.req.Z, s->slots, s->bps, &a.lat);
         if (rc == LMB_OK) rc = lmb_lattice_set_native(a.lat, a.req.particles.data(), a.req.sites.data());
@@ -342,21 +358,17 @@ extern "C" int lmb_server_step(lmb_server *s, uint32_t *active_out, uint32_t *qu
                                             LMB_OVERFLOW_CLASSIC);
             if (rc) return rc;
         }
-        // Large solves, each filling the device alone, are served in arrival
-        // order: the oldest one runs its chunk in this step, on its own
-        // stream beside the batch (the others wait their turn instead of all
-        // finishing late), while the small ones advance in the batch every
-        // step.
-        int solo = -1;
-        for (uint32_t j = 0; j < n; j++) {
+        // Large solves: the oldest one of each solo stream runs its chunk in
+        // this step, beside the batch and the other stream's.
+        int solo[SOLO_STREAMS];
+        for (uint32_t k = 0; k < SOLO_STREAMS; k++) solo[k] = -1;
+        for (uint32_t j = 0; j < n && rc == LMB_OK; j++) {
             Active &a = s->active[j];
-            if (!a.solo) continue;
+            if (!a.solo || solo[a.stream] >= 0) continue;
             const uint32_t left = a.req.timesteps - a.done;
             rc = lmb_run_async(a.lat, a.model, a.req.seed, a.done, left < s->chunk ? left : s->chunk,
                                LMB_OVERFLOW_CLASSIC);
-            if (rc) break;
-            solo = (int)j;
-            break;
+            if (rc == LMB_OK) solo[a.stream] = (int)j;
         }
         int rc_batch = LMB_OK;
         if (!small.empty()) {
@@ -364,7 +376,11 @@ extern "C" int lmb_server_step(lmb_server *s, uint32_t *active_out, uint32_t *qu
             rc_batch = lmb_batch_wait(s->batch, bst.data());
             for (size_t q = 0; q < small.size(); q++) st[small[q]] = bst[q];
         }
-        if (solo >= 0) rc = lmb_run_wait(s->active[solo].lat, &st[solo]);
+        for (uint32_t k = 0; k < SOLO_STREAMS; k++) {
+            if (solo[k] < 0) continue;
+            const int r = lmb_run_wait(s->active[solo[k]].lat, &st[solo[k]]);
+            if (rc == LMB_OK) rc = r;
+        }
         if (rc != LMB_OK && rc != LMB_E_OVERFLOW_EXHAUSTED && rc != LMB_E_OVERFLOW_UNRESOLVED) return rc;
         if (rc_batch != LMB_OK && rc_batch != LMB_E_OVERFLOW_EXHAUSTED && rc_batch != LMB_E_OVERFLOW_UNRESOLVED)
             return rc_batch;
