@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "lmb.h"
 #include "lmb_device.cuh"
 #include "lmb_fused.h"
@@ -305,8 +307,10 @@ __device__ __forceinline__ void tile_load(const uint32_t *__restrict__ src, cons
 // One timestep of the tile in shared memory, from (w, o) = the region at the
 // start of the timestep; on return (w, o) hold the owned rows after the x,
 // y and z sweeps and the reaction (the other rows are stale).  Ends with a
-// block barrier.
-template <int BPS, int S>
+// block barrier.  ROWS: transition-table lookups through rows held in
+// registers (TTable) rather than through the table set (TableSet); the two
+// give the same values and differ only in register use.
+template <int BPS, int S, bool ROWS>
 __device__ __forceinline__ void tile_timestep(const Geometry &g, const DevTables &mt, RunState *__restrict__ rs,
                                               OverflowEntry *__restrict__ list, uint32_t cap, const TileShape &ts,
                                               const TileSmem &t, uint32_t *&src_w, uint32_t *&dst_w,
@@ -325,9 +329,10 @@ __device__ __forceinline__ void tile_timestep(const Geometry &g, const DevTables
     for (uint32_t q = 0; q < mt.nst; q++) zeroth |= mt.qp0[q] != 0.0f;
     const bool react_inline = with_reaction && !zeroth;
     const unsigned long long th_rx = timestep_hash(seed, step, 3);
-    // The transition table's base and sizes, in registers for the sweeps.
-    const float *Tq = mt.T;
-    const uint32_t ns = mt.ns, nst = mt.nst;
+    using Tables = typename std::conditional<ROWS, TTable, TableSet>::type;
+    Tables tabs;
+    if constexpr (ROWS) tabs = TTable{mt.T, mt.ns, mt.nst};
+    else tabs = TableSet{&mt};
     if (tid < 4) t.cnt[tid] = 0;
     __syncthreads();
 #pragma unroll 1
@@ -376,8 +381,7 @@ __device__ __forceinline__ void tile_timestep(const Geometry &g, const DevTables
             if ((src_o[rp * MW + (xp >> 5)] >> (xp & 31u)) & 1u) load_smem<BPS, S>(src_w, R, lp, pl);
             const bool record = phase == 2 || (t.rowflag[r] & ROW_OWNED);
             own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], rowbase[r] + x, rowbase[rm] + xm,
-                                     rowbase[rp] + xp, th, Tq, ns, nst, record, (uint32_t)phase + 1, rs, list,
-                                     cap);
+                                     rowbase[rp] + xp, th, tabs, record, (uint32_t)phase + 1, rs, list, cap);
             // After the z sweep an owned site reacts right away in
             // registers, when only occupied sites can react.  Its exact
             // early exit is taken here; only a site whose draw may react
@@ -482,7 +486,7 @@ __device__ __forceinline__ void tile_store(uint32_t *__restrict__ dst, const Geo
 // whole block.  The block is flat (FUSED_THREADS threads); the tile's
 // logical bx x by layout (bx a multiple of 32, so a warp is 32 consecutive x
 // of one row) comes from the tile shape.
-template <int BPS, int S>
+template <int BPS, int S, bool ROWS>
 __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst,
                                            const uint8_t *__restrict__ sites, const Geometry &g, const DevTables &m,
                                            RunState *__restrict__ rs, OverflowEntry *__restrict__ list, uint32_t cap,
@@ -513,7 +517,8 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     tile_load<BPS, S, false>(src, sites, g, ts, t, t.A, t.occA, false, true);
 
     uint32_t *src_w = t.A, *dst_w = t.B, *src_o = t.occA, *dst_o = t.occB;
-    tile_timestep<BPS, S>(g, s_mt, rs, list, cap, ts, t, src_w, dst_w, src_o, dst_o, seed, step, with_reaction);
+    tile_timestep<BPS, S, ROWS>(g, s_mt, rs, list, cap, ts, t, src_w, dst_w, src_o, dst_o, seed, step,
+                                with_reaction);
     tile_store<BPS, S>(dst, g, ts, t, src_w, src_o);
 
     // The last block to finish resolves the overflow queue and advances the
@@ -542,15 +547,18 @@ __global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_
                                                                    const __grid_constant__ TileShape ts,
                                                                    int with_reaction)
 {
-    fused_tile<BPS, S>(src, dst, sites, g, m, rs, list, cap, ts, with_reaction, blockIdx.x, gridDim.x);
+    fused_tile<BPS, S, true>(src, dst, sites, g, m, rs, list, cap, ts, with_reaction, blockIdx.x, gridDim.x);
 }
 
 // A batch of lattices advanced together: block b runs the tile of the job
 // whose tile range holds b.  The buffers a job reads and writes alternate
 // with `parity` (flipped every timestep), from the job's buffer index at the
 // start of the run.
+// Two blocks per SM: the batch plan picks tiles of at most 100 KB of shared
+// memory for that (the bound also lets the compiler keep the tile's state in
+// registers rather than spill it).
 template <int BPS, int S>
-__global__ void __launch_bounds__(FUSED_THREADS) fused_batch_kernel(const FusedJob *__restrict__ jobs,
+__global__ void __launch_bounds__(FUSED_THREADS, 2) fused_batch_kernel(const FusedJob *__restrict__ jobs,
                                                                     uint32_t njobs, uint32_t parity)
 {
     uint32_t lo = 0, hi = njobs;
@@ -561,8 +569,8 @@ __global__ void __launch_bounds__(FUSED_THREADS) fused_batch_kernel(const FusedJ
     }
     const FusedJob &j = jobs[lo];
     const uint32_t c = j.cur0 ^ parity;
-    fused_tile<BPS, S>(j.buf[c], j.buf[c ^ 1], j.sites, j.g, j.m, j.rs, j.list, j.cap, j.ts, j.with_reaction,
-                       blockIdx.x - j.tile_begin, j.ts.tiles_y * j.ts.tiles_z);
+    fused_tile<BPS, S, false>(j.buf[c], j.buf[c ^ 1], j.sites, j.g, j.m, j.rs, j.list, j.cap, j.ts,
+                              j.with_reaction, blockIdx.x - j.tile_begin, j.ts.tiles_y * j.ts.tiles_z);
 }
 
 // ---------------------------------------------------------------------------

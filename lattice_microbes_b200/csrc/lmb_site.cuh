@@ -247,19 +247,40 @@ __device__ __forceinline__ SiteWords<BPS, S> assemble_site(const SiteWords<BPS, 
 // extra hashes.
 // gi/gim/gip: lattice indices of the site and its minus / plus neighbours
 // (they key the hash); t/tm/tp: their site types.
-template <int BPS, int S>
+// Transition-table access for sweep_site, two forms giving the same values:
+// TTable keeps the table's base and sizes in registers and reads through a
+// site's rows; TableSet reads through the table set for every lookup (fewer
+// live registers).
+struct TTable {
+    const float *T;
+    uint32_t ns, nst;
+    __device__ __forceinline__ TRow row(uint32_t src, uint32_t dst) const { return TRow(T, ns, nst, src, dst); }
+};
+
+struct TableSetRow {
+    const DevTables *m;
+    uint32_t src, dst;
+    __device__ __forceinline__ float operator()(uint32_t p) const { return lookup_T(*m, p, src, dst); }
+};
+
+struct TableSet {
+    const DevTables *m;
+    __device__ __forceinline__ TableSetRow row(uint32_t src, uint32_t dst) const { return TableSetRow{m, src, dst}; }
+};
+
+template <int BPS, int S, class Tables>
 __device__ __forceinline__ SiteWords<BPS, S> sweep_site(const SiteWords<BPS, S> &own, const SiteWords<BPS, S> &mn,
                                                         const SiteWords<BPS, S> &pl, uint32_t t, uint32_t tm,
                                                         uint32_t tp, uint32_t gi, uint32_t gim, uint32_t gip,
-                                                        unsigned long long th, const float *T, uint32_t ns,
-                                                        uint32_t nst, bool record, uint32_t phase, RunState *rs,
-                                                        OverflowEntry *list, uint32_t cap)
+                                                        unsigned long long th, const Tables &tabs, bool record,
+                                                        uint32_t phase, RunState *rs, OverflowEntry *list,
+                                                        uint32_t cap)
 {
     SiteBuilder<BPS, S> b;
     b.init();
     constexpr int CB = CountBits<S>::value;
     // The four rows of T the site's particles use.
-    const TRow own_m(T, ns, nst, t, tm), own_p(T, ns, nst, t, tp), mn_p(T, ns, nst, tm, t), pl_m(T, ns, nst, tp, t);
+    const auto own_m = tabs.row(t, tm), own_p = tabs.row(t, tp), mn_p = tabs.row(tm, t), pl_m = tabs.row(tp, t);
     // Stayers of this site, slot order.
 #pragma unroll
     for (int k = 0; k < S; k++) {
