@@ -537,8 +537,11 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     }
 }
 
-template <int BPS, int S>
-__global__ void __launch_bounds__(FUSED_THREADS) fused_step_kernel(const uint32_t *__restrict__ src,
+// MINB: blocks per SM the launch bounds promise, the number the tile's
+// shared memory lets an SM hold (2, 3 or 4): the compiler then keeps as much
+// of the tile's state in registers as that occupancy allows.
+template <int BPS, int S, int MINB>
+__global__ void __launch_bounds__(FUSED_THREADS, MINB) fused_step_kernel(const uint32_t *__restrict__ src,
                                                                    uint32_t *__restrict__ dst,
                                                                    const uint8_t *__restrict__ sites, Geometry g,
                                                                    const __grid_constant__ DevTables m,
@@ -643,7 +646,7 @@ bool fused_default_shape(const Geometry &g, int bps, int slots, TileShape &ts)
 // The dynamic shared-memory limit is raised once per instantiation (per
 // device) to the largest size any launch needs; setting it on every launch
 // costs host time comparable to the kernel itself.
-template <int BPS, int S>
+template <int BPS, int S, int MINB>
 static cudaError_t ensure_smem_limit(size_t smem)
 {
     static size_t granted[64] = {0};
@@ -653,8 +656,8 @@ static cudaError_t ensure_smem_limit(size_t smem)
     // The kernel's static shared memory counts against the default 48 KB
     // too, so the limit is raised for any size not granted yet.
     if (smem <= granted[dev]) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(fused_step_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(fused_step_kernel<BPS, S, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) granted[dev] = smem;
     return e;
 }
@@ -684,13 +687,29 @@ bool fused_batch_shape(const Geometry &g, int bps, int slots, TileShape &ts)
     return found;
 }
 
-#define FUSED_DISPATCH(BPS_, S_)                                                                       \
-    if (bps == BPS_ && slots == S_) {                                                                  \
-        cudaError_t e = ensure_smem_limit<BPS_, S_>(smem);                                             \
-        if (e != cudaSuccess) return e;                                                                \
-        fused_step_kernel<BPS_, S_><<<grid, block, smem, stream>>>(src, dst, sites, g, m, rs, list, cap, ts, \
-                                                                   with_reaction);                     \
-        return cudaGetLastError();                                                                     \
+template <int BPS, int S, int MINB>
+static cudaError_t fused_launch(dim3 grid, dim3 block, size_t smem, cudaStream_t stream, const uint32_t *src,
+                                uint32_t *dst, const uint8_t *sites, const Geometry &g, const DevTables &m,
+                                RunState *rs, OverflowEntry *list, uint32_t cap, const TileShape &ts,
+                                int with_reaction)
+{
+    cudaError_t e = ensure_smem_limit<BPS, S, MINB>(smem);
+    if (e != cudaSuccess) return e;
+    fused_step_kernel<BPS, S, MINB><<<grid, block, smem, stream>>>(src, dst, sites, g, m, rs, list, cap, ts,
+                                                                   with_reaction);
+    return cudaGetLastError();
+}
+
+#define FUSED_DISPATCH(BPS_, S_)                                                                            \
+    if (bps == BPS_ && slots == S_) {                                                                       \
+        if (per_sm >= 4)                                                                                    \
+            return fused_launch<BPS_, S_, 4>(grid, block, smem, stream, src, dst, sites, g, m, rs, list, cap, ts, \
+                                             with_reaction);                                                \
+        if (per_sm == 3)                                                                                    \
+            return fused_launch<BPS_, S_, 3>(grid, block, smem, stream, src, dst, sites, g, m, rs, list, cap, ts, \
+                                             with_reaction);                                                \
+        return fused_launch<BPS_, S_, 2>(grid, block, smem, stream, src, dst, sites, g, m, rs, list, cap, ts,    \
+                                         with_reaction);                                                    \
     }
 
 cudaError_t launch_fused(int bps, int slots, const uint32_t *src, uint32_t *dst, const uint8_t *sites,
@@ -700,6 +719,9 @@ cudaError_t launch_fused(int bps, int slots, const uint32_t *src, uint32_t *dst,
     const uint32_t W = bps == 1 ? slots / 4 : slots;
     const size_t smem = fused_smem_bytes(ts, g.X, W, cap, m.stage_bytes);
     const dim3 grid(ts.tiles_y * ts.tiles_z), block(FUSED_THREADS);
+    // Blocks of this size an SM's 228 KB of shared memory holds (the static
+    // part and 1 KB reserved per block included).
+    const uint32_t per_sm = (uint32_t)((228u * 1024u) / (smem + 3088u + 1024u));
     count_launch();
     FUSED_DISPATCH(1, 4)
     FUSED_DISPATCH(1, 8)
