@@ -221,8 +221,11 @@ public:
         onBeginTrajectory(host_);
         upload(true);
         double time = 0.0;
+        maxParticleCounts_.assign(ns_ + 1, 0);
+        maxSiteCounts_.assign(nst_, 0);
         recordSpeciesCounts(time);
-        writeLattice(time, host_);
+        writeLatticeRecord(time);
+        updateMaxSiteCounts();  // initMaxCounts (MpdRdmeSolver.cu:548, 824-850)
         hookCheck(time);
         // The reference loops while timestep * tau < maxTime: that many
         // timesteps in all.
@@ -251,7 +254,7 @@ public:
                 if (step >= nextLattice) {
                     download();
                     if (onWriteLattice(time, host_)) upload(true);
-                    writeLattice(time, host_);
+                    writeLatticeRecord(time);
                     nextLattice += latticeInterval;
                 }
                 if (step >= nextCounts) {
@@ -262,6 +265,7 @@ public:
         }
         download();
         onEndTrajectory(host_);
+        writeMaxCounts(maxParticleCounts_, maxSiteCounts_);
     }
 
     uint32_t seed() const { return seed_; }
@@ -282,6 +286,15 @@ protected:
     virtual void writeSpeciesCounts(double /*time*/, const std::vector<uint64_t> &/*counts*/) {}
     virtual void writeLattice(double /*time*/, const HostLattice &/*lattice*/) {}
     virtual void writeLatticeSites(double /*time*/, const HostLattice &/*lattice*/) {}
+    /* MpdRdmeSolver::writeMaxCounts (MpdRdmeSolver.cu:921-932), at the end of
+     * the trajectory: per species id (index 0 unused) the largest count seen
+     * at the start and at each lattice write; per site type (type 0 not
+     * counted) the largest number of sites seen at the start and at each
+     * site write. */
+    virtual void writeMaxCounts(const std::vector<uint32_t> & /*maxParticleCounts*/,
+                                const std::vector<uint32_t> & /*maxSiteCounts*/)
+    {
+    }
 
     std::string param(const char *key) const
     {
@@ -336,6 +349,27 @@ private:
         writeSpeciesCounts(time, c);
     }
 
+    /* writeLatticeData (MpdRdmeSolver.cu:854-883): the particle maxima, then
+     * the frame. */
+    void writeLatticeRecord(double time)
+    {
+        std::vector<uint64_t> c(ns_ + 1);
+        check(lmb_lattice_species_counts(lattice_, ns_, c.data()), "writeLatticeData");
+        for (uint32_t s = 1; s <= ns_; s++)
+            if (c[s] > maxParticleCounts_[s]) maxParticleCounts_[s] = (uint32_t)c[s];
+        writeLattice(time, host_);
+    }
+
+    /* The site-type maxima (MpdRdmeSolver.cu:896-912), from the host copy. */
+    void updateMaxSiteCounts()
+    {
+        std::vector<uint32_t> c(nst_, 0);
+        for (uint8_t t : host_.sites)
+            if (t > 0 && t < nst_) c[t]++;
+        for (uint32_t t = 0; t < nst_; t++)
+            if (c[t] > maxSiteCounts_[t]) maxSiteCounts_[t] = c[t];
+    }
+
     void hookCheck(double time)
     {
         switch (hookSimulation(time, host_)) {
@@ -343,9 +377,11 @@ private:
         case 1: upload(false); break;
         case 2:
             upload(true);
+            updateMaxSiteCounts();
             writeLatticeSites(time, host_);
             break;
         case 3:
+            updateMaxSiteCounts();
             writeLatticeSites(time, host_);
             stop_ = true;
             break;
@@ -368,6 +404,7 @@ private:
     HostLattice host_;
     lmb_run_stats stats_{};
     bool stop_ = false;
+    std::vector<uint32_t> maxParticleCounts_, maxSiteCounts_;
 };
 
 /* lm::rdme::IntMpdRdmeSolver: the same solver on an IntLattice. */

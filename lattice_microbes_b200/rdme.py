@@ -196,6 +196,8 @@ class MpdRdmeSolver:
         self.lattice = None
         self.speciesCounts = []       # (time, counts of species 1..ns)
         self.latticeFrames = []       # (time, particles copy, sites copy)
+        self.maxParticleCounts = None  # per species id (index 0 unused)
+        self.maxSiteCounts = None      # per site type (type 0 not counted)
         self.lastRunStats = None
         self._stop = False
 
@@ -278,6 +280,14 @@ class MpdRdmeSolver:
     def writeLatticeSites(self, time, lattice):
         pass
 
+    def writeMaxCounts(self, maxParticleCounts, maxSiteCounts):
+        """MpdRdmeSolver::writeMaxCounts (MpdRdmeSolver.cu:921-932), at the
+        end of the trajectory: per species id the largest count seen at the
+        start and at each lattice write; per site type the largest number of
+        sites seen at the start and at each site write."""
+        self.maxParticleCounts = maxParticleCounts
+        self.maxSiteCounts = maxSiteCounts
+
     # ---- the trajectory
     def _download(self):
         p, s = self.lat.get_native()
@@ -291,6 +301,19 @@ class MpdRdmeSolver:
         c = self.lat.species_counts(self._ns)
         self.writeSpeciesCounts(time, np.asarray(c[1:], dtype=np.uint64))
 
+    def _write_lattice(self, time):
+        # writeLatticeData (MpdRdmeSolver.cu:854-883): the particle maxima,
+        # then the frame.
+        c = np.asarray(self.lat.species_counts(self._ns), dtype=np.uint32)
+        c[0] = 0
+        np.maximum(self._max_particles, c, out=self._max_particles)
+        self.writeLattice(time, self.lattice)
+
+    def _update_site_maxima(self):
+        t = self.lattice.sites
+        c = np.bincount(t[(t > 0) & (t < self._nst)], minlength=self._nst)[:self._nst].astype(np.uint32)
+        np.maximum(self._max_sites, c, out=self._max_sites)
+
     def _hook(self, time):
         r = self.hookSimulation(time, self.lattice)
         if r == 0:
@@ -299,8 +322,10 @@ class MpdRdmeSolver:
             self._upload(False)
         elif r == 2:
             self._upload(True)
+            self._update_site_maxima()
             self.writeLatticeSites(time, self.lattice)
         elif r == 3:
+            self._update_site_maxima()
             self.writeLatticeSites(time, self.lattice)
             self._stop = True
         else:
@@ -323,8 +348,11 @@ class MpdRdmeSolver:
         self.onBeginTrajectory(self.lattice)
         self._upload(True)
         t = 0.0
+        self._max_particles = np.zeros(self._ns + 1, dtype=np.uint32)
+        self._max_sites = np.zeros(self._nst, dtype=np.uint32)
         self._record_counts(t)
-        self.writeLattice(t, self.lattice)
+        self._write_lattice(t)
+        self._update_site_maxima()  # initMaxCounts (MpdRdmeSolver.cu:548, 824-850)
         self._hook(t)
         total = timesteps_for(max_time, self.tau)
         done = 0
@@ -341,13 +369,14 @@ class MpdRdmeSolver:
                 self._download()
                 if self.onWriteLattice(t, self.lattice):
                     self._upload(True)
-                self.writeLattice(t, self.lattice)
+                self._write_lattice(t)
             if cnt:
                 self._record_counts(t)
         if not self._stop and done < total:
             _, self.lastRunStats = self.lat.run(self.model, self.seed, done, total - done, self.overflow_mode)
         self._download()
         self.onEndTrajectory(self.lattice)
+        self.writeMaxCounts(self._max_particles.copy(), self._max_sites.copy())
 
     def close(self):
         for h in (self.lat, self.model):

@@ -107,6 +107,14 @@ protected:
         append(dir + "/final.u32", lat.particles.data(), lat.particles.size());
         return 0;
     }
+    void writeMaxCounts(const std::vector<uint32_t> &mp, const std::vector<uint32_t> &ms) override
+    {
+        std::ofstream f(dir + "/max.txt");
+        for (uint32_t v : mp) f << v << " ";
+        f << "\n";
+        for (uint32_t v : ms) f << v << " ";
+        f << "\n";
+    }
 };
 
 template <typename Base>

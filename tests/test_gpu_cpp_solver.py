@@ -142,7 +142,22 @@ def run_driver(driver, tmp_path, spec, steps, count_every, lattice_every, hook_e
     frames = np.fromfile(os.path.join(d, "frames.u32"), dtype=np.uint32).reshape(-1, W)
     final = np.fromfile(os.path.join(d, "final.u32"), dtype=np.uint32)
     events = open(os.path.join(d, "events.txt")).read().split("\n")
-    return counts, frames, final, events, (seed_top << 16) | (replicate & 0xFFFF)
+    lines = open(os.path.join(d, "max.txt")).read().strip().split("\n")
+    maxima = [np.array([int(v) for v in ln.split()]) for ln in lines]
+    return counts, frames, final, events, (seed_top << 16) | (replicate & 0xFFFF), maxima
+
+
+def expected_maxima(spec, frames):
+    """Particle maxima over the lattice frames (the start is the first), site
+    maxima from the site types (the hooks here do not change them)."""
+    mp = np.zeros(spec.ns + 1, dtype=np.int64)
+    for f in frames:
+        c = configs.species_counts(f, spec.nsites, spec.slots, spec.bytes_per_slot, spec.ns).astype(np.int64)
+        c[0] = 0
+        mp = np.maximum(mp, c)
+    t = spec.sites
+    ms = np.bincount(t[(t > 0) & (t < spec.nst)], minlength=spec.nst)[:spec.nst]
+    return mp, ms
 
 
 @pytest.mark.parametrize("kind", ["byte", "int"])
@@ -153,7 +168,8 @@ def test_generate_trajectory_matches_replay(driver, tmp_path, kind):
     else:
         spec = configs.random_problem(8, X=16, Y=8, Z=8, slots=16, bytes_per_slot=4, density=1.5, nst=2)
     steps, ce, le, he = 301, 50, 100, 70
-    got_c, got_f, got_final, events, seed = run_driver(driver, tmp_path, spec, steps, ce, le, he, "clear_left:1")
+    got_c, got_f, got_final, events, seed, maxima = run_driver(driver, tmp_path, spec, steps, ce, le, he,
+                                                               "clear_left:1")
     ref_c, ref_f, ref_final = replay(spec, seed, steps, ce, le, he, "clear_left:1")
     assert [t for t, _ in got_c] == pytest.approx([t for t, _ in ref_c], rel=0, abs=0)
     assert len(got_c) == len(ref_c) == 1 + steps // ce
@@ -163,6 +179,8 @@ def test_generate_trajectory_matches_replay(driver, tmp_path, kind):
     for a, b in zip(got_f, ref_f):
         assert np.array_equal(a, b)
     assert np.array_equal(got_final, ref_final)
+    mp, ms = expected_maxima(spec, ref_f)
+    assert np.array_equal(maxima[0], mp) and np.array_equal(maxima[1], ms)
     assert sum(1 for e in events if e.startswith("hook")) == 1 + steps // he
     # The hook really changed the trajectory: species 1 is gone from the left half at each hook.
     assert got_c[-1][1][0] < got_c[0][1][0]
@@ -171,7 +189,7 @@ def test_generate_trajectory_matches_replay(driver, tmp_path, kind):
 def test_hook_return_3_stops(driver, tmp_path):
     spec = configs.config0(seed=6, edge=16, nA=300, nB=300)
     steps, ce, le, he = 200, 20, 1000, 30
-    got_c, _, got_final, events, seed = run_driver(driver, tmp_path, spec, steps, ce, le, he, "stop_after:3")
+    got_c, _, got_final, events, seed, _ = run_driver(driver, tmp_path, spec, steps, ce, le, he, "stop_after:3")
     ref_c, _, ref_final = replay(spec, seed, steps, ce, le, he, "stop_after:3")
     assert np.array_equal(got_final, ref_final)
     assert len(got_c) == len(ref_c) and all(np.array_equal(a[1], b[1]) for a, b in zip(got_c, ref_c))

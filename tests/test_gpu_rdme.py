@@ -8,7 +8,7 @@ import pytest
 
 from lattice_microbes_b200 import configs
 from tests import ref_cpu_lib
-from tests.test_gpu_cpp_solver import _row_major_int, clear_left, replay
+from tests.test_gpu_cpp_solver import _row_major_int, clear_left, expected_maxima, replay
 
 pytestmark = pytest.mark.gpu
 
@@ -62,6 +62,8 @@ def test_python_solver_matches_replay(gpu, kind):
         assert np.array_equal(a, b)
     assert np.array_equal(s.lattice.particles, ref_final)
     assert cls.calls == 1 + steps // he
+    mp, ms = expected_maxima(spec, ref_f)
+    assert np.array_equal(s.maxParticleCounts, mp) and np.array_equal(s.maxSiteCounts, ms)
     s.close()
 
 
