@@ -265,7 +265,7 @@ public:
         }
         download();
         onEndTrajectory(host_);
-        writeMaxCounts(maxParticleCounts_, maxSiteCounts_);
+        if (tracksMaxCounts()) writeMaxCounts(maxParticleCounts_, maxSiteCounts_);
     }
 
     uint32_t seed() const { return seed_; }
@@ -295,6 +295,9 @@ protected:
                                 const std::vector<uint32_t> & /*maxSiteCounts*/)
     {
     }
+    /* IntMpdRdmeSolver::generateTrajectory keeps no maxima (its initMaxCounts
+     * call is disabled, IntMpdRdmeSolver.cu:617) and writes none. */
+    virtual bool tracksMaxCounts() const { return true; }
 
     std::string param(const char *key) const
     {
@@ -412,6 +415,9 @@ class IntMpdRdmeSolver : public MpdRdmeSolver {
 public:
     explicit IntMpdRdmeSolver(int device = 0) : MpdRdmeSolver(device) {}
     uint32_t bytesPerParticle() const override { return 4; }
+
+protected:
+    bool tracksMaxCounts() const override { return false; }
 };
 
 }  // namespace lmb

@@ -184,6 +184,7 @@ class MpdRdmeSolver:
     """lm::rdme::MpdRdmeSolver (ByteLattice); IntMpdRdmeSolver below."""
 
     bytes_per_particle = 1
+    tracks_max_counts = True
 
     def __init__(self, device=0):
         self.ctx = Context(device)
@@ -376,7 +377,8 @@ class MpdRdmeSolver:
             _, self.lastRunStats = self.lat.run(self.model, self.seed, done, total - done, self.overflow_mode)
         self._download()
         self.onEndTrajectory(self.lattice)
-        self.writeMaxCounts(self._max_particles.copy(), self._max_sites.copy())
+        if self.tracks_max_counts:
+            self.writeMaxCounts(self._max_particles.copy(), self._max_sites.copy())
 
     def close(self):
         for h in (self.lat, self.model):
@@ -390,6 +392,9 @@ class IntMpdRdmeSolver(MpdRdmeSolver):
     """lm::rdme::IntMpdRdmeSolver: the same solver on an IntLattice."""
 
     bytes_per_particle = 4
+    # IntMpdRdmeSolver::generateTrajectory keeps no maxima (its initMaxCounts
+    # call is disabled, IntMpdRdmeSolver.cu:617) and writes none.
+    tracks_max_counts = False
 
 
 class _ModelInputs:
