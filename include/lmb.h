@@ -34,6 +34,7 @@ extern "C" {
 #define LMB_E_OVERFLOW_UNRESOLVED (-7) /* "Unable to find an available site" (MpdRdmeSolver.cu:1155-1156) */
 #define LMB_E_TIMEOUT (-8)             /* a bounded device wait gave up */
 #define LMB_E_UNSUPPORTED (-9)         /* size or layout outside the compiled variants */
+#define LMB_E_IO (-10)                 /* IOException: a file could not be created or written */
 
 /* Overflow handlers: parameter "rdme.mpd.overflowhandler" (MpdRdmeSolver.cu:126-146). */
 #define LMB_OVERFLOW_CLASSIC 0

@@ -19,6 +19,7 @@ LMB_E_OVERFLOW_EXHAUSTED = -6
 LMB_E_OVERFLOW_UNRESOLVED = -7
 LMB_E_TIMEOUT = -8
 LMB_E_UNSUPPORTED = -9
+LMB_E_IO = -10
 
 LMB_OVERFLOW_CLASSIC = 0
 LMB_OVERFLOW_RELAXED = 1
@@ -154,6 +155,23 @@ PROTOTYPES = {
     "lmb_cme_stats": (C.c_int, [vp, u64p, u32p]),
     "lmb_cme_set_kernel": (C.c_int, [vp, C.c_int]),
     "lmb_kernel_launches": (C.c_uint64, []),
+    # include/lmb_lmfile.h
+    "lmb_lmfile_create": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
+    "lmb_lmfile_set_parameter": (C.c_int, [vp, C.c_char_p, C.c_char_p]),
+    "lmb_lmfile_set_reaction_model": (C.c_int, [vp, C.c_uint32, C.c_uint32, u32p, u32p, f64p, f64p, i32p, u32p]),
+    "lmb_lmfile_set_diffusion_model": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, C.c_uint32,
+                                                 C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, f64p, u32p]),
+    "lmb_lmfile_set_diffusion_model_lattice": (C.c_int, [vp, vp, u8p]),
+    "lmb_lmfile_append_species_counts": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, f64p, i32p]),
+    "lmb_lmfile_append_lattice": (C.c_int, [vp, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32,
+                                            C.c_uint32, C.c_uint32, vp]),
+    "lmb_lmfile_append_lattice_device": (C.c_int, [vp, C.c_uint32, C.c_double, vp]),
+    "lmb_lmfile_append_sites": (C.c_int, [vp, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32, u8p]),
+    "lmb_lmfile_append_sites_device": (C.c_int, [vp, C.c_uint32, C.c_double, vp]),
+    "lmb_lmfile_write_max_counts": (C.c_int, [vp, C.c_uint32, u32p, C.c_uint32, u32p, C.c_uint32]),
+    "lmb_lmfile_flush": (C.c_int, [vp]),
+    "lmb_lmfile_stats": (C.c_int, [vp, u64p, u64p]),
+    "lmb_lmfile_close": (C.c_int, [vp]),
 }
 
 

@@ -15,7 +15,8 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "liblmb200.so")
 
-SOURCES = ["lmb_kernels.cu", "lmb_fused.cu", "lmb_capi.cu", "lmb_noalloc.cu", "lmb_cme.cu", "lmb_serve.cu"]
+SOURCES = ["lmb_kernels.cu", "lmb_fused.cu", "lmb_capi.cu", "lmb_noalloc.cu", "lmb_cme.cu", "lmb_serve.cu",
+           "lmb_lmfile.cu"]
 HEADERS = ["lmb_internal.h", "lmb_device.cuh", "lmb_site.cuh", "lmb_overflow.cuh", "lmb_fused.h"]
 
 NVCC_FLAGS = [
@@ -43,7 +44,8 @@ def _stale(target, deps):
 def build(verbose=False, force=False, extra_flags=()):
     os.makedirs(BUILD, exist_ok=True)
     inc = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "lmb.h")]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", h)
+                                                       for h in ("lmb.h", "lmb_lmfile.h")]
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
@@ -56,7 +58,7 @@ def build(verbose=False, force=False, extra_flags=()):
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
         cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs,
-               "-lcudart"]
+               "-lcudart", "-lz"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

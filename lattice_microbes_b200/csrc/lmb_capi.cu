@@ -118,6 +118,7 @@ extern "C" const char *lmb_status_string(int s)
     case LMB_E_OVERFLOW_UNRESOLVED: return "Unable to find an available site to handle a particle overflow";
     case LMB_E_TIMEOUT: return "device wait timed out";
     case LMB_E_UNSUPPORTED: return "unsupported lattice layout or size";
+    case LMB_E_IO: return "file could not be created or written";
     default: return "unknown status";
     }
 }
@@ -755,6 +756,19 @@ extern "C" int lmb_lattice_get_row_major(lmb_lattice *l, void *particles, uint8_
     cudaFree(tmp);
     if (tmp_sites) cudaFree(tmp_sites);
     if (e != cudaSuccess) return cuda_status(e);
+    return LMB_OK;
+}
+
+int lmb::lattice_view(const lmb_lattice *l, LatticeView *v)
+{
+    if (!l || !v) return LMB_E_ARG;
+    v->ctx = l->ctx;
+    v->g = l->g;
+    v->bytes_per_slot = l->bps;
+    v->slots = l->slots;
+    v->particles = l->buf[l->cur];
+    v->sites = l->sites;
+    v->pending = l->pending;
     return LMB_OK;
 }
 

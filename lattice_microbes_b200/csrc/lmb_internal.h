@@ -6,6 +6,8 @@
 
 #include <atomic>
 
+struct lmb_lattice;
+
 // A context: one device and one stream.  It lives until its handle and every
 // model, lattice, batch and CME ensemble made from it are destroyed, whatever
 // the order of those calls.
@@ -126,5 +128,17 @@ cudaError_t launch_native_to_row_major(int bytes_per_slot, int slots, const uint
 
 bool slots_supported(int bytes_per_slot, int slots);
 void count_launch(uint64_t n = 1);
+
+// Read-only view of a lattice for code outside the C ABI file (the .lm
+// writer): its context, geometry, layout and current device buffers.
+struct LatticeView {
+    lmb_ctx *ctx;
+    Geometry g;
+    uint32_t bytes_per_slot, slots;
+    const uint32_t *particles;
+    const uint8_t *sites;
+    bool pending;  // an asynchronous run is in flight
+};
+int lattice_view(const lmb_lattice *lattice, LatticeView *view);
 
 }  // namespace lmb

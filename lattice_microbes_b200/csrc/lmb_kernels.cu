@@ -564,12 +564,14 @@ __global__ void native_to_row_major_kernel(const uint32_t *__restrict__ native, 
     if (i >= g.N) return;
     const uint32_t x = i % g.X, y = (i / g.X) % g.Y, z = i / g.XY;
     const size_t r = ((size_t)x * g.Y + y) * g.Z + z;
-    SiteWords<BPS, S> s;
-    s.load(native, g.N, i);
+    if (rm) {
+        SiteWords<BPS, S> s;
+        s.load(native, g.N, i);
 #pragma unroll
-    for (int k = 0; k < S; k++) {
-        if (BPS == 1) ((uint8_t *)rm)[r * S + k] = (uint8_t)s.slot(k);
-        else ((uint32_t *)rm)[r * S + k] = s.slot(k);
+        for (int k = 0; k < S; k++) {
+            if (BPS == 1) ((uint8_t *)rm)[r * S + k] = (uint8_t)s.slot(k);
+            else ((uint32_t *)rm)[r * S + k] = s.slot(k);
+        }
     }
     if (rm_sites) rm_sites[r] = sites[i];
 }
