@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "lmb.h"
+#include "lmb_lmfile.h"
 
 namespace lmb {
 
@@ -191,6 +192,19 @@ public:
         host_.bytes_per_particle = bytesPerParticle;
     }
 
+    /* Writes the trajectory into a `.lm` file, as the reference's
+     * DataOutputQueue writes it into the simulation file
+     * (core/LocalDataOutputWorker.cpp): this replicate's species counts,
+     * lattice frames (from the device, through the file's writer thread),
+     * site frames and, for the byte lattice, the max counts.  With
+     * writeInputs the parameters, both models and the initial lattice go in
+     * too when the trajectory starts.  The caller closes the file. */
+    void setOutputFile(lmb_lmfile *file, bool writeInputs = true)
+    {
+        out_ = file;
+        outInputs_ = writeInputs;
+    }
+
     /* MpdRdmeSolver::setReactionRate (MpdRdmeSolver.h:85): the new rate is
      * used from the next timestep on. */
     virtual void setReactionRate(unsigned int rxid, float rate)
@@ -220,6 +234,7 @@ public:
         download();
         onBeginTrajectory(host_);
         upload(true);
+        if (out_ && outInputs_) writeInputs();
         double time = 0.0;
         maxParticleCounts_.assign(ns_ + 1, 0);
         maxSiteCounts_.assign(nst_, 0);
@@ -265,7 +280,14 @@ public:
         }
         download();
         onEndTrajectory(host_);
-        if (tracksMaxCounts()) writeMaxCounts(maxParticleCounts_, maxSiteCounts_);
+        if (tracksMaxCounts()) {
+            if (out_)
+                check(lmb_lmfile_write_max_counts(out_, replicate_, maxParticleCounts_.data(),
+                                                  (uint32_t)maxParticleCounts_.size(), maxSiteCounts_.data(),
+                                                  (uint32_t)maxSiteCounts_.size()),
+                      "writeMaxCounts");
+            writeMaxCounts(maxParticleCounts_, maxSiteCounts_);
+        }
     }
 
     uint32_t seed() const { return seed_; }
@@ -349,6 +371,10 @@ private:
         std::vector<uint64_t> c(ns_ + 1);
         check(lmb_lattice_species_counts(lattice_, ns_, c.data()), "recordSpeciesCounts");
         c.erase(c.begin());  // species ids are 1-based
+        if (out_) {
+            std::vector<int32_t> row(c.begin(), c.end());
+            check(lmb_lmfile_append_species_counts(out_, replicate_, 1, ns_, &time, row.data()), "writeSpeciesCounts");
+        }
         writeSpeciesCounts(time, c);
     }
 
@@ -360,6 +386,7 @@ private:
         check(lmb_lattice_species_counts(lattice_, ns_, c.data()), "writeLatticeData");
         for (uint32_t s = 1; s <= ns_; s++)
             if (c[s] > maxParticleCounts_[s]) maxParticleCounts_[s] = (uint32_t)c[s];
+        if (out_) check(lmb_lmfile_append_lattice_device(out_, replicate_, time, lattice_), "writeLatticeData");
         writeLattice(time, host_);
     }
 
@@ -373,6 +400,42 @@ private:
             if (c[t] > maxSiteCounts_[t]) maxSiteCounts_[t] = c[t];
     }
 
+    /* The host site types, [z][y][x], as a [x][y][z] site frame. */
+    void writeSitesToFile(double time)
+    {
+        if (!out_) return;
+        const uint32_t X = host_.X, Y = host_.Y, Z = host_.Z;
+        std::vector<uint8_t> rm((size_t)X * Y * Z);
+        for (uint32_t z = 0; z < Z; z++)
+            for (uint32_t y = 0; y < Y; y++)
+                for (uint32_t x = 0; x < X; x++)
+                    rm[((size_t)x * Y + y) * Z + z] = host_.sites[x + (size_t)X * (y + (size_t)Y * z)];
+        check(lmb_lmfile_append_sites(out_, replicate_, time, X, Y, Z, rm.data()), "writeLatticeSites");
+    }
+
+    /* Parameters, models and the initial lattice (SimulationFile::
+     * setParameter / setReactionModel / setDiffusionModel /
+     * setDiffusionModelLattice). */
+    void writeInputs()
+    {
+        if (parameters_)
+            for (auto &kv : *parameters_)
+                check(lmb_lmfile_set_parameter(out_, kv.first.c_str(), kv.second.c_str()), "setParameter");
+        std::vector<double> k((size_t)nr_ * 10, std::nan(""));
+        for (uint32_t r = 0; r < nr_; r++)
+            for (uint32_t c = 0; c < kcols_ && c < 10; c++) k[(size_t)r * 10 + c] = K_[(size_t)r * kcols_ + c];
+        check(lmb_lmfile_set_reaction_model(out_, ns_, nr_, initial_.data(), rtype_.data(), k.data(), nullptr,
+                                            S_.data(), D_.data()),
+              "setReactionModel");
+        check(lmb_lmfile_set_diffusion_model(out_, ns_, nr_, nst_, spacing_, host_.X, host_.Y, host_.Z, host_.slots,
+                                             host_.bytes_per_particle, DF_.data(), RL_.data()),
+              "setDiffusionModel");
+        std::vector<uint8_t> p((size_t)host_.numberSites() * host_.slots * host_.bytes_per_particle);
+        std::vector<uint8_t> s(host_.numberSites());
+        check(lmb_lattice_get_row_major(lattice_, p.data(), s.data()), "setDiffusionModelLattice");
+        check(lmb_lmfile_set_diffusion_model_lattice(out_, p.data(), s.data()), "setDiffusionModelLattice");
+    }
+
     void hookCheck(double time)
     {
         switch (hookSimulation(time, host_)) {
@@ -381,10 +444,12 @@ private:
         case 2:
             upload(true);
             updateMaxSiteCounts();
+            writeSitesToFile(time);
             writeLatticeSites(time, host_);
             break;
         case 3:
             updateMaxSiteCounts();
+            writeSitesToFile(time);
             writeLatticeSites(time, host_);
             stop_ = true;
             break;
@@ -408,6 +473,8 @@ private:
     lmb_run_stats stats_{};
     bool stop_ = false;
     std::vector<uint32_t> maxParticleCounts_, maxSiteCounts_;
+    lmb_lmfile *out_ = nullptr;
+    bool outInputs_ = false;
 };
 
 /* lm::rdme::IntMpdRdmeSolver: the same solver on an IntLattice. */

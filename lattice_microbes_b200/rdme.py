@@ -200,6 +200,8 @@ class MpdRdmeSolver:
         self.maxParticleCounts = None  # per species id (index 0 unused)
         self.maxSiteCounts = None      # per site type (type 0 not counted)
         self.lastRunStats = None
+        self.output = None            # lmfile.LMFileWriter the trajectory goes to
+        self._write_inputs = False
         self._stop = False
 
     def needsReactionModel(self):
@@ -229,6 +231,7 @@ class MpdRdmeSolver:
         K = np.asarray(K, dtype=np.float64).reshape(-1)
         self._rtype = np.asarray(reactionTypes, dtype=np.uint32).reshape(-1)
         self._K = K[::int(kCols)][:self._nr] if self._nr else np.zeros(0)
+        self._K_rows = K.reshape(-1, int(kCols))[:self._nr] if self._nr else np.zeros((0, 1))
         self._S = np.asarray(S, dtype=np.int32).reshape(-1)
         self._D = np.asarray(D, dtype=np.uint32).reshape(-1)
         self._initial = np.asarray(initialSpeciesCounts, dtype=np.uint32).reshape(-1)
@@ -253,10 +256,40 @@ class MpdRdmeSolver:
         self.lat = Lattice(self.ctx, X, Y, Z, particlesPerSite, bytesPerParticle)
         self.lat.set_row_major(latticeData, latticeSitesData, self._ns, self._nst)
         self.lattice = HostLattice(X, Y, Z, particlesPerSite, bytesPerParticle, float(latticeSpacing))
+        self._DF = spec.DF
+        self._RL = spec.RL
 
     def setReactionRate(self, rxid, rate):
         """MpdRdmeSolver::setReactionRate: used from the next timestep on."""
         self.model.set_reaction_rate(rxid, rate)
+
+    def setOutputFile(self, writer, writeInputs=True):
+        """Writes the trajectory into a `.lm` file (an lmfile.LMFileWriter),
+        as the reference's output queue writes it into the simulation file
+        (core/LocalDataOutputWorker.cpp): this replicate's species counts,
+        lattice frames (from the device, through the writer's thread), site
+        frames and, for the byte lattice, the max counts.  With writeInputs
+        the parameters, both models and the initial lattice go in too when
+        the trajectory starts (what pyLM writes before it runs a solver).
+        The caller closes the writer."""
+        self.output = writer
+        self._write_inputs = bool(writeInputs)
+
+    def _write_inputs_to_file(self):
+        w = self.output
+        for k, v in self.parameters.items():
+            w.set_parameter(k, v)
+        w.set_reaction_model(self._initial, self._rtype, [list(r) for r in self._K_rows],
+                             self._S.reshape(self._ns, self._nr), self._D.reshape(self._ns, self._nr))
+        DF = self._DF.reshape(self._nst, self._nst, self._ns)
+        w.set_diffusion_model(self.lattice.spacing, self.lattice.X, self.lattice.Y, self.lattice.Z, self.lattice.slots,
+                              self.bytes_per_particle, DF, self._RL.reshape(self._nr, self._nst))
+        p, s = self.lat.get_row_major()
+        w.set_diffusion_model_lattice(p, s)
+
+    def _write_sites_to_file(self, time):
+        L = self.lattice
+        self.output.append_sites(self.replicate, time, L.sites.reshape(L.Z, L.Y, L.X).transpose(2, 1, 0))
 
     # ---- callbacks (MpdRdmeSolver.cu:789-822); override in a subclass
     def hookSimulation(self, time, lattice):
@@ -301,6 +334,9 @@ class MpdRdmeSolver:
     def _record_counts(self, time):
         c = self.lat.species_counts(self._ns)
         self.writeSpeciesCounts(time, np.asarray(c[1:], dtype=np.uint64))
+        if self.output is not None:
+            self.output.append_species_counts(self.replicate, [time],
+                                              np.asarray(c[1:], dtype=np.int64).astype(np.int32)[None, :])
 
     def _write_lattice(self, time):
         # writeLatticeData (MpdRdmeSolver.cu:854-883): the particle maxima,
@@ -308,6 +344,8 @@ class MpdRdmeSolver:
         c = np.asarray(self.lat.species_counts(self._ns), dtype=np.uint32)
         c[0] = 0
         np.maximum(self._max_particles, c, out=self._max_particles)
+        if self.output is not None:
+            self.output.append_lattice_device(self.replicate, time, self.lat)
         self.writeLattice(time, self.lattice)
 
     def _update_site_maxima(self):
@@ -324,9 +362,13 @@ class MpdRdmeSolver:
         elif r == 2:
             self._upload(True)
             self._update_site_maxima()
+            if self.output is not None:
+                self._write_sites_to_file(time)
             self.writeLatticeSites(time, self.lattice)
         elif r == 3:
             self._update_site_maxima()
+            if self.output is not None:
+                self._write_sites_to_file(time)
             self.writeLatticeSites(time, self.lattice)
             self._stop = True
         else:
@@ -348,6 +390,8 @@ class MpdRdmeSolver:
         self._download()
         self.onBeginTrajectory(self.lattice)
         self._upload(True)
+        if self.output is not None and self._write_inputs:
+            self._write_inputs_to_file()
         t = 0.0
         self._max_particles = np.zeros(self._ns + 1, dtype=np.uint32)
         self._max_sites = np.zeros(self._nst, dtype=np.uint32)
@@ -378,6 +422,8 @@ class MpdRdmeSolver:
         self._download()
         self.onEndTrajectory(self.lattice)
         if self.tracks_max_counts:
+            if self.output is not None:
+                self.output.write_max_counts(self.replicate, self._max_particles, self._max_sites)
             self.writeMaxCounts(self._max_particles.copy(), self._max_sites.copy())
 
     def close(self):

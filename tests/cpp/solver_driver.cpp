@@ -135,12 +135,19 @@ static int run(const std::string &dir, std::map<std::string, std::string> &p)
     s.buildModel(u("ns"), u("nr"), init.data(), rtype.data(), K.data(), S.data(), D.data(), 1);
     s.buildDiffusionModel(u("nst"), DF.data(), RL.data(), u("X"), u("Y"), u("Z"), u("slots"), u("bytes"),
                           atof(p["spacing"].c_str()), lattice.data(), sites.data(), true);
+    lmb_lmfile *out = nullptr;
+    if (!p["lmfile"].empty()) {
+        if (lmb_lmfile_create(p["lmfile"].c_str(), &out) != LMB_OK) return 4;
+        s.setOutputFile(out, true);
+    }
     try {
         s.generateTrajectory();
     } catch (lmb::Exception &e) {
         std::ofstream(dir + "/error.txt") << e.status() << " " << e.what() << "\n";
+        if (out) lmb_lmfile_close(out);
         return 3;
     }
+    if (out && lmb_lmfile_close(out) != LMB_OK) return 5;
     std::cout << "seed " << s.seed() << "\n";
     return 0;
 }

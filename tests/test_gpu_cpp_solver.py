@@ -126,11 +126,11 @@ def replay(spec, seed, steps, count_every, lattice_every, hook_every, hook):
 
 
 def run_driver(driver, tmp_path, spec, steps, count_every, lattice_every, hook_every, hook, seed_top=9,
-               replicate=3):
+               replicate=3, lmfile=""):
     d = str(tmp_path)
     params = {"seed": seed_top, "replicate": replicate, "maxTime": repr((steps - 0.5) * spec.tau),
               "writeInterval": count_every, "latticeWriteInterval": lattice_every, "hookInterval": hook_every,
-              "hook": hook}
+              "hook": hook, "lmfile": lmfile}
     write_inputs(d, spec, params)
     r = subprocess.run([driver, d], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -147,6 +147,43 @@ def run_driver(driver, tmp_path, spec, steps, count_every, lattice_every, hook_e
         lines = open(os.path.join(d, "max.txt")).read().strip().split("\n")
         maxima = [np.array([int(v) for v in ln.split()]) for ln in lines]
     return counts, frames, final, events, (seed_top << 16) | (replicate & 0xFFFF), maxima
+
+
+def row_major_frame(spec, native):
+    """A native frame as the .lm file holds it: [x][y][z][p]."""
+    slots = configs.native_to_slots(native, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+    dt = np.uint8 if spec.bytes_per_slot == 1 else np.uint32
+    return np.ascontiguousarray(slots.reshape(spec.Z, spec.Y, spec.X, spec.slots).transpose(2, 1, 0, 3), dtype=dt)
+
+
+def check_lmfile(path, spec, replicate, counts, frames, lattice_times, maxima, parameters):
+    """The .lm file a solver wrote holds the records its callbacks saw."""
+    from lattice_microbes_b200.lmfile import LMFile
+    with LMFile(path) as f:
+        assert f.version == 4 and f.replicates() == [replicate]
+        for k, v in parameters.items():
+            assert f.parameters()[k] == str(v)
+        m = f.reaction_model()
+        assert (m["numberSpecies"], m["numberReactions"]) == (spec.ns, spec.nr)
+        assert m["stoichiometricMatrix"] == [int(v) for v in np.asarray(spec.S).ravel()]
+        d = f.diffusion_model()
+        assert (d["latticeXSize"], d["latticeYSize"], d["latticeZSize"]) == (spec.X, spec.Y, spec.Z)
+        assert d["particlesPerSite"] == spec.slots and d["bytes_per_particle"] == spec.bytes_per_slot
+        assert np.array_equal(d["DiffusionMatrix"].ravel(), np.asarray(spec.DF).ravel())
+        assert np.array_equal(d["Lattice"], row_major_frame(spec, spec.lattice))
+        assert np.array_equal(d["LatticeSites"], spec.sites.reshape(spec.Z, spec.Y, spec.X).transpose(2, 1, 0))
+        t, c = f.species_counts(replicate)
+        assert np.array_equal(t, [a for a, _ in counts])
+        assert np.array_equal(c, np.array([b for _, b in counts]))
+        assert np.array_equal(f.lattice_times(replicate), lattice_times)
+        assert len(f.h5["Simulations/%07d/Lattice" % replicate].keys()) == len(frames)
+        for i, fr in enumerate(frames):
+            assert np.array_equal(f.lattice(replicate, i), row_major_frame(spec, fr))
+        got = f.max_counts(replicate)
+        if maxima is None:
+            assert got is None
+        else:
+            assert np.array_equal(got[0], maxima[0]) and np.array_equal(got[1], maxima[1])
 
 
 def expected_maxima(spec, frames):
@@ -170,8 +207,9 @@ def test_generate_trajectory_matches_replay(driver, tmp_path, kind):
     else:
         spec = configs.random_problem(8, X=16, Y=8, Z=8, slots=16, bytes_per_slot=4, density=1.5, nst=2)
     steps, ce, le, he = 301, 50, 100, 70
+    lm = str(tmp_path / "out.lm")
     got_c, got_f, got_final, events, seed, maxima = run_driver(driver, tmp_path, spec, steps, ce, le, he,
-                                                               "clear_left:1")
+                                                               "clear_left:1", lmfile=lm)
     ref_c, ref_f, ref_final = replay(spec, seed, steps, ce, le, he, "clear_left:1")
     assert [t for t, _ in got_c] == pytest.approx([t for t, _ in ref_c], rel=0, abs=0)
     assert len(got_c) == len(ref_c) == 1 + steps // ce
@@ -187,6 +225,9 @@ def test_generate_trajectory_matches_replay(driver, tmp_path, kind):
     else:
         assert maxima is None  # the Int solver writes no maxima
     assert sum(1 for e in events if e.startswith("hook")) == 1 + steps // he
+    # The same records in the .lm file the solver wrote.
+    check_lmfile(lm, spec, 3, got_c, got_f, [i * le * spec.tau for i in range(len(got_f))], maxima,
+                 {"writeInterval": ce, "latticeWriteInterval": le})
     # The hook really changed the trajectory: species 1 is gone from the left half at each hook.
     assert got_c[-1][1][0] < got_c[0][1][0]
 
@@ -194,9 +235,15 @@ def test_generate_trajectory_matches_replay(driver, tmp_path, kind):
 def test_hook_return_3_stops(driver, tmp_path):
     spec = configs.config0(seed=6, edge=16, nA=300, nB=300)
     steps, ce, le, he = 200, 20, 1000, 30
-    got_c, _, got_final, events, seed, _ = run_driver(driver, tmp_path, spec, steps, ce, le, he, "stop_after:3")
+    lm = str(tmp_path / "stop.lm")
+    got_c, _, got_final, events, seed, _ = run_driver(driver, tmp_path, spec, steps, ce, le, he, "stop_after:3",
+                                                      lmfile=lm)
     ref_c, _, ref_final = replay(spec, seed, steps, ce, le, he, "stop_after:3")
     assert np.array_equal(got_final, ref_final)
     assert len(got_c) == len(ref_c) and all(np.array_equal(a[1], b[1]) for a, b in zip(got_c, ref_c))
     assert sum(1 for e in events if e.startswith("sites")) == 1
     assert got_c[-1][0] == pytest.approx(60 * spec.tau, abs=0)
+    from lattice_microbes_b200.lmfile import LMFile
+    with LMFile(lm) as f:  # the hook's return 3 wrote one site frame
+        assert np.array_equal(f.site_times(3), [60 * spec.tau])
+        assert np.array_equal(f.sites(3, 0), spec.sites.reshape(spec.Z, spec.Y, spec.X).transpose(2, 1, 0))

@@ -8,7 +8,7 @@ import pytest
 
 from lattice_microbes_b200 import configs
 from tests import ref_cpu_lib
-from tests.test_gpu_cpp_solver import _row_major_int, clear_left, expected_maxima, replay
+from tests.test_gpu_cpp_solver import _row_major_int, check_lmfile, clear_left, expected_maxima, replay
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +41,7 @@ def _solver(kind, spec, hook, params):
 
 
 @pytest.mark.parametrize("kind", ["byte", "int"])
-def test_python_solver_matches_replay(gpu, kind):
+def test_python_solver_matches_replay(gpu, kind, tmp_path):
     if kind == "byte":
         spec = configs.config0(seed=5, edge=16, nA=600, nB=600)
         spec.K = spec.K * np.array([300.0, 30.0])
@@ -51,7 +51,12 @@ def test_python_solver_matches_replay(gpu, kind):
     params = {"seed": "9", "timestep": repr(spec.tau), "maxTime": repr((steps - 0.5) * spec.tau),
               "writeInterval": str(ce), "latticeWriteInterval": str(le), "hookInterval": str(he)}
     s, cls = _solver(kind, spec, "clear_left:1", params)
+    from lattice_microbes_b200.lmfile import LMFileWriter
+    lm = str(tmp_path / "py.lm")
+    w = LMFileWriter(lm)
+    s.setOutputFile(w)
     s.generateTrajectory()
+    w.close()
     ref_c, ref_f, ref_final = replay(spec, s.seed, steps, ce, le, he, "clear_left:1")
     assert s.seed == (9 << 16) | 3
     assert len(s.speciesCounts) == len(ref_c) == 1 + steps // ce
@@ -67,6 +72,9 @@ def test_python_solver_matches_replay(gpu, kind):
         assert np.array_equal(s.maxParticleCounts, mp) and np.array_equal(s.maxSiteCounts, ms)
     else:
         assert s.maxParticleCounts is None  # the Int solver writes no maxima
+    maxima = None if kind != "byte" else (s.maxParticleCounts, s.maxSiteCounts)
+    check_lmfile(lm, spec, 3, [(t, c.astype(np.int64)) for t, c in s.speciesCounts], [b for _, b, _ in s.latticeFrames],
+                 [t for t, _, _ in s.latticeFrames], maxima, params)
     s.close()
 
 
