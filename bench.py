@@ -8,7 +8,9 @@ of that model's 50,000-timestep trajectory.  Inputs are seeded and synthetic
 (lattice_microbes_b200.configs.config1).  --workload crowded runs the
 128x128x256 IntLattice-16 crowded cell (configs.config2) the same way, 40
 timesteps per bench step; --workload batch / cme / serve run the batched,
-CME-ensemble and serving forms.
+CME-ensemble and serving forms; --workload trajectory runs the rod-cell
+model as a trajectory written to a `.lm` file (species counts and a device
+lattice frame every 100 timesteps through the file's writer thread).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -87,11 +89,13 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
-    ap.add_argument("--workload", choices=["rodcell", "crowded", "batch", "cme", "serve"], default="rodcell",
+    ap.add_argument("--workload", choices=["rodcell", "crowded", "batch", "cme", "serve", "trajectory"],
+                    default="rodcell",
                     help="rodcell: one 64x64x128 lattice (default); crowded: one 128x128x256 IntLattice-16; "
                          "batch: 256 bimolecular replicates of "
                          "uneven size in one launch per timestep; cme: 65,536 two-state gene replicates "
-                         "(direct method) to t = 3600 s; serve: a Poisson stream of solve requests")
+                         "(direct method) to t = 3600 s; serve: a Poisson stream of solve requests; trajectory: "
+                         "the rod cell with its records written to a .lm file")
     ap.add_argument("--replicates", type=int, default=0, help="batch: 256, cme: 65536 (0 = default)")
     ap.add_argument("--requests", type=int, default=48, help="serve: requests of the stream to replay")
     return ap.parse_args()
@@ -914,6 +918,96 @@ def run_serve(a):
     print(json.dumps(line), flush=True)
 
 
+def run_trajectory(a):
+    """The rod-cell model as a trajectory with output: each bench step is 500
+    timesteps in runs of 100, after each run the species counts and a lattice
+    frame go to a `.lm` file (lmb_lmfile_append_lattice_device: GPU transpose,
+    copy to pinned memory, gzip-1 16^3 chunks on the writer thread), and the
+    timed region ends when the file is flushed.  The same loop without the
+    file is timed beside it; both are wall-clock (host calls included)."""
+    import numpy as np
+    import torch
+
+    from lattice_microbes_b200.lmfile import LMFile, LMFileWriter
+    from lattice_microbes_b200.replicas import Ranks
+    from lattice_microbes_b200.solver import Context, Lattice, Model, kernel_launches
+    ranks = Ranks()
+    if ranks.rank != 0:
+        return
+    w = WORKLOADS["rodcell"]
+    spec = make_spec("rodcell", 1)
+    N, T, every = spec.nsites, a.timesteps_per_step or 500, 100
+    ctx = Context(0)
+    model = Model.from_spec(ctx, spec)
+    lat = Lattice(ctx, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+    lat.set_native(spec.lattice, spec.sites)
+    tuned = lat.autotune(model, 7, 0, 100)
+    tmp = tempfile.mkdtemp()
+
+    def loop(writer, first, steps):
+        t = first
+        for _ in range(steps):
+            for _ in range(T // every):
+                lat.run(model, 7, t, every)
+                t += every
+                c = lat.species_counts(spec.ns)
+                if writer is not None:
+                    writer.append_species_counts(0, [t * spec.tau], np.asarray(c[1:], np.int32)[None, :])
+                    writer.append_lattice_device(0, t * spec.tau, lat)
+        if writer is not None:
+            writer.flush()
+        return t
+
+    path = os.path.join(tmp, "traj.lm")
+    wr = LMFileWriter(path)
+    t = loop(wr, 0, a.warmup)
+    clocks = ClockSampler(0)
+    torch.cuda.synchronize()
+    launches0 = kernel_launches()
+    clocks.start()
+    t0 = time.perf_counter()
+    t = loop(wr, t, a.steps)
+    wall = time.perf_counter() - t0
+    clock_info = clocks.stop()
+    launches = kernel_launches() - launches0
+    frames, nbytes = wr.stats()
+    wr.close()
+    with LMFile(path) as f:
+        nframes = len(f.lattice_times(0))
+        last = f.lattice(0, nframes - 1)
+    ref_last = np.asarray(lat.get_row_major()[0])
+    assert np.array_equal(last, ref_last), "last frame in the file differs from the device lattice"
+    size = os.path.getsize(path)
+    os.unlink(path)
+    t1 = time.perf_counter()
+    loop(None, t, a.steps)
+    wall_plain = time.perf_counter() - t1
+    rate = N * T * a.steps / wall
+    fr = a.steps * T // every
+    raw = N * spec.slots * spec.bytes_per_slot
+    line = {
+        "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": wall / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": w["dtype"], "data": "synthetic (seeded, lattice_microbes_b200.configs.config1)",
+        "config": {"workload": "rod-cell trajectory to a .lm file: " + w["desc"], "timesteps_per_step": T,
+                   "frame_every": every, "sites": N, "parallelism": "single", "schedule": "fused Ty=%d Tz=%d" % (tuned[1], tuned[2]) if tuned[0] == 0 else "phases",
+                   "timing": "wall clock, host calls and the file flush included"},
+        "output": {"frames": fr, "frames_per_s": fr / wall, "raw_bytes_per_frame": raw,
+                   "gzip_bytes_per_frame": nbytes / max(frames, 1), "file_bytes": size,
+                   "raw_GB_per_s": fr * raw / wall / 1e9},
+        "without_output": {"value": N * T * a.steps / wall_plain, "unit": METRIC,
+                           "ms_per_step": wall_plain / a.steps * 1e3},
+        "output_cost_frac": 1.0 - wall_plain / wall,
+        "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": (T // every) * (raw + 8 * (spec.ns + 1))},
+        "gpu_launches": launches, "clocks": clock_info,
+    }
+    lat.close()
+    model.close()
+    ctx.close()
+    print(json.dumps(line))
+
+
 def _to_byte16(spec):
     """The request's particles in a 16-slot ByteLattice (the serving layout)."""
     import numpy as np
@@ -937,5 +1031,7 @@ if __name__ == "__main__":
         run_cme(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "trajectory":
+        run_trajectory(args)
     else:
         run_ours(args)

@@ -112,6 +112,33 @@ int lmb_lmfile_append_sites_device(lmb_lmfile *f, uint32_t replicate, double tim
 int lmb_lmfile_write_max_counts(lmb_lmfile *f, uint32_t replicate, const uint32_t *max_particle_counts,
                                 uint32_t n_particle, const uint32_t *max_site_counts, uint32_t n_site);
 
+/* Element types of the generic calls below. */
+#define LMB_H5_U8 1
+#define LMB_H5_I8 2
+#define LMB_H5_U16 3
+#define LMB_H5_I16 4
+#define LMB_H5_U32 5
+#define LMB_H5_I32 6
+#define LMB_H5_U64 7
+#define LMB_H5_I64 8
+#define LMB_H5_F32 9
+#define LMB_H5_F64 10
+#define LMB_H5_STRING 11 /* fixed-size, null-terminated ASCII */
+
+/* Generic objects, for carrying an existing file's contents into a new one
+ * (the runSolver path): a group (with its parents), an attribute on a group
+ * or dataset (string_size: bytes per string including the terminator, for
+ * LMB_H5_STRING; rank 0 is a scalar), and a dataset written now, contiguous
+ * (chunk_dims NULL) or chunked (gzip_level -1 for none).  An extendable
+ * dataset (first dimension unlimited; chunked) keeps its rows in memory so
+ * that later appends (species counts, frame times) extend it. */
+int lmb_lmfile_create_group(lmb_lmfile *f, const char *path);
+int lmb_lmfile_set_attribute(lmb_lmfile *f, const char *path, const char *name, int type, uint32_t rank,
+                             const uint64_t *dims, const void *data, uint32_t string_size);
+int lmb_lmfile_write_dataset(lmb_lmfile *f, const char *group, const char *name, int type, uint32_t rank,
+                             const uint64_t *dims, const uint64_t *chunk_dims, int gzip_level, int extendable,
+                             const void *data);
+
 /* Waits for the writer thread and writes the metadata: the file on disk is a
  * complete `.lm` file afterwards (the reference's checkpoint point,
  * SimulationFile.cpp:158-190). */

@@ -169,6 +169,10 @@ PROTOTYPES = {
     "lmb_lmfile_append_sites": (C.c_int, [vp, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32, u8p]),
     "lmb_lmfile_append_sites_device": (C.c_int, [vp, C.c_uint32, C.c_double, vp]),
     "lmb_lmfile_write_max_counts": (C.c_int, [vp, C.c_uint32, u32p, C.c_uint32, u32p, C.c_uint32]),
+    "lmb_lmfile_create_group": (C.c_int, [vp, C.c_char_p]),
+    "lmb_lmfile_set_attribute": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_uint32, u64p, vp, C.c_uint32]),
+    "lmb_lmfile_write_dataset": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_uint32, u64p, u64p, C.c_int,
+                                           C.c_int, vp]),
     "lmb_lmfile_flush": (C.c_int, [vp]),
     "lmb_lmfile_stats": (C.c_int, [vp, u64p, u64p]),
     "lmb_lmfile_close": (C.c_int, [vp]),

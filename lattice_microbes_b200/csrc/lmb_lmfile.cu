@@ -20,7 +20,9 @@
 
 #include <cuda_runtime.h>
 #include <fcntl.h>
+#include <sys/resource.h>
 #include <sys/stat.h>
+#include <sys/syscall.h>
 #include <unistd.h>
 #include <zlib.h>
 
@@ -31,6 +33,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -50,7 +53,7 @@ constexpr uint64_t FRAME_CHUNK = 16;     // TUNE_LATTICE_GZIP_CHUNK_SIZE (src/cm
 constexpr int FRAME_GZIP = 1;            // TUNE_LATTICE_GZIP_COMPRESSION_LEVEL (options.cmake:85)
 constexpr uint64_t ROW_CHUNK = 100;      // chunk rows of the extendable datasets (SimulationFile.cpp:2194)
 constexpr uint32_t FORMAT_VERSION = 4;   // SimulationFile::CURRENT_VERSION (SimulationFile.cpp:77)
-constexpr int PINNED_SLOTS = 2;          // device frames in flight to the writer thread
+constexpr int PINNED_SLOTS = 3;          // device frames in flight to the writer thread
 
 struct Bytes {
     std::vector<uint8_t> v;
@@ -77,19 +80,27 @@ struct Bytes {
     size_t size() const { return v.size(); }
 };
 
-enum class Type { U8, U32, I32, F64, STR };
+enum class Type { U8, I8, U16, I16, U32, I32, U64, I64, F32, F64, STR };
 
 uint32_t type_size(Type t, uint32_t strsize)
 {
     switch (t) {
-    case Type::U8: return 1;
+    case Type::U8:
+    case Type::I8: return 1;
+    case Type::U16:
+    case Type::I16: return 2;
     case Type::U32:
-    case Type::I32: return 4;
+    case Type::I32:
+    case Type::F32: return 4;
+    case Type::U64:
+    case Type::I64:
     case Type::F64: return 8;
     case Type::STR: return strsize;
     }
     return 0;
 }
+
+bool is_signed(Type t) { return t == Type::I8 || t == Type::I16 || t == Type::I32 || t == Type::I64; }
 
 // Datatype message, version 1: little-endian fixed point (signed bit for
 // I32), IEEE double, or a null-terminated ASCII string of fixed size.
@@ -98,11 +109,16 @@ Bytes datatype(Type t, uint32_t strsize = 0)
     Bytes b;
     switch (t) {
     case Type::U8:
+    case Type::I8:
+    case Type::U16:
+    case Type::I16:
     case Type::U32:
-    case Type::I32: {
+    case Type::I32:
+    case Type::U64:
+    case Type::I64: {
         const uint32_t n = type_size(t, 0);
         b.u8(0x10);
-        b.u8(t == Type::I32 ? 0x08 : 0x00);
+        b.u8(is_signed(t) ? 0x08 : 0x00);
         b.u8(0);
         b.u8(0);
         b.u32(n);
@@ -110,6 +126,20 @@ Bytes datatype(Type t, uint32_t strsize = 0)
         b.u16(8 * n);
         break;
     }
+    case Type::F32:
+        b.u8(0x11);
+        b.u8(0x20);
+        b.u8(31);
+        b.u8(0);
+        b.u32(4);
+        b.u16(0);
+        b.u16(32);
+        b.u8(23);
+        b.u8(8);
+        b.u8(0);
+        b.u8(23);
+        b.u32(127);
+        break;
     case Type::F64:
         b.u8(0x11);
         b.u8(0x20);  // mantissa normalisation: implied leading bit
@@ -199,24 +229,33 @@ struct Node {
     uint64_t addr = UNDEF, bytes = 0; // contiguous data
     std::vector<Chunk> chunks;
     // Written by the last flush; a group's B-tree and heap go into its
-    // parent's symbol-table entry.
+    // parent's symbol-table entry.  A dataset whose header is written and
+    // that has not changed since (every frame, once stored) keeps it.
     uint64_t header = UNDEF, btree = UNDEF, heap = UNDEF;
+    bool dirty = true;
 };
 
+// A frame for the writer thread: a host row-major copy (host calls), or a
+// pinned copy of the device lattice in its native layout (device calls:
+// slot k of site i = x + y X + z X Y is byte ((k / 4) N + i) * 4 + k % 4 of
+// a ByteLattice, word k N + i of an IntLattice; site types one byte per
+// site), which the writer reads into [x][y][z][p] chunks itself.
 struct FrameJob {
     std::string group, name;          // dataset path
     Type type;
-    std::vector<uint64_t> dims;
+    std::vector<uint64_t> dims;       // [X, Y, Z(, P)]
     std::vector<uint8_t> host;        // host copy (host calls)
     int slot = -1;                    // pinned slot (device calls)
+    uint32_t bytes_per_slot = 0;      // native layout of a device lattice frame (0: site types)
 };
 
 struct Pinned {
     void *host = nullptr;
-    void *dev = nullptr;
+    void *dev = nullptr;              // device snapshot of the frame
     size_t bytes = 0;
     bool busy = false;
-    cudaEvent_t ready = nullptr;
+    cudaEvent_t staged = nullptr;     // snapshot taken (lattice stream)
+    cudaEvent_t ready = nullptr;      // host copy done (copy stream)
 };
 
 std::string num(uint32_t v, int width)
@@ -226,12 +265,92 @@ std::string num(uint32_t v, int width)
     return b;
 }
 
+// The writer's threads run at a lower priority (nice +10) than the thread
+// that drives the GPU, so that its wake-ups for the next launch are not
+// delayed behind compression.
+void lower_priority() { setpriority(PRIO_PROCESS, (id_t)syscall(SYS_gettid), 10); }
+
+// Persistent threads for the chunk work of a frame; the calling thread
+// works too.  One parallel loop at a time.
+class Pool {
+public:
+    explicit Pool(unsigned helpers)
+    {
+        for (unsigned i = 0; i < helpers; i++) th_.emplace_back([this] { loop(); });
+    }
+    ~Pool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    // Calls fn(i) for i in [0, n) on all threads; returns when every call did.
+    void run(size_t n, const std::function<void(size_t)> &fn)
+    {
+        std::lock_guard<std::mutex> one(run_);
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            fn_ = &fn;
+            n_ = n;
+            next_ = 0;
+            pending_ = th_.size();
+            gen_++;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+        fn_ = nullptr;
+    }
+
+private:
+    void work()
+    {
+        for (;;) {
+            const size_t i = next_++;
+            if (i >= n_) break;
+            (*fn_)(i);
+        }
+    }
+    void loop()
+    {
+        lower_priority();
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            seen = gen_;
+            lk.unlock();
+            work();
+            lk.lock();
+            if (--pending_ == 0) done_.notify_all();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex m_, run_;
+    std::condition_variable cv_, done_;
+    const std::function<void(size_t)> *fn_ = nullptr;
+    size_t n_ = 0;
+    std::atomic<size_t> next_{0};
+    size_t pending_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
 }  // namespace
 
 struct lmb_lmfile {
     int fd = -1;
     uint64_t eof = SUPERBLOCK;  // relative to the superblock
     Node root;
+    // During a flush the metadata is gathered here and written at once.
+    bool buffering = false;
+    uint64_t pending_at = 0;
+    std::vector<uint8_t> pending;
     std::mutex mu;  // tree and file
     int io_error = LMB_OK;
     // Model sizes (loadModel): species for new replicates, the lattice for
@@ -247,9 +366,10 @@ struct lmb_lmfile {
     int error = LMB_OK;
     std::thread writer;
     int device = -1;
+    cudaStream_t copy = nullptr;  // device-to-host copies of frames
     Pinned pinned[PINNED_SLOTS];
     uint64_t frames = 0, chunk_bytes = 0;
-    unsigned threads = 1;
+    std::unique_ptr<Pool> pool;
 };
 
 namespace {
@@ -277,7 +397,12 @@ bool put(lmb_lmfile *f, uint64_t rel, const void *p, size_t n)
 uint64_t append(lmb_lmfile *f, const void *p, size_t n)
 {
     const uint64_t a = f->eof;
-    put(f, a, p, n);
+    if (f->buffering) {
+        const uint8_t *b = (const uint8_t *)p;
+        f->pending.insert(f->pending.end(), b, b + n);
+    } else {
+        put(f, a, p, n);
+    }
     f->eof += n;
     return a;
 }
@@ -351,8 +476,9 @@ void contiguous(lmb_lmfile *f, Node &g, const std::string &name, Type t, std::ve
     g.children[name] = std::move(d);
 }
 
-// An extendable dataset of rows (first dimension unlimited), 100-row chunks.
-Node *extendable(Node &g, const std::string &name, Type t, std::vector<uint64_t> dims)
+// An extendable dataset of rows (first dimension unlimited), `rows`-row
+// chunks (100 for the reference's own).
+Node *extendable_node(Node &g, const std::string &name, Type t, std::vector<uint64_t> dims, uint64_t rows)
 {
     auto &c = g.children[name];
     if (!c) {
@@ -362,9 +488,14 @@ Node *extendable(Node &g, const std::string &name, Type t, std::vector<uint64_t>
         c->dims = std::move(dims);
         c->extendable = true;
         c->chunk_dims = c->dims;
-        c->chunk_dims[0] = ROW_CHUNK;
+        c->chunk_dims[0] = rows;
     }
     return c.get();
+}
+
+Node *extendable(Node &g, const std::string &name, Type t, std::vector<uint64_t> dims)
+{
+    return extendable_node(g, name, t, std::move(dims), ROW_CHUNK);
 }
 
 void add_rows(Node &d, const void *p, uint64_t rows)
@@ -379,10 +510,22 @@ void add_rows(Node &d, const void *p, uint64_t rows)
 // ---- chunks ----------------------------------------------------------------
 
 // Copies the chunk at `origin` of a row-major array into `dst` (zeroed,
-// chunk-shaped); runs along the last dimension are contiguous on both sides.
-void gather_chunk(const uint8_t *src, const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd,
-                  const std::vector<uint64_t> &origin, size_t esize, uint8_t *dst)
+// chunk-shaped).  Trailing dimensions that the chunk spans whole are merged
+// with the one before them, so each copied run is as long as both layouts
+// allow (a lattice frame's z column with all its slots, for instance).
+void gather_chunk(const uint8_t *src, const std::vector<uint64_t> &dims0, const std::vector<uint64_t> &cd0,
+                  const std::vector<uint64_t> &origin0, size_t esize, uint8_t *dst)
 {
+    std::vector<uint64_t> dims = dims0, cd = cd0, origin = origin0;
+    while (dims.size() > 1 && cd.back() == dims.back() && origin.back() == 0) {
+        const uint64_t n = dims.back();
+        dims.pop_back();
+        cd.pop_back();
+        origin.pop_back();
+        dims.back() *= n;
+        cd.back() *= n;
+        origin.back() *= n;
+    }
     const size_t r = dims.size();
     std::vector<uint64_t> ss(r), ds(r), ext(r), idx(r, 0);
     ss[r - 1] = ds[r - 1] = 1;
@@ -412,8 +555,42 @@ void gather_chunk(const uint8_t *src, const std::vector<uint64_t> &dims, const s
 // Splits a row-major array into chunks (in lexicographic chunk order, the
 // order the chunk B-tree keeps), gzipped when level >= 0, on `threads`
 // threads.  Returns false when zlib fails.
-bool make_chunks(const uint8_t *data, const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd,
-                 size_t esize, int level, unsigned threads, std::vector<std::vector<uint8_t>> &out,
+using Gather = std::function<void(const std::vector<uint64_t> &origin, uint8_t *dst)>;
+
+// zlib's compress2 with a stream kept per thread: deflateInit's defaults
+// (zlib format, 32 KB window, memory level 8, default strategy) give the
+// same bytes, without allocating and clearing the stream for every chunk.
+struct Deflater {
+    z_stream s{};
+    int level = -1;
+    ~Deflater()
+    {
+        if (level >= 0) deflateEnd(&s);
+    }
+    bool run(const uint8_t *in, size_t n, int lvl, std::vector<uint8_t> &out)
+    {
+        if (level != lvl) {
+            if (level >= 0) deflateEnd(&s);
+            s = z_stream{};
+            level = -1;
+            if (deflateInit(&s, lvl) != Z_OK) return false;
+            level = lvl;
+        } else if (deflateReset(&s) != Z_OK) {
+            return false;
+        }
+        out.resize(deflateBound(&s, n));
+        s.next_in = const_cast<Bytef *>(in);
+        s.avail_in = (uInt)n;
+        s.next_out = out.data();
+        s.avail_out = (uInt)out.size();
+        if (deflate(&s, Z_FINISH) != Z_STREAM_END) return false;
+        out.resize(out.size() - s.avail_out);
+        return true;
+    }
+};
+
+bool make_chunks(const Gather &gather, const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd,
+                 size_t esize, int level, Pool &pool, std::vector<std::vector<uint8_t>> &out,
                  std::vector<std::vector<uint64_t>> &origins)
 {
     const size_t r = dims.size();
@@ -435,36 +612,18 @@ bool make_chunks(const uint8_t *data, const std::vector<uint64_t> &dims, const s
         }
     }
     const size_t cbytes = celems * esize;
-    std::atomic<size_t> next{0};
     std::atomic<bool> ok{true};
-    auto work = [&]() {
-        std::vector<uint8_t> raw(cbytes);
-        for (;;) {
-            const size_t c = next++;
-            if (c >= nch) break;
-            std::fill(raw.begin(), raw.end(), 0);
-            gather_chunk(data, dims, cd, origins[c], esize, raw.data());
-            if (level < 0) {
-                out[c] = raw;
-                continue;
-            }
-            uLongf len = compressBound(cbytes);
-            out[c].resize(len);
-            if (compress2(out[c].data(), &len, raw.data(), cbytes, level) != Z_OK) {
-                ok = false;
-                break;
-            }
-            out[c].resize(len);
+    pool.run(nch, [&](size_t c) {
+        thread_local std::vector<uint8_t> raw;
+        raw.assign(cbytes, 0);
+        gather(origins[c], raw.data());
+        if (level < 0) {
+            out[c] = raw;
+            return;
         }
-    };
-    const unsigned t = (unsigned)std::min<size_t>(threads, nch);
-    if (t <= 1) {
-        work();
-    } else {
-        std::vector<std::thread> pool;
-        for (unsigned i = 0; i < t; i++) pool.emplace_back(work);
-        for (auto &th : pool) th.join();
-    }
+        thread_local Deflater z;
+        if (!z.run(raw.data(), cbytes, level, out[c])) ok = false;
+    });
     return ok;
 }
 
@@ -472,11 +631,11 @@ bool make_chunks(const uint8_t *data, const std::vector<uint64_t> &dims, const s
 // friends): chunks are compressed outside the file lock, then appended.
 int chunked_dataset(lmb_lmfile *f, const std::string &group, const std::string &name, Type t,
                     const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd, int level,
-                    const uint8_t *data)
+                    const Gather &gather)
 {
     std::vector<std::vector<uint8_t>> out;
     std::vector<std::vector<uint64_t>> origins;
-    if (!make_chunks(data, dims, cd, type_size(t, 0), level, f->threads, out, origins)) return LMB_E_IO;
+    if (!make_chunks(gather, dims, cd, type_size(t, 0), level, *f->pool, out, origins)) return LMB_E_IO;
     std::lock_guard<std::mutex> lk(f->mu);
     std::unique_ptr<Node> d(new Node());
     d->group = false;
@@ -484,9 +643,13 @@ int chunked_dataset(lmb_lmfile *f, const std::string &group, const std::string &
     d->dims = dims;
     d->chunk_dims = cd;
     d->gzip = level;
+    // The chunks back to back, in one write.
+    std::vector<uint8_t> all;
+    for (auto &o : out) all.insert(all.end(), o.begin(), o.end());
+    const uint64_t base = append(f, all.data(), all.size());
     uint64_t total = 0;
     for (size_t c = 0; c < out.size(); c++) {
-        d->chunks.push_back({origins[c], append(f, out[c].data(), out[c].size()), (uint32_t)out[c].size()});
+        d->chunks.push_back({origins[c], base + total, (uint32_t)out[c].size()});
         total += out[c].size();
     }
     Node *g = group_at(f->root, group);
@@ -494,6 +657,45 @@ int chunked_dataset(lmb_lmfile *f, const std::string &group, const std::string &
     g->children[name] = std::move(d);
     f->chunk_bytes += total;
     return f->io_error;
+}
+
+int chunked_dataset(lmb_lmfile *f, const std::string &group, const std::string &name, Type t,
+                    const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd, int level,
+                    const uint8_t *row_major)
+{
+    const size_t esize = type_size(t, 0);
+    return chunked_dataset(f, group, name, t, dims, cd, level,
+                           [&](const std::vector<uint64_t> &o, uint8_t *dst) {
+                               gather_chunk(row_major, dims, cd, o, esize, dst);
+                           });
+}
+
+// The chunk at `o` of a [X][Y][Z]([P]) frame read from a device lattice's
+// native layout (FrameJob).
+void gather_native(const uint8_t *src, const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd,
+                   const std::vector<uint64_t> &o, uint32_t bps, uint8_t *dst)
+{
+    const uint64_t X = dims[0], Y = dims[1], Z = dims[2], N = X * Y * Z;
+    const uint64_t P = dims.size() > 3 ? dims[3] : 1, es = bps ? bps : 1;
+    const uint64_t ex = std::min(cd[0], X - o[0]), ey = std::min(cd[1], Y - o[1]), ez = std::min(cd[2], Z - o[2]);
+    const uint64_t xstride = cd[1] * cd[2] * P * es;  // dst bytes between x neighbours
+    // x innermost: the source sites are consecutive.
+    for (uint64_t zz = 0; zz < ez; zz++)
+        for (uint64_t yy = 0; yy < ey; yy++) {
+            const uint64_t i0 = o[0] + X * ((o[1] + yy) + Y * (o[2] + zz));
+            uint8_t *d = dst + (yy * cd[2] + zz) * P * es;
+            if (bps == 0) {
+                for (uint64_t xx = 0; xx < ex; xx++) d[xx * xstride] = src[i0 + xx];
+            } else if (bps == 1) {
+                const uint32_t *w = (const uint32_t *)src;
+                for (uint64_t xx = 0; xx < ex; xx++)
+                    for (uint64_t k = 0; k < P; k += 4) memcpy(d + xx * xstride + k, &w[(k >> 2) * N + i0 + xx], 4);
+            } else {
+                const uint32_t *w = (const uint32_t *)src;
+                for (uint64_t xx = 0; xx < ex; xx++)
+                    for (uint64_t k = 0; k < P; k++) memcpy(d + xx * xstride + 4 * k, &w[k * N + i0 + xx], 4);
+            }
+        }
 }
 
 // ---- metadata --------------------------------------------------------------
@@ -654,16 +856,22 @@ void write_group(lmb_lmfile *f, Node &g)
 
 void write_dataset(lmb_lmfile *f, Node &d)
 {
+    if (!d.dirty && !d.extendable && d.header != UNDEF) return;
+    d.dirty = false;
     const size_t esize = type_size(d.type, 0);
     if (d.extendable) {
         // The rows, in 100-row chunks (the last one zero-filled), uncompressed.
         size_t row = esize;
         for (size_t i = 1; i < d.dims.size(); i++) row *= d.dims[i];
+        // (Chunks span whole rows: a copied dataset chunked across its
+        // other dimensions is stored with full-width chunks.)
+        for (size_t i = 1; i < d.dims.size(); i++) d.chunk_dims[i] = std::max<uint64_t>(1, d.dims[i]);
+        const uint64_t per = d.chunk_dims[0];
         d.chunks.clear();
-        std::vector<uint8_t> buf(ROW_CHUNK * row);
-        for (uint64_t r0 = 0; r0 < d.dims[0]; r0 += ROW_CHUNK) {
+        std::vector<uint8_t> buf(per * row);
+        for (uint64_t r0 = 0; r0 < d.dims[0]; r0 += per) {
             std::fill(buf.begin(), buf.end(), 0);
-            const uint64_t n = std::min<uint64_t>(ROW_CHUNK, d.dims[0] - r0);
+            const uint64_t n = std::min<uint64_t>(per, d.dims[0] - r0);
             memcpy(buf.data(), d.rows.data() + r0 * row, n * row);
             std::vector<uint64_t> off(d.dims.size(), 0);
             off[0] = r0;
@@ -740,7 +948,14 @@ void write_node(lmb_lmfile *f, Node &n)
 // Writes the metadata and points the superblock at it (caller holds mu).
 int commit(lmb_lmfile *f)
 {
+    f->buffering = true;
+    f->pending.clear();
+    f->pending_at = f->eof;
     write_node(f, f->root);
+    f->buffering = false;
+    if (!f->pending.empty()) put(f, f->pending_at, f->pending.data(), f->pending.size());
+    f->pending.clear();
+    f->pending.shrink_to_fit();
     Bytes sb;
     sb.raw("\x89HDF\r\n\x1a\n", 8);
     sb.u8(0);  // superblock version
@@ -796,6 +1011,7 @@ uint32_t next_frame(lmb_lmfile *f, uint32_t rep, const char *group, const char *
 
 void writer_main(lmb_lmfile *f)
 {
+    lower_priority();
     for (;;) {
         FrameJob j;
         {
@@ -815,7 +1031,15 @@ void writer_main(lmb_lmfile *f)
         if (rc == LMB_OK) {
             std::vector<uint64_t> cd(j.dims.size());
             for (size_t i = 0; i < cd.size(); i++) cd[i] = i < 3 ? std::min(FRAME_CHUNK, j.dims[i]) : j.dims[i];
-            rc = chunked_dataset(f, j.group, j.name, j.type, j.dims, cd, FRAME_GZIP, data);
+            if (j.slot >= 0) {
+                const uint32_t bps = j.bytes_per_slot;
+                rc = chunked_dataset(f, j.group, j.name, j.type, j.dims, cd, FRAME_GZIP,
+                                     [&](const std::vector<uint64_t> &o, uint8_t *dst) {
+                                         gather_native(data, j.dims, cd, o, bps, dst);
+                                     });
+            } else {
+                rc = chunked_dataset(f, j.group, j.name, j.type, j.dims, cd, FRAME_GZIP, data);
+            }
         }
         if (rc == LMB_OK) {
             std::lock_guard<std::mutex> lk(f->mu);
@@ -880,6 +1104,8 @@ int take_slot(lmb_lmfile *f, size_t bytes, int *slot)
         }
         if (!p.ready && cudaEventCreateWithFlags(&p.ready, cudaEventDisableTiming) != cudaSuccess)
             return LMB_E_CUDA;
+        if (!p.staged && cudaEventCreateWithFlags(&p.staged, cudaEventDisableTiming) != cudaSuccess)
+            return LMB_E_CUDA;
         p.busy = true;
         *slot = s;
         return LMB_OK;
@@ -899,16 +1125,21 @@ int append_device(lmb_lmfile *f, uint32_t rep, double time, lmb_lattice *lat, bo
     if (cudaSetDevice(f->device) != cudaSuccess) return LMB_E_CUDA;
     const size_t N = v.g.N, esize = v.bytes_per_slot;
     const size_t bytes = sites ? N : N * v.slots * esize;
+    if (!f->copy && cudaStreamCreateWithFlags(&f->copy, cudaStreamNonBlocking) != cudaSuccess) return LMB_E_CUDA;
     int s = -1;
     rc = take_slot(f, bytes, &s);
     if (rc != LMB_OK) return rc;
     Pinned &p = f->pinned[s];
+    // A device snapshot in the lattice's stream order (the lattice may be
+    // advanced right after), then the copy to pinned memory on the file's
+    // own stream, overlapping the next timesteps.
     cudaStream_t st = v.ctx->stream;
-    cudaError_t e = lmb::launch_native_to_row_major((int)v.bytes_per_slot, (int)v.slots, v.particles, v.sites,
-                                                    sites ? nullptr : p.dev,
-                                                    sites ? (uint8_t *)p.dev : nullptr, v.g, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(p.host, p.dev, bytes, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaEventRecord(p.ready, st);
+    cudaError_t e = cudaMemcpyAsync(p.dev, sites ? (const void *)v.sites : (const void *)v.particles, bytes,
+                                    cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(p.staged, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(f->copy, p.staged, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p.host, p.dev, bytes, cudaMemcpyDeviceToHost, f->copy);
+    if (e == cudaSuccess) e = cudaEventRecord(p.ready, f->copy);
     if (e != cudaSuccess) {
         std::lock_guard<std::mutex> lk(f->qmu);
         p.busy = false;
@@ -916,6 +1147,7 @@ int append_device(lmb_lmfile *f, uint32_t rep, double time, lmb_lattice *lat, bo
     }
     FrameJob j;
     j.slot = s;
+    j.bytes_per_slot = sites ? 0 : v.bytes_per_slot;
     {
         std::lock_guard<std::mutex> lk(f->mu);
         const char *grp = sites ? "Sites" : "Lattice";
@@ -946,7 +1178,10 @@ extern "C" int lmb_lmfile_create(const char *path, lmb_lmfile **out)
     if (fd < 0) return LMB_E_IO;
     lmb_lmfile *f = new lmb_lmfile();
     f->fd = fd;
-    f->threads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    // Chunk compression threads: up to 16, leaving two host cores to the
+    // thread that drives the GPU.
+    const unsigned hw = std::thread::hardware_concurrency();
+    f->pool.reset(new Pool(std::max(1u, std::min(16u, hw > 2 ? hw - 2 : 1u)) - 1));
     // The user block: "LMH5" and zeros (SimulationFile_create.cpp:119-128).
     const uint8_t ub[USER_BLOCK] = {'L', 'M', 'H', '5'};
     if (pwrite(fd, ub, sizeof(ub), 0) != (ssize_t)sizeof(ub)) f->io_error = LMB_E_IO;
@@ -1131,6 +1366,92 @@ extern "C" int lmb_lmfile_write_max_counts(lmb_lmfile *f, uint32_t rep, const ui
                            {std::min<uint64_t>(FRAME_CHUNK, nsites)}, FRAME_GZIP, (const uint8_t *)ms);
 }
 
+static bool type_of(int code, Type *t)
+{
+    static const Type map[] = {Type::U8,  Type::I8,  Type::U16, Type::I16, Type::U32, Type::I32,
+                               Type::U64, Type::I64, Type::F32, Type::F64, Type::STR};
+    if (code < LMB_H5_U8 || code > LMB_H5_STRING) return false;
+    *t = map[code - LMB_H5_U8];
+    return true;
+}
+
+extern "C" int lmb_lmfile_create_group(lmb_lmfile *f, const char *path)
+{
+    if (!f || !path) return LMB_E_ARG;
+    std::lock_guard<std::mutex> lk(f->mu);
+    return group_at(f->root, path) ? f->io_error : LMB_E_STATE;
+}
+
+extern "C" int lmb_lmfile_set_attribute(lmb_lmfile *f, const char *path, const char *name, int type, uint32_t rank,
+                                        const uint64_t *dims, const void *data, uint32_t string_size)
+{
+    Type t;
+    if (!f || !path || !name || !*name || !type_of(type, &t) || (rank && !dims) || rank > 32 ||
+        (t == Type::STR && !string_size))
+        return LMB_E_ARG;
+    Attr a{name, t, t == Type::STR ? string_size : 0, std::vector<uint64_t>(dims, dims + rank), {}};
+    size_t n = type_size(t, string_size);
+    for (uint32_t i = 0; i < rank; i++) n *= dims[i];
+    if (n && !data) return LMB_E_ARG;
+    const uint8_t *b = (const uint8_t *)data;
+    a.data.assign(b, b + n);
+    std::lock_guard<std::mutex> lk(f->mu);
+    // The object: a group (made if missing) or an existing dataset.
+    const std::string p = path;
+    const size_t slash = p.find_last_of('/');
+    Node *parent = slash == std::string::npos ? &f->root : group_at(f->root, p.substr(0, slash));
+    const std::string leaf = slash == std::string::npos ? p : p.substr(slash + 1);
+    if (!parent) return LMB_E_STATE;
+    Node *n0 = parent;
+    if (!leaf.empty()) {
+        auto it = parent->children.find(leaf);
+        n0 = it != parent->children.end() && !it->second->group ? it->second.get() : group_at(*parent, leaf);
+    }
+    if (!n0) return LMB_E_STATE;
+    set_attr(*n0, std::move(a));
+    n0->dirty = true;
+    return f->io_error;
+}
+
+extern "C" int lmb_lmfile_write_dataset(lmb_lmfile *f, const char *group, const char *name, int type, uint32_t rank,
+                                        const uint64_t *dims, const uint64_t *chunk_dims, int gzip, int extendable,
+                                        const void *data)
+{
+    Type t;
+    if (!f || !group || !name || !*name || !type_of(type, &t) || t == Type::STR || !rank || !dims || rank > 32 ||
+        gzip > 9 || (extendable && !chunk_dims))
+        return LMB_E_ARG;
+    const std::vector<uint64_t> d(dims, dims + rank);
+    size_t n = type_size(t, 0);
+    for (uint64_t x : d) n *= x;
+    if (n && !data) return LMB_E_ARG;
+    if (chunk_dims) {
+        for (uint32_t i = 0; i < rank; i++)
+            if (!chunk_dims[i] || (!(extendable && i == 0) && chunk_dims[i] > dims[i])) return LMB_E_ARG;
+    }
+    if (extendable) {
+        std::lock_guard<std::mutex> lk(f->mu);
+        Node *g = group_at(f->root, group);
+        if (!g) return LMB_E_STATE;
+        g->children.erase(name);
+        std::vector<uint64_t> d0 = d;
+        d0[0] = 0;
+        Node *x = extendable_node(*g, name, t, d0, chunk_dims[0]);
+        add_rows(*x, data, d[0]);
+        x->chunk_dims.assign(chunk_dims, chunk_dims + rank);
+        return f->io_error;
+    }
+    if (!chunk_dims || n == 0) {
+        std::lock_guard<std::mutex> lk(f->mu);
+        Node *g = group_at(f->root, group);
+        if (!g) return LMB_E_STATE;
+        contiguous(f, *g, name, t, d, data);
+        return f->io_error;
+    }
+    return chunked_dataset(f, group, name, t, d, std::vector<uint64_t>(chunk_dims, chunk_dims + rank), gzip,
+                           (const uint8_t *)data);
+}
+
 extern "C" int lmb_lmfile_flush(lmb_lmfile *f)
 {
     if (!f) return LMB_E_ARG;
@@ -1164,7 +1485,9 @@ extern "C" int lmb_lmfile_close(lmb_lmfile *f)
         if (p.host) cudaFreeHost(p.host);
         if (p.dev) cudaFree(p.dev);
         if (p.ready) cudaEventDestroy(p.ready);
+        if (p.staged) cudaEventDestroy(p.staged);
     }
+    if (f->copy) cudaStreamDestroy(f->copy);
     const int crc = close(f->fd) == 0 ? LMB_OK : LMB_E_IO;
     delete f;
     return rc != LMB_OK ? rc : crc;

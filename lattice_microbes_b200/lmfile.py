@@ -658,6 +658,80 @@ class LMFileWriter:
         self._L.check(self._L.lib().lmb_lmfile_write_max_counts(self.h, replicate, self._p(mp, C.c_uint32), mp.size,
                                                                 self._p(ms, C.c_uint32), ms.size))
 
+    # -- generic objects (carrying an existing file's contents over) ----------
+    _CODES = {np.dtype("u1"): 1, np.dtype("i1"): 2, np.dtype("<u2"): 3, np.dtype("<i2"): 4, np.dtype("<u4"): 5,
+              np.dtype("<i4"): 6, np.dtype("<u8"): 7, np.dtype("<i8"): 8, np.dtype("<f4"): 9, np.dtype("<f8"): 10}
+
+    def create_group(self, path):
+        self._L.check(self._L.lib().lmb_lmfile_create_group(self.h, path.encode()))
+
+    def set_attribute(self, path, name, value):
+        """A string (scalar), or a numeric array / number (rank as given;
+        a Python number becomes a one-element array)."""
+        C, L = self._C, self._L
+        if isinstance(value, (str, bytes)):
+            v = value.encode() if isinstance(value, str) else value
+            buf = np.frombuffer(v + b"\0", dtype=np.uint8).copy()
+            L.check(L.lib().lmb_lmfile_set_attribute(self.h, path.encode(), name.encode(), 11, 0, None,
+                                                     buf.ctypes.data, buf.size))
+            return
+        a = np.asarray(value)
+        if a.dtype.kind == "S":
+            a = np.ascontiguousarray(a)
+            dims = np.asarray(a.shape, dtype=np.uint64)
+            L.check(L.lib().lmb_lmfile_set_attribute(self.h, path.encode(), name.encode(), 11, a.ndim,
+                                                     self._p(dims, C.c_uint64), a.ctypes.data, a.dtype.itemsize))
+            return
+        if a.ndim == 0:
+            a = a.reshape(1)
+        a = np.ascontiguousarray(a, dtype=a.dtype.newbyteorder("<"))
+        code = self._CODES.get(a.dtype)
+        if code is None:
+            raise TypeError("attribute type %s" % a.dtype)
+        dims = np.asarray(a.shape, dtype=np.uint64)
+        L.check(L.lib().lmb_lmfile_set_attribute(self.h, path.encode(), name.encode(), code, a.ndim,
+                                                 self._p(dims, C.c_uint64), a.ctypes.data, 0))
+
+    def write_dataset(self, group, name, data, chunks=None, gzip=-1, extendable=False):
+        C, L = self._C, self._L
+        a = np.ascontiguousarray(data)
+        a = np.ascontiguousarray(a, dtype=a.dtype.newbyteorder("<"))
+        code = self._CODES.get(a.dtype)
+        if code is None:
+            raise TypeError("dataset type %s" % a.dtype)
+        dims = np.asarray(a.shape, dtype=np.uint64)
+        cd = None if chunks is None else np.asarray(chunks, dtype=np.uint64)
+        L.check(L.lib().lmb_lmfile_write_dataset(self.h, group.encode(), name.encode(), code, a.ndim,
+                                                 self._p(dims, C.c_uint64), self._p(cd, C.c_uint64), int(gzip),
+                                                 int(bool(extendable)), a.ctypes.data if a.size else None))
+
+    def copy_from(self, src):
+        """Every group, attribute and dataset of an open H5File (or LMFile),
+        with each dataset's chunking, gzip level and extendability."""
+        h5 = src.h5 if isinstance(src, LMFile) else src
+
+        def walk(g, path):
+            if path:
+                self.create_group(path)
+            for k, v in g.attrs.items():
+                self.set_attribute(path or "/", k, v)
+            for name in g.keys():
+                o = g[name]
+                sub = path + "/" + name if path else name
+                if isinstance(o, Group):
+                    walk(o, sub)
+                    continue
+                gz = -1
+                for fid, _, vals in o.filters:
+                    if fid == 1:
+                        gz = vals[0] if vals else 6
+                ext = o.maxshape is not None and len(o.maxshape) > 0 and o.maxshape[0] is None
+                self.write_dataset(path or "/", name, o.read(), chunks=o.chunks, gzip=gz, extendable=ext)
+                for k, v in o.attrs.items():
+                    self.set_attribute(sub, k, v)
+
+        walk(h5.root, "")
+
     def flush(self):
         self._L.check(self._L.lib().lmb_lmfile_flush(self.h))
 

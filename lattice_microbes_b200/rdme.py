@@ -443,6 +443,64 @@ class IntMpdRdmeSolver(MpdRdmeSolver):
     tracks_max_counts = False
 
 
+def runSolver(simulationFilename, replicate, solver, cudaDevices=None, checkpointInterval=0):
+    """lm.runSolver (core/runSimulation.cpp:130-260), as pyLM's
+    RDMESimulation.runSolver and jLM call it per replicate: reads the
+    parameters, the reaction model and the diffusion model with its lattice
+    from the `.lm` file, initializes `solver` (an MpdRdmeSolver or
+    IntMpdRdmeSolver, or a subclass) for `replicate`, runs
+    generateTrajectory and writes the replicate's records into the same
+    file.  The file's existing contents, earlier replicates included, are
+    carried over: the new file is written beside it and replaces it when the
+    run ends.  Like the reference, an exception raised by the run is printed
+    and the records written so far are kept.  `cudaDevices` and
+    `checkpointInterval` are accepted for the reference's signature; the
+    solver runs on its own device."""
+    import os
+    import sys
+
+    from .lmfile import LMFile, LMFileWriter
+    with LMFile(simulationFilename) as f:
+        params = f.parameters()
+        rm = f.reaction_model() if solver.needsReactionModel() else None
+        dm = f.diffusion_model() if solver.needsDiffusionModel() else None
+    solver.initialize(replicate, params)
+    if rm is not None:
+        ns, nr = rm["numberSpecies"], rm["numberReactions"]
+        K = np.full((nr, 10), np.nan)
+        for i, r in enumerate(rm["reactions"]):
+            K[i, :len(r["rateConstants"])] = r["rateConstants"]
+        init = rm["initialSpeciesCounts"] or [0] * ns
+        solver.buildModel(ns, nr, init, [r["type"] for r in rm["reactions"]], K.ravel(),
+                          rm["stoichiometricMatrix"], rm["dependencyMatrix"], kCols=10)
+    if dm is not None:
+        nst = int(dm["numberSiteTypes"])
+        bpp = int(dm.get("bytes_per_particle", 1))
+        RL = dm.get("ReactionLocationMatrix", np.zeros((0, nst), np.uint32))
+        solver.buildDiffusionModel(nst, dm["DiffusionMatrix"].ravel(), np.asarray(RL).ravel(),
+                                   int(dm["latticeXSize"]), int(dm["latticeYSize"]), int(dm["latticeZSize"]),
+                                   int(dm["particlesPerSite"]), bpp, float(dm["latticeSpacing"]),
+                                   dm["Lattice"].reshape(-1), dm["LatticeSites"].reshape(-1))
+    tmp = "%s.%d.tmp" % (simulationFilename, os.getpid())
+    w = LMFileWriter(tmp)
+    try:
+        with LMFile(simulationFilename) as f:
+            w.copy_from(f)
+        solver.setOutputFile(w, writeInputs=False)
+        try:
+            solver.generateTrajectory()
+        except Exception as e:  # runSimulation.cpp:228-240: reported, the file is still closed
+            print("Exception during execution of replicate: %s." % e, file=sys.stderr)
+        solver.output = None
+        w.close()
+    except BaseException:
+        if w.h:
+            w.close()
+        os.unlink(tmp)
+        raise
+    os.replace(tmp, simulationFilename)
+
+
 class _ModelInputs:
     """The fields Model.from_spec reads."""
 

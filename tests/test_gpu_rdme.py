@@ -13,7 +13,7 @@ from tests.test_gpu_cpp_solver import _row_major_int, check_lmfile, clear_left, 
 pytestmark = pytest.mark.gpu
 
 
-def _solver(kind, spec, hook, params):
+def _solver(kind, spec, hook, params, replicate=3):
     from lattice_microbes_b200.rdme import IntMpdRdmeSolver, MpdRdmeSolver
     base = MpdRdmeSolver if kind == "byte" else IntMpdRdmeSolver
 
@@ -30,7 +30,7 @@ def _solver(kind, spec, hook, params):
             return 0
 
     s = Solver(0)
-    s.initialize(3, params)
+    s.initialize(replicate, params)
     init = configs.species_counts(spec.lattice, spec.nsites, spec.slots, spec.bytes_per_slot, spec.ns)[1:]
     s.buildModel(spec.ns, spec.nr, init, spec.rtype, spec.K, np.asarray(spec.S).reshape(-1),
                  np.asarray(spec.D).reshape(-1))
@@ -91,3 +91,44 @@ def test_python_solver_hook_3_stops(gpu):
     assert all(np.array_equal(a[1], b[1]) for a, b in zip(s.speciesCounts, ref_c))
     assert s.speciesCounts[-1][0] == 60 * spec.tau
     s.close()
+
+
+@pytest.mark.parametrize("kind", ["byte", "int"])
+def test_run_solver_from_an_lm_file(gpu, kind, tmp_path):
+    """lm.runSolver on a `.lm` file: a first replicate written with its
+    inputs, then runSolver reads the parameters, models and lattice back
+    from the file and appends replicate 4; its records equal a solver set up
+    directly for replicate 4, and replicate 3 is carried over unchanged."""
+    from lattice_microbes_b200.lmfile import LMFile, LMFileWriter
+    from lattice_microbes_b200.rdme import IntMpdRdmeSolver, MpdRdmeSolver, runSolver
+    if kind == "byte":
+        spec = configs.config0(seed=11, edge=16, nA=500, nB=500)
+        spec.K = spec.K * np.array([300.0, 30.0])
+    else:
+        spec = configs.random_problem(8, X=16, Y=8, Z=8, slots=16, bytes_per_slot=4, density=1.5, nst=2)
+    steps, ce, le = 120, 20, 40
+    params = {"seed": "9", "timestep": repr(spec.tau), "maxTime": repr((steps - 0.5) * spec.tau),
+              "writeInterval": str(ce), "latticeWriteInterval": str(le)}
+    lm = str(tmp_path / "run.lm")
+    first, _ = _solver(kind, spec, "none", params, replicate=3)
+    w = LMFileWriter(lm)
+    first.setOutputFile(w)
+    first.generateTrajectory()
+    w.close()
+    first.close()
+    cls = MpdRdmeSolver if kind == "byte" else IntMpdRdmeSolver
+    runSolver(lm, 4, cls(0))
+    direct, _ = _solver(kind, spec, "none", params, replicate=4)
+    direct.generateTrajectory()
+    with LMFile(lm) as f:
+        assert f.replicates() == [3, 4]
+        t, c = f.species_counts(4)
+        assert np.array_equal(t, [a for a, _ in direct.speciesCounts])
+        assert np.array_equal(c, np.array([b for _, b in direct.speciesCounts]))
+        assert np.array_equal(f.lattice_times(4), [a for a, _, _ in direct.latticeFrames])
+        from tests.test_gpu_cpp_solver import row_major_frame
+        for i, (_, fr, _) in enumerate(direct.latticeFrames):
+            assert np.array_equal(f.lattice(4, i), row_major_frame(spec, fr))
+        t3, c3 = f.species_counts(3)
+        assert len(t3) == 1 + steps // ce and not np.array_equal(c3, c)  # replicate 3 kept, another seed
+    direct.close()

@@ -144,3 +144,64 @@ def test_refuses_existing_file_and_bad_arguments(tmp_path):
             w.write_max_counts(0, np.zeros(3), np.zeros(3))
         with pytest.raises(L.LmbError):  # no diffusion model yet
             w.set_diffusion_model_lattice(np.zeros((2, 2, 2, 8), np.uint8), np.zeros((2, 2, 2), np.uint8))
+
+
+@pytest.mark.parametrize("name", ["SimulationFile_GetSpatialModelObjects.h5", "SimulationFile_GetReactionModel_Noise.h5",
+                                  "SimulationFile_GetDiffusionModel.h5", "SimulationFile_3.h5"])
+def test_copy_of_a_libhdf5_file(tmp_path, name):
+    """Every group, attribute and dataset of a libhdf5-written file survives
+    a copy through the writer (the runSolver path), with chunking and
+    extendability; appends then extend the copied extendable datasets."""
+    from lattice_microbes_b200.lmfile import Group
+    src = os.path.join(os.path.dirname(__file__), "golden", "lmfile", name)
+    p = str(tmp_path / "c.lm")
+    with LMFile(src) as a, LMFileWriter(p) as w:
+        w.copy_from(a)
+    with LMFile(src) as a, LMFile(p) as b:
+        assert a.version == b.version
+
+        def same(ga, gb):
+            assert sorted(ga.keys()) == sorted(gb.keys())
+            assert sorted(ga.attrs) == sorted(gb.attrs)
+            for k in ga.attrs:
+                va, vb = ga.attrs[k], gb.attrs[k]
+                assert (va == vb) if isinstance(va, str) else np.array_equal(va, vb)
+            for k in ga.keys():
+                oa, ob = ga[k], gb[k]
+                if isinstance(oa, Group):
+                    same(oa, ob)
+                else:
+                    assert oa.dtype == ob.dtype and oa.shape == ob.shape
+                    assert (oa.maxshape or oa.shape) == (ob.maxshape or ob.shape)  # no max: fixed
+                    assert oa.chunks == ob.chunks
+                    assert oa.read().tobytes() == ob.read().tobytes()  # bit for bit (NaN included)
+        same(a.h5.root, b.h5.root)
+    if "Spatial" in name:
+        p2 = str(tmp_path / "d.lm")
+        with LMFile(p) as a, LMFileWriter(p2) as w:
+            w.copy_from(a)
+            w.append_species_counts(0, [0.5, 1.0], [[3], [4]])
+        with LMFile(p2) as b:
+            t, c = b.species_counts(0)
+            assert np.array_equal(t, [0.5, 1.0]) and np.array_equal(c, [[3], [4]])
+
+
+def test_gzip_chunks_are_zlib_level_1(tmp_path):
+    """Each stored chunk is exactly zlib's level-1 stream of the chunk's
+    bytes, as libhdf5's deflate filter (compress2) stores it."""
+    import zlib
+    rng = np.random.default_rng(3)
+    a = (rng.random((20, 16, 16, 8)) < 0.02).astype(np.uint8) * 3
+    p = str(tmp_path / "z.lm")
+    with LMFileWriter(p) as w:
+        w.write_dataset("g", "d", a, chunks=(16, 16, 16, 8), gzip=1)
+    with LMFile(p) as f:
+        ds = f.h5["g/d"]
+        kids = f.h5._btree_children(ds.layout[1], 1, 4)
+        assert len(kids) == 2
+        for addr, nbytes, mask, offs in kids:
+            chunk = np.zeros((16, 16, 16, 8), np.uint8)
+            part = a[offs[0]:offs[0] + 16]
+            chunk[:part.shape[0]] = part
+            raw = bytes(f.h5.b[f.h5._addr(addr):f.h5._addr(addr) + nbytes])
+            assert mask == 0 and raw == zlib.compress(chunk.tobytes(), 1)
