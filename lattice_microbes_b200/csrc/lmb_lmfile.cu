@@ -236,17 +236,14 @@ struct Node {
 };
 
 // A frame for the writer thread: a host row-major copy (host calls), or a
-// pinned copy of the device lattice in its native layout (device calls:
-// slot k of site i = x + y X + z X Y is byte ((k / 4) N + i) * 4 + k % 4 of
-// a ByteLattice, word k N + i of an IntLattice; site types one byte per
-// site), which the writer reads into [x][y][z][p] chunks itself.
+// pinned copy of a device lattice frame already in chunk order (device
+// calls, frame_chunks_kernel).
 struct FrameJob {
     std::string group, name;          // dataset path
     Type type;
     std::vector<uint64_t> dims;       // [X, Y, Z(, P)]
     std::vector<uint8_t> host;        // host copy (host calls)
-    int slot = -1;                    // pinned slot (device calls)
-    uint32_t bytes_per_slot = 0;      // native layout of a device lattice frame (0: site types)
+    int slot = -1;                    // pinned slot (device calls): the frame in chunk order
 };
 
 struct Pinned {
@@ -670,32 +667,36 @@ int chunked_dataset(lmb_lmfile *f, const std::string &group, const std::string &
                            });
 }
 
-// The chunk at `o` of a [X][Y][Z]([P]) frame read from a device lattice's
-// native layout (FrameJob).
-void gather_native(const uint8_t *src, const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd,
-                   const std::vector<uint64_t> &o, uint32_t bps, uint8_t *dst)
+// A device lattice frame written straight into chunk order: chunk c =
+// (cx * gy + cy) * gz + cz of cx x cy x cz sites (x slowest), each chunk
+// [xx][yy][zz][p] contiguous (the layout its HDF5 chunk stores), so that the
+// host only compresses.  One thread per native word (ByteLattice: 4 slots,
+// IntLattice: 1 slot) or per site type; consecutive threads read
+// consecutive sites of one word plane.  Positions of edge chunks beyond the
+// lattice are left as they are (zeroed before the launch).
+struct ChunkShape {
+    uint32_t X, Y, Z, P, cx, cy, cz, gy, gz;
+};
+
+__global__ void frame_chunks_kernel(const uint32_t *__restrict__ native, const uint8_t *__restrict__ sites,
+                                    uint8_t *__restrict__ out, ChunkShape k, uint32_t words, uint32_t bps)
 {
-    const uint64_t X = dims[0], Y = dims[1], Z = dims[2], N = X * Y * Z;
-    const uint64_t P = dims.size() > 3 ? dims[3] : 1, es = bps ? bps : 1;
-    const uint64_t ex = std::min(cd[0], X - o[0]), ey = std::min(cd[1], Y - o[1]), ez = std::min(cd[2], Z - o[2]);
-    const uint64_t xstride = cd[1] * cd[2] * P * es;  // dst bytes between x neighbours
-    // x innermost: the source sites are consecutive.
-    for (uint64_t zz = 0; zz < ez; zz++)
-        for (uint64_t yy = 0; yy < ey; yy++) {
-            const uint64_t i0 = o[0] + X * ((o[1] + yy) + Y * (o[2] + zz));
-            uint8_t *d = dst + (yy * cd[2] + zz) * P * es;
-            if (bps == 0) {
-                for (uint64_t xx = 0; xx < ex; xx++) d[xx * xstride] = src[i0 + xx];
-            } else if (bps == 1) {
-                const uint32_t *w = (const uint32_t *)src;
-                for (uint64_t xx = 0; xx < ex; xx++)
-                    for (uint64_t k = 0; k < P; k += 4) memcpy(d + xx * xstride + k, &w[(k >> 2) * N + i0 + xx], 4);
-            } else {
-                const uint32_t *w = (const uint32_t *)src;
-                for (uint64_t xx = 0; xx < ex; xx++)
-                    for (uint64_t k = 0; k < P; k++) memcpy(d + xx * xstride + 4 * k, &w[k * N + i0 + xx], 4);
-            }
-        }
+    const uint64_t N = (uint64_t)k.X * k.Y * k.Z;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * (sites ? 1 : words)) return;
+    const uint64_t i = t % N, w = t / N;
+    const uint32_t x = (uint32_t)(i % k.X), y = (uint32_t)((i / k.X) % k.Y), z = (uint32_t)(i / ((uint64_t)k.X * k.Y));
+    const uint32_t bx = x / k.cx, by = y / k.cy, bz = z / k.cz;
+    const uint64_t c = ((uint64_t)bx * k.gy + by) * k.gz + bz;
+    const uint64_t e = ((uint64_t)(x - bx * k.cx) * k.cy + (y - by * k.cy)) * k.cz + (z - bz * k.cz);
+    const uint64_t cell = (uint64_t)k.cx * k.cy * k.cz;
+    if (sites) {
+        out[c * cell + e] = sites[i];
+    } else {
+        const uint64_t cb = cell * k.P * bps;  // chunk bytes
+        const uint64_t off = c * cb + (bps == 1 ? e * k.P + 4 * w : (e * k.P + w) * 4);
+        *(uint32_t *)(out + off) = native[w * N + i];
+    }
 }
 
 // ---- metadata --------------------------------------------------------------
@@ -1032,10 +1033,14 @@ void writer_main(lmb_lmfile *f)
             std::vector<uint64_t> cd(j.dims.size());
             for (size_t i = 0; i < cd.size(); i++) cd[i] = i < 3 ? std::min(FRAME_CHUNK, j.dims[i]) : j.dims[i];
             if (j.slot >= 0) {
-                const uint32_t bps = j.bytes_per_slot;
+                // Already in chunk order (frame_chunks_kernel).
+                const uint64_t gy = (j.dims[1] + cd[1] - 1) / cd[1], gz = (j.dims[2] + cd[2] - 1) / cd[2];
+                size_t cb = type_size(j.type, 0);
+                for (uint64_t c : cd) cb *= c;
                 rc = chunked_dataset(f, j.group, j.name, j.type, j.dims, cd, FRAME_GZIP,
                                      [&](const std::vector<uint64_t> &o, uint8_t *dst) {
-                                         gather_native(data, j.dims, cd, o, bps, dst);
+                                         const uint64_t c = ((o[0] / cd[0]) * gy + o[1] / cd[1]) * gz + o[2] / cd[2];
+                                         memcpy(dst, data + c * cb, cb);
                                      });
             } else {
                 rc = chunked_dataset(f, j.group, j.name, j.type, j.dims, cd, FRAME_GZIP, data);
@@ -1124,18 +1129,37 @@ int append_device(lmb_lmfile *f, uint32_t rep, double time, lmb_lattice *lat, bo
     if (f->device != v.ctx->device) return LMB_E_ARG;
     if (cudaSetDevice(f->device) != cudaSuccess) return LMB_E_CUDA;
     const size_t N = v.g.N, esize = v.bytes_per_slot;
-    const size_t bytes = sites ? N : N * v.slots * esize;
+    ChunkShape k;
+    k.X = v.g.X;
+    k.Y = v.g.Y;
+    k.Z = v.g.Z;
+    k.P = sites ? 1 : v.slots;
+    k.cx = (uint32_t)std::min<uint64_t>(FRAME_CHUNK, k.X);
+    k.cy = (uint32_t)std::min<uint64_t>(FRAME_CHUNK, k.Y);
+    k.cz = (uint32_t)std::min<uint64_t>(FRAME_CHUNK, k.Z);
+    const uint32_t gx = (k.X + k.cx - 1) / k.cx;
+    k.gy = (k.Y + k.cy - 1) / k.cy;
+    k.gz = (k.Z + k.cz - 1) / k.cz;
+    const bool ragged = k.X % k.cx || k.Y % k.cy || k.Z % k.cz;
+    const size_t bytes = (size_t)gx * k.gy * k.gz * k.cx * k.cy * k.cz * k.P * (sites ? 1 : esize);
+    const uint32_t words = esize == 1 ? v.slots / 4 : v.slots;
     if (!f->copy && cudaStreamCreateWithFlags(&f->copy, cudaStreamNonBlocking) != cudaSuccess) return LMB_E_CUDA;
     int s = -1;
     rc = take_slot(f, bytes, &s);
     if (rc != LMB_OK) return rc;
     Pinned &p = f->pinned[s];
-    // A device snapshot in the lattice's stream order (the lattice may be
-    // advanced right after), then the copy to pinned memory on the file's
-    // own stream, overlapping the next timesteps.
+    // The frame in chunk order, in the lattice's stream order (the lattice
+    // may be advanced right after), then the copy to pinned memory on the
+    // file's own stream, overlapping the next timesteps.
     cudaStream_t st = v.ctx->stream;
-    cudaError_t e = cudaMemcpyAsync(p.dev, sites ? (const void *)v.sites : (const void *)v.particles, bytes,
-                                    cudaMemcpyDeviceToDevice, st);
+    cudaError_t e = ragged ? cudaMemsetAsync(p.dev, 0, bytes, st) : cudaSuccess;
+    if (e == cudaSuccess) {
+        const uint64_t threads = (uint64_t)N * (sites ? 1 : words);
+        frame_chunks_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+            v.particles, sites ? v.sites : nullptr, (uint8_t *)p.dev, k, words, (uint32_t)esize);
+        lmb::count_launch();
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaEventRecord(p.staged, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(f->copy, p.staged, 0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(p.host, p.dev, bytes, cudaMemcpyDeviceToHost, f->copy);
@@ -1147,7 +1171,6 @@ int append_device(lmb_lmfile *f, uint32_t rep, double time, lmb_lattice *lat, bo
     }
     FrameJob j;
     j.slot = s;
-    j.bytes_per_slot = sites ? 0 : v.bytes_per_slot;
     {
         std::lock_guard<std::mutex> lk(f->mu);
         const char *grp = sites ? "Sites" : "Lattice";
