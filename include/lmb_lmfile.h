@@ -144,6 +144,12 @@ int lmb_lmfile_write_dataset(lmb_lmfile *f, const char *group, const char *name,
  * SimulationFile.cpp:158-190). */
 int lmb_lmfile_flush(lmb_lmfile *f);
 
+/* SimulationFile::checkpoint (SimulationFile.cpp:158-190): flushes, then
+ * copies the complete file to "<path>.chk" and writes that name (with its
+ * terminator) to checkpoint_path when it fits in size bytes (else
+ * LMB_E_ARG after the copy).  checkpoint_path may be NULL. */
+int lmb_lmfile_checkpoint(lmb_lmfile *f, char *checkpoint_path, uint64_t size);
+
 /* Frames written and bytes of compressed chunk data appended so far. */
 int lmb_lmfile_stats(lmb_lmfile *f, uint64_t *frames, uint64_t *chunk_bytes);
 

@@ -174,6 +174,7 @@ PROTOTYPES = {
     "lmb_lmfile_write_dataset": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_int, C.c_uint32, u64p, u64p, C.c_int,
                                            C.c_int, vp]),
     "lmb_lmfile_flush": (C.c_int, [vp]),
+    "lmb_lmfile_checkpoint": (C.c_int, [vp, C.c_char_p, C.c_uint64]),
     "lmb_lmfile_stats": (C.c_int, [vp, u64p, u64p]),
     "lmb_lmfile_close": (C.c_int, [vp]),
 }

@@ -342,6 +342,7 @@ private:
 
 struct lmb_lmfile {
     int fd = -1;
+    std::string path;
     uint64_t eof = SUPERBLOCK;  // relative to the superblock
     Node root;
     // During a flush the metadata is gathered here and written at once.
@@ -1201,6 +1202,7 @@ extern "C" int lmb_lmfile_create(const char *path, lmb_lmfile **out)
     if (fd < 0) return LMB_E_IO;
     lmb_lmfile *f = new lmb_lmfile();
     f->fd = fd;
+    f->path = path;
     // Chunk compression threads: up to 16, leaving two host cores to the
     // thread that drives the GPU.
     const unsigned hw = std::thread::hardware_concurrency();
@@ -1482,6 +1484,36 @@ extern "C" int lmb_lmfile_flush(lmb_lmfile *f)
     if (rc != LMB_OK) return rc;
     std::lock_guard<std::mutex> lk(f->mu);
     return commit(f);
+}
+
+extern "C" int lmb_lmfile_checkpoint(lmb_lmfile *f, char *out, uint64_t size)
+{
+    if (!f) return LMB_E_ARG;
+    int rc = drain(f);
+    if (rc != LMB_OK) return rc;
+    const std::string chk = f->path + ".chk";
+    {
+        std::lock_guard<std::mutex> lk(f->mu);
+        rc = commit(f);
+        if (rc != LMB_OK) return rc;
+        const int fd = open(chk.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+        if (fd < 0) return LMB_E_IO;
+        std::vector<uint8_t> buf(1 << 20);
+        const uint64_t total = USER_BLOCK + f->eof;
+        for (uint64_t off = 0; off < total && rc == LMB_OK;) {
+            const size_t n = (size_t)std::min<uint64_t>(buf.size(), total - off);
+            const ssize_t r = pread(f->fd, buf.data(), n, (off_t)off);
+            if (r <= 0 || write(fd, buf.data(), (size_t)r) != r) rc = LMB_E_IO;
+            off += r > 0 ? (uint64_t)r : 0;
+        }
+        if (close(fd) != 0) rc = LMB_E_IO;
+        if (rc != LMB_OK) return rc;
+    }
+    if (out) {
+        if (chk.size() + 1 > size) return LMB_E_ARG;
+        memcpy(out, chk.c_str(), chk.size() + 1);
+    }
+    return LMB_OK;
 }
 
 extern "C" int lmb_lmfile_stats(lmb_lmfile *f, uint64_t *frames, uint64_t *chunk_bytes)

@@ -554,6 +554,33 @@ class LMFile:
         """Site-type frame `index`, shape (X, Y, Z)."""
         return self._rep(replicate)["Sites/%010d" % index].read()
 
+    # The reference's SimulationFile getter names (io/SimulationFile.h:134-266).
+    def getParameters(self):
+        return self.parameters()
+
+    def getParameter(self, key, defaultValue=""):
+        return self.parameters().get(key, defaultValue)
+
+    def getReactionModel(self):
+        return self.reaction_model()
+
+    def getDiffusionModel(self):
+        return self.diffusion_model()
+
+    def getLatticeTimes(self, replicate):
+        return list(self.lattice_times(replicate))
+
+    def getLattice(self, replicate, latticeIndex):
+        return self.lattice(replicate, latticeIndex)
+
+    def getSpeciesCountTimes(self, replicate):
+        return list(self.species_counts(replicate)[0])
+
+    def getSpeciesCounts(self, replicate):
+        """{time: counts of species 1..ns} as SimulationFile::getSpeciesCounts."""
+        t, c = self.species_counts(replicate)
+        return {float(a): [int(v) for v in b] for a, b in zip(t, c)}
+
     def max_counts(self, replicate):
         g = self._rep(replicate)
         if "MaxParticleCounts" not in g:
@@ -734,6 +761,13 @@ class LMFileWriter:
 
     def flush(self):
         self._L.check(self._L.lib().lmb_lmfile_flush(self.h))
+
+    def checkpoint(self):
+        """SimulationFile::checkpoint: the file so far, complete, copied to
+        "<path>.chk"; returns that name."""
+        buf = self._C.create_string_buffer(len(os.fsencode(self.path)) + 16)
+        self._L.check(self._L.lib().lmb_lmfile_checkpoint(self.h, buf, len(buf)))
+        return os.fsdecode(buf.value)
 
     def stats(self):
         C = self._C

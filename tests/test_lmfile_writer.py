@@ -205,3 +205,24 @@ def test_gzip_chunks_are_zlib_level_1(tmp_path):
             chunk[:part.shape[0]] = part
             raw = bytes(f.h5.b[f.h5._addr(addr):f.h5._addr(addr) + nbytes])
             assert mask == 0 and raw == zlib.compress(chunk.tobytes(), 1)
+
+
+def test_checkpoint_copies_the_file_so_far(tmp_path):
+    """SimulationFile::checkpoint: the checkpoint is a complete file with the
+    records written so far; the run goes on in the original."""
+    p = str(tmp_path / "k.lm")
+    a = np.arange(4 * 4 * 4 * 8, dtype=np.uint8).reshape(4, 4, 4, 8)
+    w = LMFileWriter(p)
+    w.set_parameter("maxTime", "2.0")
+    w.append_lattice(1, 0.0, a)
+    w.append_species_counts(1, [0.0], [[5, 6]])
+    chk = w.checkpoint()
+    assert chk == p + ".chk"
+    w.append_lattice(1, 1.0, a + 1)
+    w.close()
+    with LMFile(chk) as f:
+        assert f.getParameter("maxTime") == "2.0" and f.getParameter("absent", "x") == "x"
+        assert f.getLatticeTimes(1) == [0.0] and np.array_equal(f.getLattice(1, 0), a)
+        assert f.getSpeciesCounts(1) == {0.0: [5, 6]}
+    with LMFile(p) as f:
+        assert f.getLatticeTimes(1) == [0.0, 1.0] and np.array_equal(f.getLattice(1, 1), a + 1)
