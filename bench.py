@@ -105,6 +105,24 @@ def parse():
 # CPU side: the reference's code on the host cores
 # --------------------------------------------------------------------------
 
+class stdout_to_stderr:
+    """Sends what the reference's code prints on standard output (its
+    Print::printf warnings) to standard error while it runs, at the file
+    descriptor level, so that standard output holds only the JSON line.
+    Worker processes started inside inherit the redirection."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def host_cores():
     """Host threads this process may run on."""
     try:
@@ -354,10 +372,13 @@ def run_ours(a):
     cpu_mpd = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = host_cores()
-        val, sample = cpu_nsm_sample(a.workload, a.cpu_sample_time or w["nsm_time"], cores)
+        with stdout_to_stderr():
+            val, sample = cpu_nsm_sample(a.workload, a.cpu_sample_time or w["nsm_time"], cores)
         if val is not None:
             cpu = {"value": val, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample}
-        val, sample = cpu_reference_sample(a.workload, a.cpu_sample_timesteps or w["ref_mpd_timesteps"], cores)
+        with stdout_to_stderr():
+            val, sample = cpu_reference_sample(a.workload, a.cpu_sample_timesteps or w["ref_mpd_timesteps"],
+                                               cores)
         if val is not None:
             cpu_mpd = {"value": val, "unit": METRIC, "cores": cores, "sample": sample}
 
@@ -384,7 +405,8 @@ def run_ours(a):
             from tests.cases import oracle_tables
             from tests.oracle_lib import reference_gpu_time
             nref = w["ref_timesteps"]
-            r = reference_gpu_time(oracle_tables(spec), spec.lattice, spec.sites, seed, 0, nref)
+            with stdout_to_stderr():
+                r = reference_gpu_time(oracle_tables(spec), spec.lattice, spec.sites, seed, 0, nref)
             if r is not None and r[0] == 0:
                 ref_gpu = {"value": N * nref / (r[1] / 1e3), "unit": METRIC, "timesteps": nref,
                            "what": "reference device functions built for sm_100a, reference host loop "
@@ -548,9 +570,11 @@ def run_reference(a):
     sim_time = a.cpu_sample_time or w["nsm_time"] / 4
     vals, samples = [], []
     for _ in range(min(a.warmup, 1)):
-        cpu_nsm_sample(wname, sim_time / 4, cores)
+        with stdout_to_stderr():
+            cpu_nsm_sample(wname, sim_time / 4, cores)
     for _ in range(a.steps):
-        v, s = cpu_nsm_sample(wname, sim_time, cores)
+        with stdout_to_stderr():
+            v, s = cpu_nsm_sample(wname, sim_time, cores)
         if v is None:
             print(json.dumps({"impl": "reference", "unavailable": s}))
             return
@@ -724,7 +748,8 @@ def run_cme(a):
     cores = host_cores()
     cpu = None
     if not a.no_cpu_baseline:
-        v, sample = cpu_gillespie_sample(1500, cores)
+        with stdout_to_stderr():
+            v, sample = cpu_gillespie_sample(1500, cores)
         if v is not None:
             cpu = {"value": v, "unit": "replicates/s", "cores": cores, "kind": "reference", "sample": sample}
     torch.cuda.set_device(0)
