@@ -565,6 +565,7 @@ struct Deflater {
     {
         if (level >= 0) deflateEnd(&s);
     }
+    std::vector<uint8_t> scratch;  // deflateBound-sized, reused: only the result is copied out
     bool run(const uint8_t *in, size_t n, int lvl, std::vector<uint8_t> &out)
     {
         if (level != lvl) {
@@ -576,20 +577,23 @@ struct Deflater {
         } else if (deflateReset(&s) != Z_OK) {
             return false;
         }
-        out.resize(deflateBound(&s, n));
+        const size_t bound = deflateBound(&s, n);
+        if (scratch.size() < bound) scratch.resize(bound);
         s.next_in = const_cast<Bytef *>(in);
         s.avail_in = (uInt)n;
-        s.next_out = out.data();
-        s.avail_out = (uInt)out.size();
+        s.next_out = scratch.data();
+        s.avail_out = (uInt)bound;
         if (deflate(&s, Z_FINISH) != Z_STREAM_END) return false;
-        out.resize(out.size() - s.avail_out);
+        out.assign(scratch.data(), scratch.data() + (bound - s.avail_out));
         return true;
     }
 };
 
+// `direct`, when given, holds the chunks already in chunk order, each
+// contiguous: they are compressed where they lie.
 bool make_chunks(const Gather &gather, const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd,
                  size_t esize, int level, Pool &pool, std::vector<std::vector<uint8_t>> &out,
-                 std::vector<std::vector<uint64_t>> &origins)
+                 std::vector<std::vector<uint64_t>> &origins, const uint8_t *direct = nullptr)
 {
     const size_t r = dims.size();
     std::vector<uint64_t> grid(r);
@@ -613,14 +617,18 @@ bool make_chunks(const Gather &gather, const std::vector<uint64_t> &dims, const 
     std::atomic<bool> ok{true};
     pool.run(nch, [&](size_t c) {
         thread_local std::vector<uint8_t> raw;
-        raw.assign(cbytes, 0);
-        gather(origins[c], raw.data());
+        const uint8_t *in = direct ? direct + c * cbytes : nullptr;
+        if (!in) {
+            raw.assign(cbytes, 0);
+            gather(origins[c], raw.data());
+            in = raw.data();
+        }
         if (level < 0) {
-            out[c] = raw;
+            out[c].assign(in, in + cbytes);
             return;
         }
         thread_local Deflater z;
-        if (!z.run(raw.data(), cbytes, level, out[c])) ok = false;
+        if (!z.run(in, cbytes, level, out[c])) ok = false;
     });
     return ok;
 }
@@ -629,11 +637,11 @@ bool make_chunks(const Gather &gather, const std::vector<uint64_t> &dims, const 
 // friends): chunks are compressed outside the file lock, then appended.
 int chunked_dataset(lmb_lmfile *f, const std::string &group, const std::string &name, Type t,
                     const std::vector<uint64_t> &dims, const std::vector<uint64_t> &cd, int level,
-                    const Gather &gather)
+                    const Gather &gather, const uint8_t *direct = nullptr)
 {
     std::vector<std::vector<uint8_t>> out;
     std::vector<std::vector<uint64_t>> origins;
-    if (!make_chunks(gather, dims, cd, type_size(t, 0), level, *f->pool, out, origins)) return LMB_E_IO;
+    if (!make_chunks(gather, dims, cd, type_size(t, 0), level, *f->pool, out, origins, direct)) return LMB_E_IO;
     std::lock_guard<std::mutex> lk(f->mu);
     std::unique_ptr<Node> d(new Node());
     d->group = false;
@@ -1034,15 +1042,9 @@ void writer_main(lmb_lmfile *f)
             std::vector<uint64_t> cd(j.dims.size());
             for (size_t i = 0; i < cd.size(); i++) cd[i] = i < 3 ? std::min(FRAME_CHUNK, j.dims[i]) : j.dims[i];
             if (j.slot >= 0) {
-                // Already in chunk order (frame_chunks_kernel).
-                const uint64_t gy = (j.dims[1] + cd[1] - 1) / cd[1], gz = (j.dims[2] + cd[2] - 1) / cd[2];
-                size_t cb = type_size(j.type, 0);
-                for (uint64_t c : cd) cb *= c;
+                // Already in chunk order (frame_chunks_kernel): compressed in place.
                 rc = chunked_dataset(f, j.group, j.name, j.type, j.dims, cd, FRAME_GZIP,
-                                     [&](const std::vector<uint64_t> &o, uint8_t *dst) {
-                                         const uint64_t c = ((o[0] / cd[0]) * gy + o[1] / cd[1]) * gz + o[2] / cd[2];
-                                         memcpy(dst, data + c * cb, cb);
-                                     });
+                                     [](const std::vector<uint64_t> &, uint8_t *) {}, data);
             } else {
                 rc = chunked_dataset(f, j.group, j.name, j.type, j.dims, cd, FRAME_GZIP, data);
             }
