@@ -132,3 +132,47 @@ def test_run_solver_from_an_lm_file(gpu, kind, tmp_path):
         t3, c3 = f.species_counts(3)
         assert len(t3) == 1 + steps // ce and not np.array_equal(c3, c)  # replicate 3 kept, another seed
     direct.close()
+
+
+def test_python_solver_site_frames_in_the_lm_file(gpu, tmp_path):
+    """A hook that changes a site type and returns 2 (sites copied to the
+    device and written): the file's site frame is the changed [x][y][z]
+    site-type lattice, and the site maxima count the change."""
+    from lattice_microbes_b200.lmfile import LMFile, LMFileWriter
+    from lattice_microbes_b200.rdme import MpdRdmeSolver
+    spec = configs.random_problem(8, X=16, Y=8, Z=8, slots=8, bytes_per_slot=1, density=0.5, nst=3)
+
+    class Solver(MpdRdmeSolver):
+        def hookSimulation(self, time, lattice):
+            if time > 0.0:
+                return 0
+            old = lattice.getSiteType(3, 2, 1)
+            lattice.setSiteType(3, 2, 1, 2 if old != 2 else 1)
+            return 2
+
+    params = {"seed": "5", "timestep": repr(spec.tau), "maxTime": repr(39.5 * spec.tau), "writeInterval": "10",
+              "latticeWriteInterval": "20", "hookInterval": "20"}
+    s = Solver(0)
+    s.initialize(1, params)
+    init = configs.species_counts(spec.lattice, spec.nsites, spec.slots, spec.bytes_per_slot, spec.ns)[1:]
+    s.buildModel(spec.ns, spec.nr, init, spec.rtype, spec.K, np.asarray(spec.S).reshape(-1),
+                 np.asarray(spec.D).reshape(-1))
+    lat_rm, sites_rm = ref_cpu_lib.row_major(spec)
+    s.buildDiffusionModel(spec.nst, np.asarray(spec.DF).reshape(-1), np.asarray(spec.RL).reshape(-1), spec.X,
+                          spec.Y, spec.Z, spec.slots, spec.bytes_per_slot, spec.spacing, lat_rm, sites_rm)
+    p = str(tmp_path / "sites.lm")
+    w = LMFileWriter(p)
+    s.setOutputFile(w)
+    s.generateTrajectory()
+    w.close()
+    want = spec.sites.reshape(spec.Z, spec.Y, spec.X).transpose(2, 1, 0).copy()
+    want[3, 2, 1] = 2 if want[3, 2, 1] != 2 else 1
+    with LMFile(p) as f:
+        assert np.array_equal(f.site_times(1), [0.0])
+        assert np.array_equal(f.sites(1, 0), want)
+        ms = f.max_counts(1)[1]
+    t = want.ravel()
+    expect = np.maximum(np.bincount(spec.sites[(spec.sites > 0) & (spec.sites < spec.nst)], minlength=spec.nst),
+                        np.bincount(t[(t > 0) & (t < spec.nst)], minlength=spec.nst))
+    assert np.array_equal(ms, expect) and np.array_equal(s.maxSiteCounts, expect)
+    s.close()
