@@ -427,6 +427,9 @@ Node *group_at(Node &root, const std::string &path)
     return n;
 }
 
+// An attribute message must fit a header message's 16-bit size.
+bool attr_fits(const Attr &a) { return attribute(a).size() <= 0xFFF8; }
+
 void set_attr(Node &n, Attr a)
 {
     for (auto &x : n.attrs)
@@ -1234,8 +1237,10 @@ extern "C" int lmb_lmfile_create(const char *path, lmb_lmfile **out)
 extern "C" int lmb_lmfile_set_parameter(lmb_lmfile *f, const char *key, const char *value)
 {
     if (!f || !key || !value || !*key) return LMB_E_ARG;
+    Attr a = string_attr(key, value);
+    if (!attr_fits(a)) return LMB_E_ARG;
     std::lock_guard<std::mutex> lk(f->mu);
-    set_attr(*group_at(f->root, "Parameters"), string_attr(key, value));
+    set_attr(*group_at(f->root, "Parameters"), std::move(a));
     return f->io_error;
 }
 
@@ -1422,6 +1427,7 @@ extern "C" int lmb_lmfile_set_attribute(lmb_lmfile *f, const char *path, const c
     if (n && !data) return LMB_E_ARG;
     const uint8_t *b = (const uint8_t *)data;
     a.data.assign(b, b + n);
+    if (!attr_fits(a)) return LMB_E_ARG;
     std::lock_guard<std::mutex> lk(f->mu);
     // The object: a group (made if missing) or an existing dataset.
     const std::string p = path;

@@ -226,3 +226,17 @@ def test_checkpoint_copies_the_file_so_far(tmp_path):
         assert f.getSpeciesCounts(1) == {0.0: [5, 6]}
     with LMFile(p) as f:
         assert f.getLatticeTimes(1) == [0.0, 1.0] and np.array_equal(f.getLattice(1, 1), a + 1)
+
+
+def test_oversized_attribute_is_refused(tmp_path):
+    """A header message holds at most 64 KiB: a longer parameter is refused,
+    and the file stays valid."""
+    from lattice_microbes_b200 import _lib as L
+    p = str(tmp_path / "big_attr.lm")
+    with LMFileWriter(p) as w:
+        with pytest.raises(L.LmbError) as e:
+            w.set_parameter("long", "x" * 70000)
+        assert e.value.status == L.LMB_E_ARG
+        w.set_parameter("short", "y" * 60000)
+    with LMFile(p) as f:
+        assert f.parameters() == {"short": "y" * 60000}
