@@ -166,6 +166,15 @@ class HostLattice:
         ids, counts = np.unique(v[v != 0], return_counts=True)
         return {int(s): int(c) for s, c in zip(ids, counts)}
 
+    def rowMajor(self):
+        """(particles [x][y][z][p], site types [x][y][z]): the arrays
+        buildDiffusionModel takes, as Lattice::rowMajorByteSerialize /
+        rowMajorIntSerialize and rowMajorByteSerializeSites lay them out."""
+        v = self.getParticleLatticeView()                    # (words, Z, Y, X, per-word slots)
+        p = np.moveaxis(v, 0, 3).reshape(self.Z, self.Y, self.X, self.slots)
+        return (np.ascontiguousarray(p.transpose(2, 1, 0, 3)),
+                np.ascontiguousarray(self.getSiteLatticeView().transpose(2, 1, 0)))
+
     # Views (lm.i:894-895, 913-914)
     def getSiteLatticeView(self):
         """Site types, shape (Z, Y, X), sharing memory with the lattice."""
@@ -178,6 +187,29 @@ class HostLattice:
         if self.bytes_per_particle == 1:
             return self.particles.view(np.uint8).reshape(self.words, self.Z, self.Y, self.X, 4)
         return self.particles.reshape(self.words, self.Z, self.Y, self.X, 1)
+
+
+def getCompiledLatticeMaxOccupancy():
+    """lm.getCompiledLatticeMaxOccupancy (lm.i:854): the particles per site
+    pyLM and jLM give new lattices -- 16, the reference build's default
+    MPD_LATTICE_MAX_OCCUPANCY (src/cmake/options.cmake:61).  The solvers here
+    take 4, 8, 16 or 32 slots per site on a ByteLattice and 4, 8 or 16 on an
+    IntLattice, chosen per lattice at run time."""
+    return 16
+
+
+class ByteLattice(HostLattice):
+    """lm.ByteLattice(xSize, ySize, zSize, spacing, particlesPerSite)."""
+
+    def __init__(self, xSize, ySize, zSize, spacing, particlesPerSite):
+        super().__init__(xSize, ySize, zSize, particlesPerSite, 1, spacing)
+
+
+class IntLattice(HostLattice):
+    """lm.IntLattice(xSize, ySize, zSize, spacing, particlesPerSite)."""
+
+    def __init__(self, xSize, ySize, zSize, spacing, particlesPerSite):
+        super().__init__(xSize, ySize, zSize, particlesPerSite, 4, spacing)
 
 
 class MpdRdmeSolver:

@@ -73,3 +73,30 @@ def test_host_lattice_accessors(slots, bps):
         h.addParticle(x, y, z, 3)
     with pytest.raises(IndexError):
         h.getSiteType(spec.X, 0, 0)
+
+
+def test_lattice_constructors_and_row_major_export():
+    """lm.ByteLattice / lm.IntLattice built in a script, filled with
+    addParticle, exported in the row-major order buildDiffusionModel takes."""
+    from lattice_microbes_b200 import configs
+    from lattice_microbes_b200.rdme import ByteLattice, IntLattice, getCompiledLatticeMaxOccupancy
+    assert getCompiledLatticeMaxOccupancy() == 16
+    for cls, bps in ((ByteLattice, 1), (IntLattice, 4)):
+        lat = cls(6, 5, 4, 16e-9, 8)
+        assert (lat.getXSize(), lat.getMaxOccupancy(), lat.getSpacing()) == (6, 8, 16e-9)
+        rng = np.random.default_rng(bps)
+        want = np.zeros((6, 5, 4, 8), dtype=np.uint8 if bps == 1 else np.uint32)
+        for _ in range(60):
+            x, y, z = (int(v) for v in rng.integers(0, (6, 5, 4)))
+            n = lat.getOccupancy(x, y, z)
+            if n < 8:
+                sp = int(rng.integers(1, 200))
+                lat.addParticle(x, y, z, sp)
+                want[x, y, z, n] = sp
+        lat.setSiteType(1, 2, 3, 2)
+        p, s = lat.rowMajor()
+        assert p.dtype == want.dtype and np.array_equal(p, want)
+        assert s.shape == (6, 5, 4) and s[1, 2, 3] == 2 and s.sum() == 2
+        # the native words agree with the oracle-side reader
+        slots = configs.native_to_slots(lat.particles, 6, 5, 4, 8, bps)
+        assert np.array_equal(slots.reshape(4, 5, 6, 8).transpose(2, 1, 0, 3), want)
