@@ -234,6 +234,8 @@ class MpdRdmeSolver:
         self.lastRunStats = None
         self.output = None            # lmfile.LMFileWriter the trajectory goes to
         self._write_inputs = False
+        self.checkpointInterval = 0.0  # seconds between checkpoints of the output file (0: none)
+        self._last_checkpoint = 0.0
         self._stop = False
 
     def needsReactionModel(self):
@@ -307,6 +309,17 @@ class MpdRdmeSolver:
         self.output = writer
         self._write_inputs = bool(writeInputs)
 
+    def _maybe_checkpoint(self):
+        # CheckpointSignaler (core/CheckpointSignaler.cpp:72-180): every
+        # checkpointInterval seconds of wall time the file is checkpointed
+        # (here at the next record written).
+        if self.output is None or self.checkpointInterval <= 0:
+            return
+        now = _time.monotonic()
+        if now - self._last_checkpoint >= self.checkpointInterval:
+            self.output.checkpoint()
+            self._last_checkpoint = now
+
     def _write_inputs_to_file(self):
         w = self.output
         for k, v in self.parameters.items():
@@ -369,6 +382,7 @@ class MpdRdmeSolver:
         if self.output is not None:
             self.output.append_species_counts(self.replicate, [time],
                                               np.asarray(c[1:], dtype=np.int64).astype(np.int32)[None, :])
+            self._maybe_checkpoint()
 
     def _write_lattice(self, time):
         # writeLatticeData (MpdRdmeSolver.cu:854-883): the particle maxima,
@@ -424,6 +438,7 @@ class MpdRdmeSolver:
         self._upload(True)
         if self.output is not None and self._write_inputs:
             self._write_inputs_to_file()
+        self._last_checkpoint = _time.monotonic()
         t = 0.0
         self._max_particles = np.zeros(self._ns + 1, dtype=np.uint32)
         self._max_sites = np.zeros(self._nst, dtype=np.uint32)
@@ -485,9 +500,12 @@ def runSolver(simulationFilename, replicate, solver, cudaDevices=None, checkpoin
     file.  The file's existing contents, earlier replicates included, are
     carried over: the new file is written beside it and replaces it when the
     run ends.  Like the reference, an exception raised by the run is printed
-    and the records written so far are kept.  `cudaDevices` and
-    `checkpointInterval` are accepted for the reference's signature; the
-    solver runs on its own device."""
+    and the records written so far are kept.  With `checkpointInterval` > 0
+    the file so far is copied, complete, to "<file>.chk" every that many
+    seconds (at the next record), as the reference's CheckpointSignaler has
+    it done; the copy is of the file being written beside the original.
+    `cudaDevices` is accepted for the reference's signature; the solver runs
+    on its own device."""
     import os
     import sys
 
@@ -519,6 +537,7 @@ def runSolver(simulationFilename, replicate, solver, cudaDevices=None, checkpoin
         with LMFile(simulationFilename) as f:
             w.copy_from(f)
         solver.setOutputFile(w, writeInputs=False)
+        solver.checkpointInterval = float(checkpointInterval or 0)
         try:
             solver.generateTrajectory()
         except Exception as e:  # runSimulation.cpp:228-240: reported, the file is still closed

@@ -100,3 +100,28 @@ def test_lattice_constructors_and_row_major_export():
         # the native words agree with the oracle-side reader
         slots = configs.native_to_slots(lat.particles, 6, 5, 4, 8, bps)
         assert np.array_equal(slots.reshape(4, 5, 6, 8).transpose(2, 1, 0, 3), want)
+
+
+def test_checkpoint_timer_checkpoints_at_the_next_record():
+    """The CheckpointSignaler stand-in: a checkpoint at the first record once
+    the interval has passed, none before, none without an interval."""
+    from lattice_microbes_b200.rdme import MpdRdmeSolver
+
+    class Out:
+        n = 0
+
+        def checkpoint(self):
+            Out.n += 1
+
+    s = MpdRdmeSolver.__new__(MpdRdmeSolver)
+    s.output, s.checkpointInterval, s._last_checkpoint = Out(), 0.0, 0.0
+    s._maybe_checkpoint()
+    assert Out.n == 0
+    import time
+    s.checkpointInterval, s._last_checkpoint = 3600.0, time.monotonic()
+    s._maybe_checkpoint()
+    assert Out.n == 0
+    s._last_checkpoint -= 3601.0
+    s._maybe_checkpoint()
+    s._maybe_checkpoint()
+    assert Out.n == 1
