@@ -603,6 +603,7 @@ class LMFileWriter:
         L.check(L.lib().lmb_lmfile_create(os.fsencode(path), C.byref(h)), "lmb_lmfile_create(%s)" % path)
         self.h = h
         self.path = path
+        self.checkpoint_path = None  # where checkpoint() puts the copy (None: "<path>.chk")
 
     def _p(self, a, t):
         return a.ctypes.data_as(self._C.POINTER(t)) if a is not None else None
@@ -767,7 +768,11 @@ class LMFileWriter:
         "<path>.chk"; returns that name."""
         buf = self._C.create_string_buffer(len(os.fsencode(self.path)) + 16)
         self._L.check(self._L.lib().lmb_lmfile_checkpoint(self.h, buf, len(buf)))
-        return os.fsdecode(buf.value)
+        chk = os.fsdecode(buf.value)
+        if self.checkpoint_path:
+            os.replace(chk, self.checkpoint_path)
+            chk = self.checkpoint_path
+        return chk
 
     def stats(self):
         C = self._C

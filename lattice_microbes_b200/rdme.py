@@ -533,6 +533,7 @@ def runSolver(simulationFilename, replicate, solver, cudaDevices=None, checkpoin
                                    dm["Lattice"].reshape(-1), dm["LatticeSites"].reshape(-1))
     tmp = "%s.%d.tmp" % (simulationFilename, os.getpid())
     w = LMFileWriter(tmp)
+    w.checkpoint_path = simulationFilename + ".chk"
     try:
         with LMFile(simulationFilename) as f:
             w.copy_from(f)
