@@ -117,7 +117,7 @@ def test_run_solver_from_an_lm_file(gpu, kind, tmp_path):
     w.close()
     first.close()
     cls = MpdRdmeSolver if kind == "byte" else IntMpdRdmeSolver
-    runSolver(lm, 4, cls(0))
+    runSolver(lm, 4, cls(0), checkpointInterval=1e-9)  # a checkpoint at every record
     direct, _ = _solver(kind, spec, "none", params, replicate=4)
     direct.generateTrajectory()
     with LMFile(lm) as f:
@@ -131,6 +131,12 @@ def test_run_solver_from_an_lm_file(gpu, kind, tmp_path):
             assert np.array_equal(f.lattice(4, i), row_major_frame(spec, fr))
         t3, c3 = f.species_counts(3)
         assert len(t3) == 1 + steps // ce and not np.array_equal(c3, c)  # replicate 3 kept, another seed
+    import os
+    with LMFile(lm + ".chk") as k:  # the last checkpoint: every species-count record
+        assert k.replicates() == [3, 4]
+        tk, ck = k.species_counts(4)
+        assert np.array_equal(tk, t) and np.array_equal(ck, c)
+    os.unlink(lm + ".chk")
     direct.close()
 
 
