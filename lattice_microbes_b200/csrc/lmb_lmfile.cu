@@ -31,6 +31,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -1209,9 +1210,14 @@ extern "C" int lmb_lmfile_create(const char *path, lmb_lmfile **out)
     f->fd = fd;
     f->path = path;
     // Chunk compression threads: up to 16, leaving two host cores to the
-    // thread that drives the GPU.
+    // thread that drives the GPU; LMB_LMFILE_THREADS sets the number.
     const unsigned hw = std::thread::hardware_concurrency();
-    f->pool.reset(new Pool(std::max(1u, std::min(16u, hw > 2 ? hw - 2 : 1u)) - 1));
+    unsigned nt = std::max(1u, std::min(16u, hw > 2 ? hw - 2 : 1u));
+    if (const char *e = getenv("LMB_LMFILE_THREADS")) {
+        const int v = atoi(e);
+        if (v >= 1 && v <= 256) nt = (unsigned)v;
+    }
+    f->pool.reset(new Pool(nt - 1));
     // The user block: "LMH5" and zeros (SimulationFile_create.cpp:119-128).
     const uint8_t ub[USER_BLOCK] = {'L', 'M', 'H', '5'};
     if (pwrite(fd, ub, sizeof(ub), 0) != (ssize_t)sizeof(ub)) f->io_error = LMB_E_IO;
