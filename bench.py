@@ -1,16 +1,17 @@
 #!/usr/bin/env python
-"""MPD-RDME throughput on the rod-cell oscillator workload (B200).
+"""MPD-RDME throughput on the crowded-cell workload (B200).
 
-One bench step = 500 MPD timesteps (x, y, z sweeps, reaction, overflow
-handling) of the 64x64x128 rod-cell model (16 nm, 3 site types, 5 species,
-8 reactions, 4000 D + 1400 E, ByteLattice 8 slots, tau = 25 us), a segment
-of that model's 50,000-timestep trajectory.  Inputs are seeded and synthetic
-(lattice_microbes_b200.configs.config1).  --workload crowded runs the
-128x128x256 IntLattice-16 crowded cell (configs.config2) the same way, 40
-timesteps per bench step; --workload batch / cme / serve run the batched,
-CME-ensemble and serving forms; --workload trajectory runs the rod-cell
-model as a trajectory written to a `.lm` file (species counts and a device
-lattice frame every 100 timesteps through the file's writer thread).
+One bench step = 40 MPD timesteps (x, y, z sweeps, reaction, overflow
+handling) of the 128x128x256 crowded cell (10 nm, 8 site types with 20 %
+obstacles, 200 species, 500 first- and second-order reactions, 1M particles,
+IntLattice 16 slots, tau = 10 us), a segment of that model's 5,000-timestep
+trajectory.  Inputs are seeded and synthetic (lattice_microbes_b200.configs.
+config2).  --workload rodcell runs the 64x64x128 rod-cell model (ByteLattice
+8 slots, configs.config1) the same way, 500 timesteps per bench step;
+--workload batch / cme / serve run the batched, CME-ensemble and serving
+forms; --workload trajectory runs the rod-cell model as a trajectory written
+to a `.lm` file (species counts and a device lattice frame every 100
+timesteps through the file's writer thread).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -20,12 +21,12 @@ the value is all ranks' site-steps over the slowest rank's device time.
 
 --impl reference times the reference's own CPU RDME solver on the host
 cores: lm::rdme::NextSubvolumeSolver compiled from the reference sources
-(oracle/_ref), one replicate of the same workload per host core as
-ReplicateRunner runs replicates, each bench step a bounded stretch of
-simulated time; its site-steps are sites x simulated time / tau.  The
-default run reports the same figure as cpu_baseline, and beside it the
-reference's MPD device functions compiled for the host (the reference has no
-CPU MPD solver of its own).
+(oracle/_ref), one trajectory of the same workload per host core as
+ReplicateRunner runs replicates, each bench step one stretch of simulated
+time timed by the trajectory's own species-count records; its site-steps are
+sites x simulated time / tau.  The default run reports the same figure as
+cpu_baseline, and beside it the reference's MPD device functions compiled
+for the host (the reference has no CPU MPD solver of its own).
 """
 import argparse
 import json
@@ -49,15 +50,19 @@ WORKLOADS = {
     "rodcell": dict(
         desc="rod-cell 64x64x128 ByteLattice-8, 3 site types, 5 species, 8 reactions, 5400 particles",
         config="config1", S=8, b=1, tau=25e-6, dtype="u8", timesteps_per_step=500, ref_timesteps=1000,
-        nsm_time=0.04, ref_mpd_timesteps=60,
+        nsm_seg=0.005, nsm_segments=8, ref_mpd_timesteps=60,
         l2="flushed between timed steps (256 MB write); working set 9 MB is L2-resident within a step"),
     "crowded": dict(
         desc="crowded cell 128x128x256 IntLattice-16, 8 site types (20% obstacles), 200 species, "
              "500 reactions, 1M particles",
         config="config2", S=16, b=4, tau=10e-6, dtype="u32", timesteps_per_step=40, ref_timesteps=100,
-        nsm_time=2e-5, ref_mpd_timesteps=2,
+        nsm_seg=1e-6, nsm_segments=20, ref_mpd_timesteps=2,
         l2="inputs larger than L2: 537 MB of particle buffers + 4 MB site types per timestep"),
 }
+
+
+# The largest single-GPU configuration: the crowded cell.
+DEFAULT_WORKLOAD = "crowded"
 
 
 def make_spec(workload, seed):
@@ -83,15 +88,15 @@ def parse():
     ap.add_argument("--cpu-sample-timesteps", type=int, default=0,
                     help="timesteps per core of the reference MPD functions on the host (0 = auto)")
     ap.add_argument("--cpu-sample-time", type=float, default=0.0,
-                    help="simulated seconds per core of the reference NextSubvolumeSolver (0 = auto)")
+                    help="simulated seconds per timed stretch of the reference NextSubvolumeSolver (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
-    ap.add_argument("--workload", choices=["rodcell", "crowded", "batch", "cme", "serve", "trajectory"],
-                    default="rodcell",
-                    help="rodcell: one 64x64x128 lattice (default); crowded: one 128x128x256 IntLattice-16; "
+    ap.add_argument("--workload", choices=["crowded", "rodcell", "batch", "cme", "serve", "trajectory"],
+                    default=DEFAULT_WORKLOAD,
+                    help="crowded: one 128x128x256 IntLattice-16 (default); rodcell: one 64x64x128 ByteLattice-8; "
                          "batch: 256 bimolecular replicates of "
                          "uneven size in one launch per timestep; cme: 65,536 two-state gene replicates "
                          "(direct method) to t = 3600 s; serve: a Poisson stream of solve requests; trajectory: "
@@ -181,44 +186,47 @@ def _byte_lattice(spec):
 
 def _nsm_worker(args):
     """One replicate of the reference NextSubvolumeSolver on one core
-    (spawned): a run to a tenth of a timestep (the solver's set-up: lattice,
-    queue, all subvolume propensities) and a run to `sim_time`; the
-    difference is the simulation itself."""
-    workload, seed, sim_time = args
+    (spawned): one trajectory of `segments` stretches of `seg_time` simulated
+    seconds, with a species-count record at the end of each.  The records'
+    wall-clock stamps time the stretches; the solver's set-up (lattice, queue,
+    every subvolume's propensities) comes before the first record and is not
+    timed."""
+    workload, seed, seg_time, segments = args
     sys.path.insert(0, ROOT)
     from tests import ref_cpu_lib
     if not ref_cpu_lib.available():
         return None
     spec = _byte_lattice(make_spec(workload, seed))
-    short = WORKLOADS[workload]["tau"] / 10
-    t0 = time.perf_counter()
-    ref_cpu_lib.nsm_run(spec, 1000 + seed, seed + 1, short, short)
-    t1 = time.perf_counter()
-    ref_cpu_lib.nsm_run(spec, 1000 + seed, seed + 1, sim_time, sim_time / 4)
-    t2 = time.perf_counter()
-    return t1 - t0, t2 - t1, spec.nsites
+    ref_cpu_lib.nsm_run(spec, 1000 + seed, seed + 1, seg_time * segments, seg_time)
+    walls = ref_cpu_lib.record_walls()
+    if len(walls) < segments + 1:
+        return None
+    return [float(x) for x in walls[:segments + 1]], spec.nsites
 
 
-def cpu_nsm_sample(workload, sim_time, cores):
+def cpu_nsm_sample(workload, seg_time, segments, skip, cores):
     """Reference NextSubvolumeSolver, `cores` replicates of the workload in
-    parallel; returns (site-steps/s, sample) with site-steps = sites x
-    simulated time / tau, set-up time excluded."""
+    parallel, each one trajectory of `segments` stretches of `seg_time`
+    simulated seconds, the first `skip` stretches untimed.  Returns
+    (site-steps/s, sample, per-stretch site-steps/s) with site-steps = sites x
+    simulated time / tau over the slowest core's wall time."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        res = pool.map(_nsm_worker, [(workload, s, sim_time) for s in range(cores)])
+        res = pool.map(_nsm_worker, [(workload, s, seg_time, segments) for s in range(cores)])
     if any(r is None for r in res):
-        return None, "reference CPU solvers not built (oracle/_ref)"
+        return None, "reference CPU solvers not built (oracle/_ref)", []
     tau = WORKLOADS[workload]["tau"]
-    short = tau / 10
-    wall = max(r[1] - r[0] for r in res)
-    setup = max(r[0] for r in res)
-    value = res[0][2] * ((sim_time - short) / tau) * cores / wall
-    sample = ("%d replicates of the %s workload, one per core, each %.4g s of simulated time (%d "
-              "MPD-timestep equivalents), reference NextSubvolumeSolver built from its sources; %.1f s wall "
-              "after the solver's set-up (%.1f s, excluded)" % (cores, workload, sim_time, round(sim_time / tau),
-                                                               wall, setup))
-    return value, sample
+    N = res[0][1]
+    timed = segments - skip
+    wall = max(r[0][segments] - r[0][skip] for r in res)
+    value = N * (timed * seg_time / tau) * cores / wall
+    per = [N * (seg_time / tau) * cores / max(r[0][k + 1] - r[0][k] for r in res) for k in range(skip, segments)]
+    sample = ("%d replicates of the %s workload, one per core, each one trajectory of %d stretches of %.4g s of "
+              "simulated time (%.4g MPD-timestep equivalents each), the first %d untimed; reference "
+              "NextSubvolumeSolver built from its sources; %.1f s wall over the timed stretches, the solver's "
+              "set-up excluded" % (cores, workload, segments, seg_time, seg_time / tau, skip, wall))
+    return value, sample, per
 
 
 # --------------------------------------------------------------------------
@@ -373,7 +381,8 @@ def run_ours(a):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = host_cores()
         with stdout_to_stderr():
-            val, sample = cpu_nsm_sample(a.workload, a.cpu_sample_time or w["nsm_time"], cores)
+            val, sample, _ = cpu_nsm_sample(a.workload, a.cpu_sample_time or w["nsm_seg"], w["nsm_segments"] + 1,
+                                            1, cores)
         if val is not None:
             cpu = {"value": val, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample}
         with stdout_to_stderr():
@@ -458,22 +467,32 @@ def run_ours(a):
     # ---- per-kernel device times (roofline of the dominant kernel) ----
     st, phase_ms, phase_n = lat.run_profiled(model, seed, step, T)
     step += T
+    # The profiled run brackets every launch with events (no graph replay), so
+    # its absolute times run long; only its shares are used, applied to the
+    # device-timed, graph-replayed bench step: per-launch times below sum to
+    # ms_per_step.
     names = ["sweep_x", "sweep_y", "sweep_z", "reaction", "overflow", "fused_step"]
     total_ms = float(phase_ms.sum())
-    phases = {names[k]: {"launches": int(phase_n[k]), "ms_per_launch": float(phase_ms[k]) / int(phase_n[k]),
-                         "share": float(phase_ms[k]) / total_ms}
+    step_ms = ms_total / a.steps                  # T timesteps, as the profiled run
+    phases = {names[k]: {"launches": int(phase_n[k]),
+                         "ms_per_launch": step_ms * float(phase_ms[k]) / total_ms / int(phase_n[k]),
+                         "share": float(phase_ms[k]) / total_ms,
+                         "profiled_ms_per_launch": float(phase_ms[k]) / int(phase_n[k])}
               for k in range(6) if phase_n[k] > 0}
     peak, peak_kind = measured_peak_hbm()
+    sweep_fraction = None
     if phase_n[5] > 0:
         kern = "fused_step_kernel (x, y, z sweeps + reaction + overflow, one timestep)"
-        launch_ms = float(phase_ms[5]) / int(phase_n[5])
+        launch_ms = phases["fused_step"]["ms_per_launch"]
         alg_bytes = N * B_STEP                 # site-steps per launch x per-site-step bytes
         own_bytes = N * B_SWEEP                # its own dataflow: read slots + site type, write slots
     else:
         kern = "sweep_kernel (x/y/z hop sweeps)"
-        launch_ms = float(phase_ms[:3].sum()) / max(1, int(phase_n[:3].sum()))
+        sweep_share = float(phase_ms[:3].sum()) / total_ms
+        launch_ms = step_ms * sweep_share / max(1, int(phase_n[:3].sum()))
         alg_bytes = N * B_SWEEP
         own_bytes = alg_bytes
+        sweep_fraction = alg_bytes / (launch_ms / 1e3) / 1e9 / peak
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     # ---- end to end through the public API with host buffers ----
     words = spec.words * N
@@ -532,11 +551,15 @@ def run_ours(a):
                 "own_dataflow_bytes_per_launch": own_bytes,
                 "own_dataflow_frac": own_bytes / (launch_ms / 1e3) / 1e9 / peak,
                 "peak_kind": peak_kind,
-                "note": ("achieved = algorithmic bytes of the reference schedule (B_step per site-step) per "
-                         "launch / launch time; own_dataflow_frac counts the fused kernel's single read and "
-                         "write of the lattice" + ("; working set 9 MB is L2-resident" if a.workload == "rodcell"
-                                                   else "")),
+                "note": (("achieved = N x B_step (reference-schedule bytes of a site-step) per fused launch / "
+                          "launch time; own_dataflow_frac counts the fused kernel's single read and write of the "
+                          "lattice" if phase_n[5] > 0 else
+                          "achieved = N x B_sweep per sweep launch / sweep launch time") +
+                         "; launch times are the device-timed step x the kernel's share of device time in an "
+                         "event-bracketed run" + ("; working set 9 MB is L2-resident" if a.workload == "rodcell"
+                                                  else "")),
                 "phases": phases,
+                "sweep_fraction": sweep_fraction,
                 "step_fraction_reference_schedule": value * B_STEP / (peak * 1e9),
             },
             "e2e": {
@@ -560,27 +583,24 @@ def run_ours(a):
 
 
 def run_reference(a):
+    """The reference's CPU RDME solver on the host cores, same workload and
+    metric as our arm: one NextSubvolumeSolver trajectory per core, each
+    bench step one stretch of simulated time (min(W, 1) untimed stretch
+    first), timed by the trajectory's own records."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    wname = a.workload if a.workload in WORKLOADS else "rodcell"
+    wname = a.workload if a.workload in WORKLOADS else DEFAULT_WORKLOAD
     w = WORKLOADS[wname]
     cores = host_cores()
-    sim_time = a.cpu_sample_time or w["nsm_time"] / 4
-    vals, samples = [], []
-    for _ in range(min(a.warmup, 1)):
-        with stdout_to_stderr():
-            cpu_nsm_sample(wname, sim_time / 4, cores)
-    for _ in range(a.steps):
-        with stdout_to_stderr():
-            v, s = cpu_nsm_sample(wname, sim_time, cores)
-        if v is None:
-            print(json.dumps({"impl": "reference", "unavailable": s}))
-            return
-        vals.append(v)
-        samples.append(s)
-    value = statistics.mean(vals)
+    seg = a.cpu_sample_time or w["nsm_seg"]
+    skip = min(a.warmup, 1)
+    with stdout_to_stderr():
+        value, sample, per = cpu_nsm_sample(wname, seg, a.steps + skip, skip, cores)
+    if value is None:
+        print(json.dumps({"impl": "reference", "unavailable": sample}))
+        return
     spec_sites = {"rodcell": 64 * 64 * 128, "crowded": 128 * 128 * 256}[wname]
     T = a.timesteps_per_step or w["timesteps_per_step"]
     line = {
@@ -600,7 +620,8 @@ def run_reference(a):
         "config": {"workload": w["desc"], "timesteps_per_step": T, "sites": spec_sites,
                    "parallelism": "host cores"},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "reference",
-                         "sample": samples[-1]},
+                         "sample": sample},
+        "per_step_values": per,
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

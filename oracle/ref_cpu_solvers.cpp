@@ -77,6 +77,7 @@ void reset_queue()
     q->counts.clear();
     q->numberSpecies = 0;
     q->latticeFrames = 0;
+    lm::io::record_walls().clear();
 }
 
 int copy_out(uint32_t ns, uint32_t max_entries, double *times, uint32_t *counts, uint32_t *entries)
@@ -211,6 +212,21 @@ int ref_gillespie_run(uint32_t ns, uint32_t nr, const uint32_t *init_counts, con
         set_error(err, errlen, e.what());
         return -1;
     }
+}
+
+/*
+ * Wall-clock stamps (steady clock, seconds) of the species-count records of
+ * the last trajectory run on this thread, one per record in record order:
+ * entry 0 is the record at t = 0, taken after the solver's set-up, and entry
+ * k the record at k write intervals.  Returns how many there were; copies at
+ * most max_entries.
+ */
+uint32_t ref_record_walls(double *walls, uint32_t max_entries)
+{
+    const std::vector<double> &w = lm::io::record_walls();
+    const size_t m = w.size() < max_entries ? w.size() : max_entries;
+    if (walls && m) memcpy(walls, w.data(), m * sizeof(double));
+    return (uint32_t)w.size();
 }
 
 }  // extern "C"

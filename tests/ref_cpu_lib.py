@@ -40,6 +40,8 @@ def lib():
             C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double, u8p, u8p,
             C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_uint32, f64p, u32p, u32p, u8p,
             C.c_char_p, C.c_size_t]
+        L.ref_record_walls.restype = C.c_uint32
+        L.ref_record_walls.argtypes = [f64p, C.c_uint32]
         L.ref_gillespie_run.restype = C.c_int
         L.ref_gillespie_run.argtypes = [
             C.c_uint32, C.c_uint32, u32p, u32p, f64p, C.c_uint32, i32p, u32p, C.c_uint32, C.c_uint32,
@@ -95,6 +97,17 @@ def nsm_run(spec, seed, replicate, max_time, write_interval, final_lattice=False
     n = int(entries[0])
     out = (times[:n], counts[:n])
     return out + (fin,) if final_lattice else out
+
+
+def record_walls():
+    """Wall-clock seconds (steady clock) at which the last trajectory run on
+    this thread took each species-count record: entry 0 follows the solver's
+    set-up, entry k is the record at k write intervals."""
+    L = lib()
+    n = L.ref_record_walls(None, 0)
+    w = np.zeros(max(n, 1), dtype=np.float64)
+    L.ref_record_walls(_p(w, f64p), n)
+    return w[:n]
 
 
 def gillespie_run(ns, rtype, K, S, D, init, seed, replicate, max_time, write_interval):

@@ -85,3 +85,36 @@ def test_reference_kernels_config1_short(gpu):
     ours, rc, st = _ours(spec, spec.lattice, spec.sites, 77, 0, 200, from_spec=True)
     assert rc == 0
     assert np.array_equal(ours, g)
+
+
+@pytest.mark.parametrize("schedule", ["phases", "fused"])
+def test_reference_kernels_config2_full_size(gpu, schedule):
+    """The crowded cell at full size (128x128x256 IntLattice-16, 8 site types,
+    200 species, 500 reactions, 1M particles), 30 timesteps: the reference
+    kernels and ours give the same lattice, with no overflow on either side
+    (an overflow's reinsertion order is not deterministic in the reference)."""
+    _need("int", 16)
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import Context, Lattice, Model
+    spec = configs.config2(seed=3)
+    t = oracle_tables(spec)
+    g, rc_g, ovf_g = reference_gpu_run(t, spec.lattice, spec.sites, 5150, 0, 30)
+    assert rc_g == 0 and ovf_g == 0
+    assert not np.array_equal(g, spec.lattice)
+    ctx = Context(0)
+    m = Model.from_spec(ctx, spec)
+    lat = Lattice(ctx, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+    lat.set_native(spec.lattice, spec.sites)
+    if schedule == "phases":
+        lat.set_schedule(L.LMB_SCHEDULE_PHASES)
+    else:
+        lat.set_schedule(L.LMB_SCHEDULE_FUSED, 1, 1)  # the one tile of 128-site Int-16 rows that fits
+    rc, st = lat.run(m, 5150, 0, 30, check=False)
+    out, _ = lat.get_native()
+    lat.close()
+    m.close()
+    ctx.close()
+    assert rc == 0
+    assert st.overflows == 0
+    assert st.reactions > 0
+    assert np.array_equal(out, g)
