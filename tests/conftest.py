@@ -8,7 +8,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE_SRC = "/root/reference/src"
+# The reference source tree the checkers under oracle/_ref are built from
+# (the same variable oracle/Makefile reads); absent on machines that only
+# run the prebuilt checkers.
+REFERENCE_SRC = os.path.join(os.environ.get("REFERENCE", "/root/reference"), "src")
 
 
 def pytest_configure(config):
