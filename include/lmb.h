@@ -197,7 +197,10 @@ int lmb_lattice_species_counts(lmb_lattice *lattice, uint32_t number_species, ui
  * LMB_E_UNSUPPORTED.  The first call on a device looks up that array's
  * address, so make it before any stream capture.  Each call clears the array
  * on `cuda_stream` before counting and waits for the result; calls whose
- * work overlaps on the GPU share the array and race. */
+ * work overlaps on the GPU share the array and race.  The looked-up address
+ * is kept for the life of the process: after cudaDeviceReset on a device
+ * (which ends every lmb handle on it too) this entry point must not be
+ * called on that device again. */
 #define LMB_NOALLOC_MAX_SPECIES 4095
 int lmb_species_counts_noalloc(const uint32_t *particles, uint32_t X, uint32_t Y, uint32_t Z,
                                uint32_t particles_per_site, uint32_t bytes_per_particle, uint32_t number_species,

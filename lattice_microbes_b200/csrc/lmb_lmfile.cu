@@ -234,6 +234,13 @@ struct Node {
     // that has not changed since (every frame, once stored) keeps it.
     uint64_t header = UNDEF, btree = UNDEF, heap = UNDEF;
     bool dirty = true;
+    // Extendable datasets: rows stored by the last flush, and how many leading
+    // chunks were full then (rows are only appended, so those chunks stay as
+    // they are).  Groups: what the last flush wrote them from (member names,
+    // member header / B-tree / heap addresses, attributes).
+    uint64_t written_rows = UINT64_MAX;
+    size_t full_chunks = 0;
+    std::string written_as;
 };
 
 // A frame for the writer thread: a host row-major copy (host calls), or a
@@ -804,9 +811,25 @@ uint64_t header(lmb_lmfile *f, const std::vector<std::pair<uint16_t, Bytes>> &ms
 
 void write_node(lmb_lmfile *f, Node &n);
 
+// A group is written again only when a member was added or rewritten (its
+// header, B-tree or heap moved) or an attribute changed; otherwise its header,
+// heap and B-tree stay where the last flush put them.
 void write_group(lmb_lmfile *f, Node &g)
 {
     for (auto &c : g.children) write_node(f, *c.second);
+    std::string as;
+    for (auto &c : g.children) {
+        as += c.first;
+        as.push_back('\0');
+        const uint64_t a[3] = {c.second->header, c.second->btree, c.second->heap};
+        as.append((const char *)a, sizeof a);
+    }
+    for (auto &a : g.attrs) {
+        const Bytes b = attribute(a);
+        as.append((const char *)b.v.data(), b.size());
+    }
+    if (g.header != UNDEF && as == g.written_as) return;
+    g.written_as = std::move(as);
     // Local heap: "" at offset 0, then each name, 8-byte aligned.
     Bytes data;
     data.zeros(8);
@@ -870,7 +893,7 @@ void write_group(lmb_lmfile *f, Node &g)
 
 void write_dataset(lmb_lmfile *f, Node &d)
 {
-    if (!d.dirty && !d.extendable && d.header != UNDEF) return;
+    if (!d.dirty && d.header != UNDEF && (!d.extendable || d.written_rows == d.dims[0])) return;
     d.dirty = false;
     const size_t esize = type_size(d.type, 0);
     if (d.extendable) {
@@ -881,9 +904,12 @@ void write_dataset(lmb_lmfile *f, Node &d)
         // other dimensions is stored with full-width chunks.)
         for (size_t i = 1; i < d.dims.size(); i++) d.chunk_dims[i] = std::max<uint64_t>(1, d.dims[i]);
         const uint64_t per = d.chunk_dims[0];
-        d.chunks.clear();
+        // Chunks that were full at an earlier flush are kept; the partial
+        // last one and any new ones are appended.
+        if (d.full_chunks > d.chunks.size()) d.full_chunks = d.chunks.size();
+        d.chunks.resize(d.full_chunks);
         std::vector<uint8_t> buf(per * row);
-        for (uint64_t r0 = 0; r0 < d.dims[0]; r0 += per) {
+        for (uint64_t r0 = d.full_chunks * per; r0 < d.dims[0]; r0 += per) {
             std::fill(buf.begin(), buf.end(), 0);
             const uint64_t n = std::min<uint64_t>(per, d.dims[0] - r0);
             memcpy(buf.data(), d.rows.data() + r0 * row, n * row);
@@ -891,6 +917,8 @@ void write_dataset(lmb_lmfile *f, Node &d)
             off[0] = r0;
             d.chunks.push_back({off, append(f, buf.data(), buf.size()), (uint32_t)buf.size()});
         }
+        d.full_chunks = (size_t)(d.dims[0] / per);
+        d.written_rows = d.dims[0];
     }
     std::vector<std::pair<uint16_t, Bytes>> msgs;
     msgs.push_back({0x0001, dataspace(d.dims, d.extendable)});
@@ -1172,8 +1200,16 @@ int append_device(lmb_lmfile *f, uint32_t rep, double time, lmb_lattice *lat, bo
     if (e == cudaSuccess) e = cudaMemcpyAsync(p.host, p.dev, bytes, cudaMemcpyDeviceToHost, f->copy);
     if (e == cudaSuccess) e = cudaEventRecord(p.ready, f->copy);
     if (e != cudaSuccess) {
-        std::lock_guard<std::mutex> lk(f->qmu);
-        p.busy = false;
+        // Work already queued on either stream may still write the slot's
+        // buffers: wait for both streams before the slot is handed out again,
+        // and wake a thread waiting for a free slot.
+        cudaStreamSynchronize(st);
+        cudaStreamSynchronize(f->copy);
+        {
+            std::lock_guard<std::mutex> lk(f->qmu);
+            p.busy = false;
+        }
+        f->qcv.notify_all();
         return LMB_E_CUDA;
     }
     FrameJob j;

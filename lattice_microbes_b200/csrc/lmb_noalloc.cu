@@ -14,7 +14,10 @@
 // exists once per device for the whole process, from the first use of the
 // library on that device until exit.  The first call on a device looks up the
 // array's device address (cudaGetSymbolAddress), so that call should come
-// before any stream capture on that device.  Every call zeroes it on the stream
+// before any stream capture on that device.  The address is kept until exit; a
+// cudaDeviceReset reloads the module, possibly elsewhere, so the entry point is
+// not usable on a device after it has been reset (as no lmb handle on that
+// device is).  Every call zeroes it on the stream
 // before counting, so a call never sees the previous call's totals; two calls
 // whose work overlaps on the GPU (different streams, no ordering between
 // them) write the same array and race.

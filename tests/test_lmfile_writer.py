@@ -240,3 +240,40 @@ def test_oversized_attribute_is_refused(tmp_path):
         w.set_parameter("short", "y" * 60000)
     with LMFile(p) as f:
         assert f.parameters() == {"short": "y" * 60000}
+
+
+def test_repeated_flushes_grow_the_file_linearly(tmp_path):
+    """Flushes and checkpoints re-append only what changed: chunks of species
+    count rows that were full at an earlier flush stay where they are, and
+    groups no record touched keep their headers.  K flushes over R records
+    add at most about one row chunk and a fixed amount of metadata per flush
+    to the size a single flush gives, independent of R."""
+    rng = np.random.default_rng(3)
+    ns, R, every = 50, 2000, 10
+    times = np.arange(R) * 0.5
+    counts = rng.integers(0, 1000, (R, ns))
+    one = str(tmp_path / "one.lm")
+    with LMFileWriter(one) as w:
+        w.append_lattice(1, 0.0, np.ones((8, 8, 8, 8), np.uint8))
+        w.append_species_counts(1, times, counts)
+        w.flush()
+    many = str(tmp_path / "many.lm")
+    K = 0
+    with LMFileWriter(many) as w:
+        w.append_lattice(1, 0.0, np.ones((8, 8, 8, 8), np.uint8))
+        for r0 in range(0, R, every):
+            w.append_species_counts(1, times[r0:r0 + every], counts[r0:r0 + every])
+            if (r0 // every) % 50 == 49:
+                w.checkpoint()
+            else:
+                w.flush()
+            K += 1
+    row_chunk = 100 * (4 * ns + 8)
+    grown = os.path.getsize(many) - os.path.getsize(one)
+    assert grown <= K * (row_chunk + 24 * 1024), (grown, K)
+    with LMFile(many) as f:
+        t, c = f.species_counts(1)
+        assert np.array_equal(t, times) and np.array_equal(c, counts)
+    with LMFile(many + ".chk") as f:
+        t, c = f.species_counts(1)
+        assert np.array_equal(t, times[:len(t)]) and len(t) == 2000
