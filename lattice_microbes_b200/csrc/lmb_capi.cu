@@ -68,6 +68,10 @@ struct lmb_lattice {
     // chosen).
     uint32_t *rx_sites;
     uint32_t rx_cap;
+    // Per-phase schedule, X a multiple of 32: plane bounds of buf[0] (first
+    // nseg words) and buf[1] (next nseg), one per segment of 32 sites.
+    uint32_t *pb;
+    uint32_t nseg;
     unsigned long long *counts_dev;
     uint32_t counts_len;
     bool validated;
@@ -626,6 +630,14 @@ extern "C" int lmb_lattice_set_schedule(lmb_lattice *l, int schedule, uint32_t T
             CK(cudaMalloc(&l->rx_sites, (size_t)cap * 2 * sizeof(uint32_t)));
             l->rx_cap = cap;
         }
+        // Plane bounds need every warp of a sweep tile to hold one whole
+        // segment: x rows a multiple of 32 sites.
+        if (!l->pb && l->g.X % 32u == 0) {
+            CK(cudaSetDevice(l->ctx->device));
+            const uint32_t nseg = l->g.N >> PB_SHIFT;
+            CK(cudaMalloc(&l->pb, (size_t)nseg * 2 * sizeof(uint32_t)));
+            l->nseg = nseg;
+        }
         l->schedule = schedule;
         return LMB_OK;
     }
@@ -659,6 +671,7 @@ extern "C" int lmb_lattice_destroy(lmb_lattice *l)
     if (l->rs) cudaFree(l->rs);
     if (l->list) cudaFree(l->list);
     if (l->rx_sites) cudaFree(l->rx_sites);
+    if (l->pb) cudaFree(l->pb);
     if (l->counts_dev) cudaFree(l->counts_dev);
     if (l->rs_host) cudaFreeHost(l->rs_host);
     for (auto &gr : l->graph)
@@ -811,6 +824,9 @@ extern "C" int lmb_lattice_species_counts(lmb_lattice *l, uint32_t ns, uint64_t 
 
 static const uint32_t GRAPH_STEPS = 32;  // even: a replay returns to the same buffer parity
 
+// Plane bounds of buffer b, or null when the lattice keeps none.
+static uint32_t *plane_bounds(lmb_lattice *l, int b) { return l->pb ? l->pb + (size_t)b * l->nseg : nullptr; }
+
 // Queues one timestep (schedule of the lattice) and flips the buffer index.
 static cudaError_t enqueue_step(lmb_lattice *l, lmb_model *m, cudaStream_t st)
 {
@@ -823,20 +839,30 @@ static cudaError_t enqueue_step(lmb_lattice *l, lmb_model *m, cudaStream_t st)
         return e;
     }
     uint32_t *rx = m->nr > 0 ? l->rx_sites : nullptr;
-    if ((e = launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, st)) !=
-        cudaSuccess)
+    uint32_t *pa = plane_bounds(l, l->cur), *pbb = plane_bounds(l, l->cur ^ 1);
+    if ((e = launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, pa, pbb,
+                          st)) != cudaSuccess)
         return e;
-    if ((e = launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, st)) !=
-        cudaSuccess)
+    if ((e = launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, pbb, pa,
+                          st)) != cudaSuccess)
         return e;
-    if ((e = launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap, st)) !=
-        cudaSuccess)
+    if ((e = launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap, pa, pbb,
+                          st)) != cudaSuccess)
         return e;
     l->cur ^= 1;
     if (m->nr > 0 && (e = launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap,
-                                          rx, l->rx_cap, st)) != cudaSuccess)
+                                          rx, l->rx_cap, pbb, st)) != cudaSuccess)
         return e;
-    return launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, rx ? l->rx_cap : 0, st);
+    return launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, rx ? l->rx_cap : 0, pbb,
+                          st);
+}
+
+// Both buffers' plane bounds set to every plane: the start of a per-phase
+// run, whatever was written to the buffers since the last one.
+static cudaError_t reset_plane_bounds(lmb_lattice *l, cudaStream_t st)
+{
+    if (!l->pb || l->schedule != LMB_SCHEDULE_PHASES) return cudaSuccess;
+    return launch_fill_bounds(l->pb, 2 * l->nseg, l->words, st);
 }
 
 // Captures GRAPH_STEPS timesteps starting at the current buffer parity, or
@@ -927,6 +953,7 @@ extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed,
     int rc = validate_for_model(l, m);
     if (rc) return rc;
     CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream));
+    CK(reset_plane_bounds(l, c->stream));
     l->pending_cur0 = l->cur;
     uint32_t done = 0;
     // Whole graphs of GRAPH_STEPS timesteps, then single launches.
@@ -991,6 +1018,7 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
     int rc = validate_for_model(l, m);
     if (rc) return rc;
     CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream));
+    CK(reset_plane_bounds(l, c->stream));
     std::vector<cudaEvent_t> ev((size_t)n * 12);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     const int bps = (int)l->bps, S = (int)l->slots;
@@ -1009,22 +1037,26 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
         }
         CK(cudaEventRecord(E[0], c->stream));
         uint32_t *rx = m->nr > 0 ? l->rx_sites : nullptr;
-        CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, c->stream));
+        uint32_t *pa = plane_bounds(l, l->cur), *pbb = plane_bounds(l, l->cur ^ 1);
+        CK(launch_sweep(bps, S, 0, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, pa, pbb,
+                        c->stream));
         CK(cudaEventRecord(E[1], c->stream));
         CK(cudaEventRecord(E[2], c->stream));
-        CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, c->stream));
+        CK(launch_sweep(bps, S, 1, b, a, l->sites, l->g, m->dev, l->rs, l->list, l->cap, nullptr, 0, pbb, pa,
+                        c->stream));
         CK(cudaEventRecord(E[3], c->stream));
         CK(cudaEventRecord(E[4], c->stream));
-        CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap, c->stream));
+        CK(launch_sweep(bps, S, 2, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap, pa, pbb,
+                        c->stream));
         CK(cudaEventRecord(E[5], c->stream));
         l->cur ^= 1;
         CK(cudaEventRecord(E[6], c->stream));
         if (m->nr > 0)
             CK(launch_reaction(bps, S, l->buf[l->cur], l->sites, l->g, m->dev, l->rs, l->list, l->cap, rx, l->rx_cap,
-                               c->stream));
+                               pbb, c->stream));
         CK(cudaEventRecord(E[7], c->stream));
         CK(cudaEventRecord(E[8], c->stream));
-        CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, rx ? l->rx_cap : 0,
+        CK(launch_resolve(bps, S, l->buf[l->cur], l->sites, l->g, l->rs, l->list, l->cap, rx ? l->rx_cap : 0, pbb,
                           c->stream));
         CK(cudaEventRecord(E[9], c->stream));
     }

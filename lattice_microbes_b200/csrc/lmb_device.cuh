@@ -92,6 +92,22 @@ struct SiteWords {
             }
         }
     }
+    // Loads words 0 .. nw - 1 through the read-only path and clears the
+    // rest: a site whose words from nw on are known to be zero (a plane
+    // bound), in a buffer nothing writes during the kernel.
+    __device__ __forceinline__ void load_planes(const uint32_t *__restrict__ lat, uint32_t N, uint32_t i,
+                                                uint32_t nw)
+    {
+#pragma unroll
+        for (int k = 0; k < W; k++) w[k] = (uint32_t)k < nw ? __ldg(lat + (size_t)k * N + i) : 0u;
+    }
+    // Stores words 0 .. nw - 1.
+    __device__ __forceinline__ void store_first(uint32_t *lat, uint32_t N, uint32_t i, uint32_t nw) const
+    {
+#pragma unroll
+        for (int k = 0; k < W; k++)
+            if ((uint32_t)k < nw) lat[(size_t)k * N + i] = w[k];
+    }
     // Loads words 0 .. nw - 1 (independent loads) and clears the rest: a
     // packed site whose particle count is known.
     __device__ __forceinline__ void load_first(const uint32_t *lat, uint32_t N, uint32_t i, uint32_t nw)

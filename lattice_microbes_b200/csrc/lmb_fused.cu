@@ -533,7 +533,7 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     if (s_last) {
         __threadfence();
         if (tid == 0) rs->tiles_done = 0;
-        resolve_block_flat<BPS, S>(dst, sites, g, rs, list, cap, (OverflowEntry *)smem, tid, nthr);
+        resolve_block_flat<BPS, S>(dst, sites, g, rs, list, cap, (OverflowEntry *)smem, tid, nthr, nullptr);
     }
 }
 

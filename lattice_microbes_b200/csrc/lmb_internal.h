@@ -92,23 +92,42 @@ struct RunState {
     uint32_t rx_skip;     // timesteps left to run without the list (it overflowed recently)
 };
 
+// Plane bounds (per-phase schedule, lattices whose X is a multiple of 32):
+// for each segment of 32 consecutive sites (site i in segment i >> PB_SHIFT),
+// and for each of a lattice's two buffers, a count of word planes such that
+// every word of those sites in planes at or above it is zero.  Sites are
+// packed by every sweep and the reaction, so a segment's bound is the largest
+// number of words any of its sites uses; a larger bound is always allowed.
+// A sweep reads only the planes below its source segment's bound and writes
+// the planes below the larger of its new bound and the destination's old one
+// (clearing what the destination held above the new content), then stores the
+// new bound.  The reaction and overflow reinsertion raise a bound when they
+// fill a slot above it.  Both buffers' bounds are set to the full plane count
+// at the start of every run, so the first sweep reads and writes every plane.
+constexpr uint32_t PB_SHIFT = 5;
+
 // Kernel launchers (lmb_kernels.cu).  Each returns a cudaError_t.
 // The z sweep (dim 2) lists in rx_sites the sites whose reaction step could
 // change them, when rx_sites is given (rx_cap entries of two words: the site
 // and its type << 8 | particle count); launch_reaction then visits only
 // those (every site when the list is absent or overflowed rx_cap).
+// pb_src / pb_dst (sweeps) and pb (reaction, resolution): the plane bounds of
+// the buffers read and written, or null when the lattice keeps none.
 cudaError_t launch_sweep(int bytes_per_slot, int slots, int dim, const uint32_t *src, uint32_t *dst,
                          const uint8_t *sites, const Geometry &g, const DevTables &m, RunState *rs,
                          OverflowEntry *list, uint32_t cap, uint32_t *rx_sites, uint32_t rx_cap,
-                         cudaStream_t stream);
+                         const uint32_t *pb_src, uint32_t *pb_dst, cudaStream_t stream);
 cudaError_t launch_reaction(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
                             const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list,
-                            uint32_t cap, const uint32_t *rx_sites, uint32_t rx_cap, cudaStream_t stream);
+                            uint32_t cap, const uint32_t *rx_sites, uint32_t rx_cap, uint32_t *pb,
+                            cudaStream_t stream);
 // Also closes the timestep's reaction list (rx_cap: its capacity, 0 when
 // there is none).
 cudaError_t launch_resolve(int bytes_per_slot, int slots, uint32_t *lat, const uint8_t *sites,
                            const Geometry &g, RunState *rs, OverflowEntry *list, uint32_t cap, uint32_t rx_cap,
-                           cudaStream_t stream);
+                           uint32_t *pb, cudaStream_t stream);
+// Sets `count` plane bounds to `planes`.
+cudaError_t launch_fill_bounds(uint32_t *pb, uint32_t count, uint32_t planes, cudaStream_t stream);
 cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
                              cudaStream_t stream);
 cudaError_t launch_begin_batch(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,

@@ -119,13 +119,45 @@ __device__ __forceinline__ void list_for_reaction(uint32_t n, uint32_t t, uint32
     if (idx < rx_cap) reinterpret_cast<uint2 *>(rx_sites)[idx] = make_uint2(i, (t << 8) | n);
 }
 
+// Planes of site i's segment that may hold particles (all W without plane
+// bounds).
+template <int W>
+__device__ __forceinline__ uint32_t planes_at(const uint32_t *__restrict__ pb, uint32_t i)
+{
+    if (!pb) return (uint32_t)W;
+    const uint32_t b = __ldg(pb + (i >> PB_SHIFT));
+    return b < (uint32_t)W ? b : (uint32_t)W;
+}
+
+// Writes the warp's new sites with plane bounds: every lane of the warp holds
+// one site of the same segment (nw: words its new content uses; `word(k)`:
+// word k of it).  Planes below the larger of the warp's new bound and the
+// destination's old one are written (zeros above a site's content), then the
+// new bound replaces the old.
+template <int W, typename WordFn>
+__device__ __forceinline__ void store_bounded(uint32_t *__restrict__ dst, uint32_t *__restrict__ pb_dst,
+                                              uint32_t N, uint32_t i, uint32_t nw, WordFn word)
+{
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, nw);
+    const uint32_t seg = i >> PB_SHIFT;
+    const uint32_t old = pb_dst[seg];
+    const uint32_t lim = wmax > old ? wmax : (old < (uint32_t)W ? old : (uint32_t)W);
+#pragma unroll
+    for (int k = 0; k < W; k++)
+        if ((uint32_t)k < lim) dst[(size_t)k * N + i] = word(k);
+    __syncwarp();
+    if ((threadIdx.x & 31u) == 0) pb_dst[seg] = wmax;
+}
+
 template <int BPS, int S, int DIM>
 __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t *__restrict__ src,
                                                                   uint32_t *__restrict__ dst,
                                                                   const uint8_t *__restrict__ sites, Geometry g,
                                                                   DevTables m, RunState *__restrict__ rs,
                                                                   OverflowEntry *__restrict__ list, uint32_t cap,
-                                                                  uint32_t *__restrict__ rx_sites, uint32_t rx_cap)
+                                                                  uint32_t *__restrict__ rx_sites, uint32_t rx_cap,
+                                                                  const uint32_t *__restrict__ pb_src,
+                                                                  uint32_t *__restrict__ pb_dst)
 {
     using Code = typename ChoiceCode<S>::type;
     constexpr int W = SiteWords<BPS, S>::W;
@@ -149,7 +181,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
     uint32_t occ = 0;
     if (in) {
         sweep_neighbours<DIM>(g, x, y, z, lid, i, im, ip, lm, lp);
-        own.load(src, g.N, i);
+        own.load_planes(src, g.N, i, planes_at<W>(pb_src, i));
         t = __ldg(sites + i);
         tm = __ldg(sites + im);
         tp = __ldg(sites + ip);
@@ -262,7 +294,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
             c_mn = sc[lm];
         } else {
             SiteWords<BPS, S> mn;
-            mn.load(src, g.N, im);
+            mn.load_planes(src, g.N, im, planes_at<W>(pb_src, im));
             const uint32_t o = occupied_slots<BPS, S>(mn);
             if (o) c_mn = choices_mem(im, o, tm, __ldg(sites + outer_minus()), t);
         }
@@ -270,7 +302,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
             c_pl = sc[lp];
         } else {
             SiteWords<BPS, S> pl;
-            pl.load(src, g.N, ip);
+            pl.load_planes(src, g.N, ip, planes_at<W>(pb_src, ip));
             const uint32_t o = occupied_slots<BPS, S>(pl);
             if (o) c_pl = choices_mem(ip, o, tp, t, __ldg(sites + outer_plus()));
         }
@@ -298,8 +330,13 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
             in_p &= in_p - 1;
             push(DIM != 0 || lp >= 0 ? sw[k][lp] : __ldg(src + (size_t)k * g.N + ip));
         }
+        if (pb_dst) {
+            store_bounded<W>(dst, pb_dst, g.N, i, n < (uint32_t)S ? n : (uint32_t)S,
+                             [&](int k) { return (uint32_t)k < n ? so[k][oid] : 0u; });
+        } else {
 #pragma unroll
-        for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][oid] : 0u;
+            for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][oid] : 0u;
+        }
         if (DIM == 2 && rx_sites && listing)
             list_for_reaction(n < (uint32_t)S ? n : (uint32_t)S, t, i, lid, m, rs, rx_sites, rx_cap);
     } else {
@@ -311,7 +348,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
             for (int k = 0; k < W; k++) mn.w[k] = sw[k][lm];
             c_mn = sc[lm];
         } else {
-            mn.load(src, g.N, im);
+            mn.load_planes(src, g.N, im, planes_at<W>(pb_src, im));
             if (!mn.empty()) c_mn = site_choices<BPS, S>(mn, tm, __ldg(sites + outer_minus()), t, im, th, m);
         }
         if (DIM != 0 || lp >= 0) {
@@ -319,15 +356,177 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
             for (int k = 0; k < W; k++) pl.w[k] = sw[k][lp];
             c_pl = sc[lp];
         } else {
-            pl.load(src, g.N, ip);
+            pl.load_planes(src, g.N, ip, planes_at<W>(pb_src, ip));
             if (!pl.empty()) c_pl = site_choices<BPS, S>(pl, tp, t, __ldg(sites + outer_plus()), ip, th, m);
         }
         const SiteWords<BPS, S> out = assemble_site<BPS, S>(own, c_own, mn, c_mn, pl, c_pl, i, true,
                                                             (uint32_t)DIM + 1, rs, list, cap);
-        out.store(dst, g.N, i);
-        if (DIM == 2 && rx_sites && listing)
-            list_for_reaction((uint32_t)__popc(occupied_slots<BPS, S>(out)), t, i, lid, m, rs, rx_sites, rx_cap);
+        const uint32_t n_out = (uint32_t)__popc(occupied_slots<BPS, S>(out));
+        if (pb_dst) store_bounded<W>(dst, pb_dst, g.N, i, (n_out + 3u) >> 2, [&](int k) { return out.w[k]; });
+        else out.store(dst, g.N, i);
+        if (DIM == 2 && rx_sites && listing) list_for_reaction(n_out, t, i, lid, m, rs, rx_sites, rx_cap);
     }
+}
+
+// ---------------------------------------------------------------------------
+// IntLattice sweep with plane bounds
+// ---------------------------------------------------------------------------
+
+// y and z tiles of the plane-bounded sweep: 16 sites along the axis plus a
+// halo row on either side, 32 sites (one segment) across.
+constexpr int SWEEP_PB_TILE = 16;
+constexpr int SWEEP_PB_YZ_THREADS = 32 * (SWEEP_PB_TILE + 2);
+
+// The rule of sweep_kernel's IntLattice path for lattices that keep plane
+// bounds (X a multiple of 32: every warp holds the 32 sites of one segment of
+// one x row).  A thread moves only the word planes below its segment's bound,
+// in loops whose trip count the whole warp shares: it stages its own site's
+// words in shared memory as they arrive, writes each particle of its new site
+// straight to the destination as it is placed, then clears its planes from
+// its new content up to the larger of the warp's new bound and the
+// destination's old one, and the warp stores its new bound.
+template <int S, int DIM, int NT>
+__global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 2)
+    sweep_int_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, const uint8_t *__restrict__ sites,
+                     Geometry g, DevTables m, RunState *__restrict__ rs, OverflowEntry *__restrict__ list,
+                     uint32_t cap, uint32_t *__restrict__ rx_sites, uint32_t rx_cap,
+                     const uint32_t *__restrict__ pb_src, uint32_t *__restrict__ pb_dst)
+{
+    using Code = typename ChoiceCode<S>::type;
+    constexpr int CB = CountBits<S>::value;
+    constexpr uint32_t LOW = (1u << S) - 1u;
+    __shared__ uint32_t sw[S][NT];
+    __shared__ Code sc[NT];
+    if (rs->status != LMB_OK) return;
+    const bool listing = DIM == 2 && rx_sites && rs->rx_skip == 0;
+    uint32_t x, y, z;
+    bool in, out;
+    sweep_site_of<DIM>(g, x, y, z, in, out);
+    const int lid = (int)(threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z));
+    const uint32_t lane = (uint32_t)lid & 31u;
+    uint32_t i = 0, im = 0, ip = 0;
+    int lm = -1, lp = -1;
+    uint32_t t = 0, tm = 0, tp = 0, occ = 0;
+    const unsigned long long th = timestep_hash(rs->seed, rs->step, DIM);
+    if (in) {
+        sweep_neighbours<DIM>(g, x, y, z, lid, i, im, ip, lm, lp);
+        const uint32_t npl = planes_at<S>(pb_src, i);
+        for (uint32_t k = 0; k < npl; k++) {
+            const uint32_t v = __ldg(src + (size_t)k * g.N + i);
+            sw[k][lid] = v;
+            occ |= (v != 0u ? 1u : 0u) << k;
+        }
+        t = __ldg(sites + i);
+        tm = __ldg(sites + im);
+        tp = __ldg(sites + ip);
+    }
+    sc[lid] = 0;
+    __syncwarp();
+    // The warp's particles drawn together, particle q (site, then slot
+    // order) on lane q % 32, as in sweep_kernel.
+    {
+        const uint32_t wbase = (uint32_t)lid & ~31u;
+        const uint32_t cnt = __popc(occ);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - cnt;
+        for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t q = base + lane;
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t step = 16; step >= 1; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xffffffffu, excl, (o + step) & 31u);
+                if (o + step < 32 && e <= q) o += step;
+            }
+            const uint32_t occ_o = __shfl_sync(0xffffffffu, occ, o);
+            const uint32_t j = q - __shfl_sync(0xffffffffu, excl, o);
+            const uint32_t t_o = __shfl_sync(0xffffffffu, t, o), tm_o = __shfl_sync(0xffffffffu, tm, o);
+            const uint32_t tp_o = __shfl_sync(0xffffffffu, tp, o), gi_o = __shfl_sync(0xffffffffu, i, o);
+            if (q < total) {
+                uint32_t mbits = occ_o;
+                for (uint32_t r = 0; r < j; r++) mbits &= mbits - 1;
+                const uint32_t k = __ffs(mbits) - 1;
+                const uint32_t so = wbase + o;
+                const uint32_t p = sw[k][so];
+                const float rv = hash_float(((unsigned long long)gi_o << CB) | k, th);
+                Code bit = 0;
+                if ((rv >= 0.5f) && (rv < __fadd_rn(lookup_T(m, p, t_o, tp_o), 0.5f))) bit = (Code)1 << (S + k);
+                else if (rv < lookup_T(m, p, t_o, tm_o)) bit = (Code)1 << k;
+                if (bit) atomicOr(&sc[so], bit);
+            }
+        }
+    }
+    __syncthreads();
+    if (!out) return;
+    const Code c_own = sc[lid];
+    // Neighbours outside the tile (ends of x rows longer than the block):
+    // their occupied slots and choices, drawn here.
+    auto outside = [&](uint32_t idx, uint32_t t_n, uint32_t tm_n, uint32_t tp_n) {
+        const uint32_t npl = planes_at<S>(pb_src, idx);
+        uint32_t o = 0;
+        for (uint32_t k = 0; k < npl; k++) o |= (__ldg(src + (size_t)k * g.N + idx) != 0u ? 1u : 0u) << k;
+        Code c = 0;
+        while (o) {
+            const uint32_t k = __ffs(o) - 1;
+            o &= o - 1;
+            const uint32_t p = __ldg(src + (size_t)k * g.N + idx);
+            const float r = hash_float(((unsigned long long)idx << CB) | k, th);
+            if ((r >= 0.5f) && (r < __fadd_rn(lookup_T(m, p, t_n, tp_n), 0.5f))) c |= (Code)1 << (S + k);
+            else if (r < lookup_T(m, p, t_n, tm_n)) c |= (Code)1 << k;
+        }
+        return c;
+    };
+    auto outer = [&](uint32_t xn) { return i - x + xn; };
+    Code c_mn, c_pl;
+    if (DIM != 0 || lm >= 0) {
+        c_mn = sc[lm];
+    } else {
+        const uint32_t xm = x == 0 ? g.X - 1 : x - 1;
+        c_mn = outside(im, tm, __ldg(sites + outer(xm == 0 ? g.X - 1 : xm - 1)), t);
+    }
+    if (DIM != 0 || lp >= 0) {
+        c_pl = sc[lp];
+    } else {
+        const uint32_t xp = x == g.X - 1 ? 0 : x + 1;
+        c_pl = outside(ip, tp, t, __ldg(sites + outer(xp == g.X - 1 ? 0 : xp + 1)));
+    }
+    uint32_t n = 0;
+    auto push = [&](uint32_t p) {
+        if (n < (uint32_t)S) dst[(size_t)n * g.N + i] = p;
+        else push_overflow(rs, list, cap, (uint32_t)DIM + 1, i, n - (uint32_t)S, p);
+        n++;
+    };
+    uint32_t stay = occ & ~((uint32_t)c_own | (uint32_t)(c_own >> S)) & LOW;
+    while (stay) {
+        const uint32_t k = __ffs(stay) - 1;
+        stay &= stay - 1;
+        push(sw[k][lid]);
+    }
+    uint32_t in_m = (uint32_t)(c_mn >> S) & LOW;
+    while (in_m) {
+        const uint32_t k = __ffs(in_m) - 1;
+        in_m &= in_m - 1;
+        push(DIM != 0 || lm >= 0 ? sw[k][lm] : __ldg(src + (size_t)k * g.N + im));
+    }
+    uint32_t in_p = (uint32_t)c_pl & LOW;
+    while (in_p) {
+        const uint32_t k = __ffs(in_p) - 1;
+        in_p &= in_p - 1;
+        push(DIM != 0 || lp >= 0 ? sw[k][lp] : __ldg(src + (size_t)k * g.N + ip));
+    }
+    const uint32_t nw = n < (uint32_t)S ? n : (uint32_t)S;
+    const uint32_t wmax = __reduce_max_sync(0xffffffffu, nw);
+    const uint32_t seg = i >> PB_SHIFT;
+    const uint32_t old = pb_dst[seg];
+    const uint32_t lim = wmax > old ? wmax : (old < (uint32_t)S ? old : (uint32_t)S);
+    for (uint32_t k = nw; k < lim; k++) dst[(size_t)k * g.N + i] = 0u;
+    __syncwarp();
+    if (lane == 0) pb_dst[seg] = wmax;
+    if (listing) list_for_reaction(nw, t, i, lid, m, rs, rx_sites, rx_cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -338,8 +537,10 @@ template <int BPS, int S>
 __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ lat, const uint8_t *__restrict__ sites,
                                                        Geometry g, DevTables m, RunState *__restrict__ rs,
                                                        OverflowEntry *__restrict__ list, uint32_t cap,
-                                                       const uint32_t *__restrict__ rx_sites, uint32_t rx_cap)
+                                                       const uint32_t *__restrict__ rx_sites, uint32_t rx_cap,
+                                                       uint32_t *__restrict__ pb)
 {
+    constexpr int W = SiteWords<BPS, S>::W;
     if (rs->status != LMB_OK) return;
     // The sites the z sweep listed, or every site when it listed none or
     // more than the list holds.
@@ -356,7 +557,8 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
         if (all) {
             i = j;
             t = __ldg(sites + i);
-            s.load_packed(lat, g.N, i);
+            if (pb) s.load_first(lat, g.N, i, planes_at<W>(pb, i));
+            else s.load_packed(lat, g.N, i);
         } else {
             const uint2 e = reinterpret_cast<const uint2 *>(rx_sites)[j];
             const uint32_t np = e.y & 0xFFu;
@@ -364,7 +566,14 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
             t = e.y >> 8;
             s.load_first(lat, g.N, i, BPS == 1 ? (np + 3u) / 4u : np);
         }
-        if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) s.store(lat, g.N, i);
+        if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) {
+            s.store(lat, g.N, i);
+            if (pb) {
+                // Products may fill slots above the segment's bound.
+                const uint32_t n = (uint32_t)__popc(occupied_slots<BPS, S>(s));
+                if (n) cover_slot<BPS>(pb, i, n - 1u);
+            }
+        }
     }
 }
 
@@ -379,7 +588,7 @@ __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__re
                                                                   const uint8_t *__restrict__ sites, Geometry g,
                                                                   RunState *__restrict__ rs,
                                                                   OverflowEntry *__restrict__ list, uint32_t cap,
-                                                                  uint32_t rx_cap)
+                                                                  uint32_t rx_cap, uint32_t *__restrict__ pb)
 {
     extern __shared__ OverflowEntry sh[];
     if (rs->status != LMB_OK) return;
@@ -391,7 +600,7 @@ __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__re
         else if (rs->rx_count > rx_cap) rs->rx_skip = 31;
         rs->rx_count = 0;
     }
-    resolve_block<BPS, S>(lat, sites, g, rs, list, cap, sh);
+    resolve_block<BPS, S>(lat, sites, g, rs, list, cap, sh, pb);
 }
 
 // Sets the run state for a new run without a host round trip.  The relaxed
@@ -413,6 +622,11 @@ __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, ui
         rs->ovf_count = 0;
         rs->carried = 0;
     }
+}
+
+__global__ void fill_bounds_kernel(uint32_t *pb, uint32_t count, uint32_t planes)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) pb[j] = planes;
 }
 
 // Batch forms: run state j lives at *rs_ptrs[j]; seeds[j] is its seed.
@@ -462,6 +676,16 @@ cudaError_t launch_gather_states(RunState *const *rs_ptrs, uint32_t count, RunSt
 {
     count_launch();
     gather_states_kernel<<<(count + 127) / 128, 128, 0, stream>>>(rs_ptrs, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_bounds(uint32_t *pb, uint32_t count, uint32_t planes, cudaStream_t stream)
+{
+    uint32_t blocks = (count + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    if (blocks == 0) return cudaSuccess;
+    count_launch();
+    fill_bounds_kernel<<<blocks, 256, 0, stream>>>(pb, count, planes);
     return cudaGetLastError();
 }
 
@@ -635,19 +859,60 @@ bool slots_supported(int bps, int slots)
 
 cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint32_t *dst, const uint8_t *sites,
                          const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
-                         uint32_t *rx_sites, uint32_t rx_cap, cudaStream_t stream)
+                         uint32_t *rx_sites, uint32_t rx_cap, const uint32_t *pb_src, uint32_t *pb_dst,
+                         cudaStream_t stream)
 {
     dim3 grid, block;
     sweep_shape(g, dim, grid, block);
+    // Plane bounds need each warp on one whole segment of 32 sites.
+    if (g.X % 32u != 0) pb_src = pb_dst = nullptr;
+    if (!pb_src || !pb_dst) pb_src = pb_dst = nullptr;
+    if (bps == 4 && pb_src) {
+        // IntLattices with plane bounds: y and z tiles of SWEEP_PB_TILE sites
+        // along the axis, one segment across.
+        if (dim != 0) {
+            const uint32_t A = dim == 1 ? g.Y : g.Z;
+            const uint32_t L = A < (uint32_t)SWEEP_PB_TILE ? A : (uint32_t)SWEEP_PB_TILE;
+            if (dim == 1) {
+                block = dim3(32, L + 2, 1);
+                grid = dim3(g.X / 32, (g.Y + L - 1) / L, g.Z);
+            } else {
+                block = dim3(32, 1, L + 2);
+                grid = dim3(g.X / 32, g.Y, (g.Z + L - 1) / L);
+            }
+        }
+        count_launch();
+        constexpr int YZ = SWEEP_PB_YZ_THREADS;
+#define LMB_INT_SWEEP(S_)                                                                                        \
+    if (slots == S_) {                                                                                          \
+        if (dim == 0)                                                                                           \
+            sweep_int_kernel<S_, 0, SWEEP_THREADS><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list,  \
+                                                                               cap, nullptr, 0, pb_src, pb_dst); \
+        else if (dim == 1)                                                                                      \
+            sweep_int_kernel<S_, 1, YZ><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap,       \
+                                                                    nullptr, 0, pb_src, pb_dst);                \
+        else                                                                                                    \
+            sweep_int_kernel<S_, 2, YZ><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap,       \
+                                                                    rx_sites, rx_cap, pb_src, pb_dst);          \
+        return cudaGetLastError();                                                                              \
+    }
+        LMB_INT_SWEEP(4)
+        LMB_INT_SWEEP(8)
+        LMB_INT_SWEEP(16)
+#undef LMB_INT_SWEEP
+        return cudaErrorInvalidValue;
+    }
     count_launch();
     LMB_DISPATCH_ALL({
         if (dim == 0)
-            sweep_kernel<BPS, S, 0><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0);
+            sweep_kernel<BPS, S, 0><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0,
+                                                                pb_src, pb_dst);
         else if (dim == 1)
-            sweep_kernel<BPS, S, 1><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0);
+            sweep_kernel<BPS, S, 1><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0,
+                                                                pb_src, pb_dst);
         else
             sweep_kernel<BPS, S, 2><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, rx_sites,
-                                                                rx_cap);
+                                                                rx_cap, pb_src, pb_dst);
     })
 }
 
@@ -656,19 +921,21 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
 // would.
 cudaError_t launch_reaction(int bps, int slots, uint32_t *lat, const uint8_t *sites, const Geometry &g,
                             const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
-                            const uint32_t *rx_sites, uint32_t rx_cap, cudaStream_t stream)
+                            const uint32_t *rx_sites, uint32_t rx_cap, uint32_t *pb, cudaStream_t stream)
 {
     const uint32_t threads = 256;
     uint32_t blocks = (g.N + threads - 1) / threads;
     if (blocks > 148 * 8) blocks = 148 * 8;
+    if (g.X % 32u != 0) pb = nullptr;
     count_launch();
     LMB_DISPATCH_ALL(reaction_kernel<BPS, S><<<blocks, threads, 0, stream>>>(lat, sites, g, m, rs, list, cap,
-                                                                             rx_sites, rx_cap))
+                                                                             rx_sites, rx_cap, pb))
 }
 
 cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sites, const Geometry &g, RunState *rs,
-                           OverflowEntry *list, uint32_t cap, uint32_t rx_cap, cudaStream_t stream)
+                           OverflowEntry *list, uint32_t cap, uint32_t rx_cap, uint32_t *pb, cudaStream_t stream)
 {
+    if (g.X % 32u != 0) pb = nullptr;
     uint32_t pow2 = 1;
     while (pow2 < cap) pow2 <<= 1;
     const size_t smem = (size_t)pow2 * sizeof(OverflowEntry);
@@ -681,7 +948,7 @@ cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sit
             cudaFuncSetAttribute(resolve_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             raised[dev] = true;
         }
-        resolve_kernel<BPS, S><<<1, RESOLVE_THREADS, smem, stream>>>(lat, sites, g, rs, list, cap, rx_cap);
+        resolve_kernel<BPS, S><<<1, RESOLVE_THREADS, smem, stream>>>(lat, sites, g, rs, list, cap, rx_cap, pb);
     })
 }
 

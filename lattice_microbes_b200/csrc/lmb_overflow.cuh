@@ -35,9 +35,20 @@ __device__ uint32_t occupancy_at(const uint32_t *lat, uint32_t N, uint32_t i)
     return k;
 }
 
+// Raises the plane bound of site i's segment to cover slot k (pb may be
+// null: the lattice keeps no plane bounds).
+template <int BPS>
+__device__ __forceinline__ void cover_slot(uint32_t *pb, uint32_t i, uint32_t k)
+{
+    if (pb) {
+        const uint32_t planes = (BPS == 1 ? k >> 2 : k) + 1u;
+        if (__ldcg(pb + (i >> PB_SHIFT)) < planes) atomicMax(pb + (i >> PB_SHIFT), planes);
+    }
+}
+
 // First empty slot of site i gets p (ByteLattice.cpp:265-289); false if full.
 template <int BPS, int S>
-__device__ bool add_particle(uint32_t *lat, uint32_t N, uint32_t i, uint32_t p)
+__device__ bool add_particle(uint32_t *lat, uint32_t N, uint32_t i, uint32_t p, uint32_t *pb)
 {
     SiteWords<BPS, S> s;
     load_site_cg<BPS, S>(lat, N, i, s);
@@ -46,6 +57,7 @@ __device__ bool add_particle(uint32_t *lat, uint32_t N, uint32_t i, uint32_t p)
         if (s.slot(j) == 0) {
             s.put(j, p);
             s.store(lat, N, i);
+            cover_slot<BPS>(pb, i, (uint32_t)j);
             return true;
         }
     }
@@ -56,7 +68,8 @@ __device__ bool add_particle(uint32_t *lat, uint32_t N, uint32_t i, uint32_t p)
 // from Lattice::getNearbySites (Lattice.cpp:106-128: clamped to the lattice,
 // x outer, y, z inner), first site of the same type with a free slot.
 template <int BPS, int S>
-__device__ bool reinsert_classic(uint32_t *lat, const uint8_t *sites, const Geometry &g, uint32_t idx, uint32_t p)
+__device__ bool reinsert_classic(uint32_t *lat, const uint8_t *sites, const Geometry &g, uint32_t idx, uint32_t p,
+                                 uint32_t *pb)
 {
     const uint32_t xc = idx % g.X, yc = (idx / g.X) % g.Y, zc = idx / g.XY;
     const uint8_t tc = sites[idx];
@@ -74,7 +87,7 @@ __device__ bool reinsert_classic(uint32_t *lat, const uint8_t *sites, const Geom
                     if (!(r2 <= max2 && (r2 > min2 || mind == maxd))) continue;
                     const uint32_t j = x + y * g.X + z * g.XY;
                     if (sites[j] == tc && occupancy_at<BPS, S>(lat, g.N, j) < (uint32_t)S)
-                        if (add_particle<BPS, S>(lat, g.N, j, p)) return true;
+                        if (add_particle<BPS, S>(lat, g.N, j, p, pb)) return true;
                 }
     }
     return false;
@@ -90,11 +103,12 @@ __host__ __device__ __forceinline__ uint32_t pow2_at_least(uint32_t n)
 
 // Resolves the step's overflow queue with the whole block (thread `tid` of
 // `nthreads`); `sh` holds pow2_at_least(cap) entries.  On success the step
-// counter advances.
+// counter advances.  pb: the lattice's plane bounds, raised for every slot
+// filled here (null when it keeps none).
 template <int BPS, int S>
 __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Geometry &g, RunState *rs,
                                    OverflowEntry *list, uint32_t cap, OverflowEntry *sh, uint32_t tid,
-                                   uint32_t nthreads)
+                                   uint32_t nthreads, uint32_t *pb)
 {
     const uint32_t n = *(volatile uint32_t *)&rs->ovf_count;
     const uint32_t carried = rs->carried;
@@ -146,7 +160,7 @@ __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Ge
     rs->overflows += (unsigned long long)(n - carried);
     if (rs->mode == LMB_OVERFLOW_CLASSIC) {
         for (uint32_t e = 0; e < n; e++) {
-            if (!reinsert_classic<BPS, S>(lat, sites, g, sh[e].site, sh[e].particle)) {
+            if (!reinsert_classic<BPS, S>(lat, sites, g, sh[e].site, sh[e].particle, pb)) {
                 rs->status = LMB_E_OVERFLOW_UNRESOLVED;
                 rs->failed_step = rs->step;
                 return;
@@ -159,7 +173,7 @@ __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Ge
         // queued, in order, for the next timestep.
         uint32_t kept = 0;
         for (uint32_t e = 0; e < n; e++) {
-            if (!add_particle<BPS, S>(lat, g.N, sh[e].site, sh[e].particle)) {
+            if (!add_particle<BPS, S>(lat, g.N, sh[e].site, sh[e].particle, pb)) {
                 OverflowEntry o = sh[e];
                 o.key = (unsigned long long)kept;  // phase 0, list order
                 list[kept++] = o;
@@ -174,9 +188,9 @@ __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Ge
 
 template <int BPS, int S>
 __device__ void resolve_block(uint32_t *lat, const uint8_t *sites, const Geometry &g, RunState *rs,
-                              OverflowEntry *list, uint32_t cap, OverflowEntry *sh)
+                              OverflowEntry *list, uint32_t cap, OverflowEntry *sh, uint32_t *pb)
 {
-    resolve_block_flat<BPS, S>(lat, sites, g, rs, list, cap, sh, threadIdx.x, blockDim.x);
+    resolve_block_flat<BPS, S>(lat, sites, g, rs, list, cap, sh, threadIdx.x, blockDim.x, pb);
 }
 
 }  // namespace lmb

@@ -399,3 +399,55 @@ def test_lattice_with_holes_vs_oracle(ctx, schedule, slots, bps):
     out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 777, 0, 9, schedule=schedule, chunks=[1, 1, 7])
     assert rc == rc_ref == 0
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("slots,bps", [(8, 1), (16, 1), (16, 4), (8, 4)])
+def test_plane_bounds_across_runs_and_edits(ctx, slots, bps):
+    """Per-phase schedule on lattices whose rows are multiples of 32 sites
+    (the sweeps keep per-segment plane bounds): a sparse lattice run in
+    chunks, edited between chunks so that some segments fill every slot (far
+    above the bounds the previous run ended with), then run again; a second
+    lattice starts empty and fills through zeroth-order reactions.  Every
+    chunk equals the oracle."""
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import Lattice, Model
+    spec = configs.random_problem(41, X=64, Y=8, Z=16, slots=slots, bytes_per_slot=bps, density=0.05, nst=2)
+    t = oracle_tables(spec)
+    model = Model.from_tables(ctx, t)
+    lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
+    lat.set_schedule(L.LMB_SCHEDULE_PHASES)
+    lat.set_native(spec.lattice, spec.sites)
+    ref = spec.lattice.copy()
+    rng = np.random.default_rng(7)
+    step = 0
+    N = spec.nsites
+    words = spec.words
+    for chunk in (3, 9, 4, 40):
+        rc, _ = lat.run(model, 99, step, chunk, check=False)
+        assert rc == 0
+        ref, rc_ref, _ = oracle_run(t, ref, spec.sites, 99, step, chunk)
+        assert rc_ref == 0
+        out, _ = lat.get_native()
+        assert np.array_equal(out, ref), "chunk at step %d" % step
+        step += chunk
+        # Fill every slot of a few sites (one full site per edited segment
+        # is enough to lift the segment's bound to every plane).
+        edited = ref.copy()
+        for i in rng.choice(N, size=6, replace=False):
+            if bps == 1:
+                for w in range(words):
+                    edited[w * N + i] = 0x01010101
+            else:
+                for w in range(words):
+                    edited[w * N + i] = 1 + (w % spec.ns)
+        lat.set_native(edited, None)
+        ref = edited
+    lat.close()
+    model.close()
+
+    empty = configs.empty_lattice(t.X, t.Y, t.Z, slots, bps)
+    out, rc, _ = _gpu_run(ctx, t, empty, spec.sites, 5, 0, 30, schedule="phases")
+    ref, rc_ref, _ = oracle_run(t, empty, spec.sites, 5, 0, 30)
+    assert rc == rc_ref == 0
+    assert out.any()
+    assert np.array_equal(out, ref)
