@@ -32,12 +32,17 @@ def golden():
 
 
 def compare(a, b, p_min, z, what):
+    """Two-sample KS, means within z standard errors, and equal variances
+    (Brown-Forsythe: Levene's test about the medians), each at p_min."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     ks = stats.ks_2samp(a, b)
     assert ks.pvalue > p_min, (what, ks)
     se = np.sqrt(a.var() / a.size + b.var() / b.size)
     assert abs(a.mean() - b.mean()) <= z * se + 1e-12, (what, a.mean(), b.mean(), se)
+    if a.var() > 0 or b.var() > 0:
+        bf = stats.levene(a, b, center="median")
+        assert bf.pvalue > p_min, (what, "variance", a.var(), b.var(), bf)
 
 
 def run_ensemble(ctx, reps, seed=5, segments=1, spec=None):
@@ -72,6 +77,12 @@ def test_two_state_ensemble_matches_reference_gillespie(ctx):
     assert np.all(out[:, :, 0] + out[:, :, 1] == 1)  # one gene copy, always
     assert np.array_equal(out[:, 0, :], np.tile([1, 0, 0, 0], (65536, 1)))
     compare(out[:, -1, 3], ref[:, -1, 3], 0.01, 2.0, "protein at t_end")
+    # The reference's own regression bar for expression models
+    # (testing/regression/testsuites/CMEBase/testCME.py:117-178): mean and
+    # variance of the output within 10 %.
+    a, b = out[:, -1, 3].astype(np.float64), ref[:, -1, 3].astype(np.float64)
+    assert abs(a.mean() / b.mean() - 1) < 0.10 and abs(a.var() / b.var() - 1) < 0.10, (a.mean(), b.mean(),
+                                                                                        a.var(), b.var())
     pairs = [(e, s) for e in range(1, len(times)) for s in range(1, 4)]
     m = len(pairs)
     z = stats.norm.ppf(1 - 0.025 / m)

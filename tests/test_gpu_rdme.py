@@ -182,3 +182,56 @@ def test_python_solver_site_frames_in_the_lm_file(gpu, tmp_path):
                         np.bincount(t[(t > 0) & (t < spec.nst)], minlength=spec.nst))
     assert np.array_equal(ms, expect) and np.array_equal(s.maxSiteCounts, expect)
     s.close()
+
+
+def test_jlm_sim_run_sequence(gpu, tmp_path):
+    """jLM's Sim, call for call: the lattice made as RDME.py:145-150 makes it
+    (lm.getCompiledLatticeMaxOccupancy, lm.ByteLattice), the file written with
+    LmWriteMixin.finalize's lm calls (LmInteract.py:55-84), then Sim.run
+    (RDME.py:447-455): lm.MpdRdmeSolver(), lm.simulationFile(name) with
+    setParameter("seed", ...) and close, lm.runSolver(name, replicate, solver,
+    cudaDevices, checkpointInterval).  The replicate read back from the file
+    equals the same solver set up directly with those inputs."""
+    import lattice_microbes_b200.lm  # noqa: F401  (makes `import lm` this package's)
+    import lm
+    from lattice_microbes_b200.lmfile import LMFile
+    from lattice_microbes_b200.rdme import MpdRdmeSolver
+    from tests.test_lm_module import write_jlm_file
+    spec = configs.config0(seed=11, edge=16, nA=500, nB=500)
+    spec.K = spec.K * np.array([300.0, 30.0])
+    steps, ce, le = 120, 20, 40
+    params = {"writeInterval": str(ce), "latticeWriteInterval": str(le),
+              "maxTime": "{:.10e}".format((steps - 0.5) * spec.tau), "timestep": "{:.10e}".format(spec.tau),
+              "hookInterval": ""}
+    path = str(tmp_path / "sim.lm")
+    pps = lm.getCompiledLatticeMaxOccupancy()
+    lattice, init = write_jlm_file(lm, path, spec, pps, params)
+    solver = lm.MpdRdmeSolver()
+    f = lm.simulationFile(path)
+    f.setParameter("seed", str(77))
+    f.close()
+    lm.runSolver(path, 1, solver, [0], int(0))
+    direct = MpdRdmeSolver(0)
+    direct.initialize(1, dict(params, seed="77"))
+    direct.buildModel(spec.ns, spec.nr, init, spec.rtype, spec.K, np.asarray(spec.S).reshape(-1),
+                      np.asarray(spec.D).reshape(-1))
+    p, s = lattice.rowMajor()
+    direct.buildDiffusionModel(spec.nst, np.asarray(spec.DF).reshape(-1), np.asarray(spec.RL).reshape(-1), spec.X,
+                               spec.Y, spec.Z, pps, 1, spec.spacing, p.reshape(-1), s.reshape(-1))
+    direct.generateTrajectory()
+    with LMFile(path) as g:
+        assert g.replicates() == [1]
+        assert g.getParameter("seed") == "77"
+        t, c = g.species_counts(1)
+        assert len(t) == 1 + steps // ce
+        assert np.array_equal(t, [a for a, _ in direct.speciesCounts])
+        assert np.array_equal(c, np.array([b for _, b in direct.speciesCounts]))
+        assert c[-1, 2] > 0  # C formed
+        assert np.array_equal(g.lattice_times(1), [a for a, _, _ in direct.latticeFrames])
+        for i, (_, fr, _) in enumerate(direct.latticeFrames):
+            X, Y, Z = spec.X, spec.Y, spec.Z
+            v = fr.view(np.uint8).reshape(pps // 4, Z, Y, X, 4)
+            expect = np.moveaxis(v, 0, 3).reshape(Z, Y, X, pps).transpose(2, 1, 0, 3)
+            assert np.array_equal(g.lattice(1, i), expect)
+    direct.close()
+    solver.close()
