@@ -630,10 +630,11 @@ def run_reference(a):
 def run_batch(a):
     """Batched replicates: config-0 chemistry (A + B <-> C, 32 nm, tau = 50 us)
     on cubic lattices with edges drawn from {16, 24, 32, 48, 64}, all advanced
-    by one launch per timestep.  Metric: replicates/s, a replicate being one
-    10,000-timestep trajectory.  Compared with the plain solver running the
-    same replicates one after another (each lattice alone, graph replay)."""
-    import numpy as np
+    by one launch per timestep with tile shapes chosen per edge by the batch
+    autotuner.  Metric: replicates/s, a replicate being one 10,000-timestep
+    trajectory.  Compared with the plain solver running the same replicates
+    one after another, each with the schedule its own autotuner picks for its
+    edge, over the same timesteps."""
     import torch
 
     from lattice_microbes_b200 import configs
@@ -656,6 +657,12 @@ def run_batch(a):
     seeds = [compose_seed(2024, k) for k in range(len(lats))]
     sites_total = sum(e ** 3 for e in edges)
     batch = Batch(ctx, lats, models)
+    t0 = time.perf_counter()
+    batch.autotune(seeds, 0, 16)
+    tune_s = time.perf_counter() - t0
+    plan = {}
+    for e, (ty, tz) in zip(edges, batch.plan()):
+        plan[str(e)] = "%dx%d" % (ty, tz)
     step = 0
     for _ in range(a.warmup):
         batch.run(seeds, step, T)
@@ -679,22 +686,29 @@ def run_batch(a):
     ms_step = sum(times) / a.steps / T                       # per timestep, all replicates
     rep_per_s = len(lats) / (10000 * ms_step / 1e3)
 
-    # Plain solver, one replicate at a time: per-timestep time of one lattice
-    # of each edge, summed over the replicates.
-    per_edge = {}
+    # Plain solver, one replicate after another on the same stream: each edge's
+    # schedule from the single-lattice autotuner, every replicate run for the
+    # same T timesteps (one untimed pass first: graph capture).
+    sched = {}
     for e in sorted(set(edges)):
         k = edges.index(e)
-        lat, m = lats[k], models[k]
-        lat.run(m, seeds[k], 0, 64)
+        s_, ty, tz, _ = lats[k].autotune(models[k], seeds[k], step, 32)
+        sched[e] = (s_, ty, tz)
+    for lat, e in zip(lats, edges):
+        lat.set_schedule(*sched[e])
+    for lat, m, sd in zip(lats, models, seeds):
+        lat.run(m, sd, step, T)
+    step += T
+    with torch.cuda.stream(stream):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-            lat.run_async(m, seeds[k], 64, T)
-            e1.record(stream)
+        e0.record(stream)
+        for lat, m, sd in zip(lats, models, seeds):
+            lat.run_async(m, sd, step, T)
+        e1.record(stream)
+        for lat in lats:
             lat.wait()
-        per_edge[e] = e0.elapsed_time(e1) / T
-    seq_ms_step = sum(per_edge[e] for e in edges)
+    seq_ms_step = e0.elapsed_time(e1) / T
     seq_rep_per_s = len(lats) / (10000 * seq_ms_step / 1e3)
     line = {
         "metric": "replicates/s",
@@ -711,10 +725,13 @@ def run_batch(a):
         "data": "synthetic (seeded bimolecular replicates, lattice_microbes_b200.configs.config0)",
         "config": {"workload": "batch of %d bimolecular replicates, edges {16,24,32,48,64}, %d sites"
                                % (len(lats), sites_total),
-                   "timesteps_per_step": T, "trajectory_timesteps": 10000},
+                   "timesteps_per_step": T, "trajectory_timesteps": 10000,
+                   "batch_plan_by_edge": plan, "autotune_s": tune_s},
         "site_steps_per_s": sites_total / (ms_step / 1e3),
         "sequential_plain": {"value": seq_rep_per_s, "unit": "replicates/s",
-                             "ms_per_timestep_by_edge": per_edge},
+                             "what": "all %d replicates, one after another, %d timesteps each" % (len(lats), T),
+                             "schedule_by_edge": {str(e): ("fused %dx%d" % (v[1], v[2]) if v[0] == 0 else "phases")
+                                                  for e, v in sched.items()}},
         "speedup_vs_sequential": rep_per_s / seq_rep_per_s,
         "gpu_launches": int(launches),
         "clocks": clock_info,

@@ -258,6 +258,17 @@ int lmb_batch_run_ranges_async(lmb_batch *batch, const uint32_t *seeds, const ui
  * slot); no run may be pending. */
 int lmb_batch_set_lattices(lmb_batch *batch, uint32_t count, lmb_lattice *const *lattices,
                            const lmb_model *const *models);
+/* Chooses the tile shape of each lattice size in the batch by timing: for
+ * each size (largest total first) every tile shape the batch kernel can use
+ * runs `number_timesteps` timesteps of the whole batch from the lattices'
+ * current states, and the fastest is kept (best_ms: that run's time).  The
+ * lattices end where they started.  The choice holds for lattices of that
+ * size from then on, after lmb_batch_set_lattices too.  No counterpart in the
+ * reference (one solver per lattice, fixed launch geometry). */
+int lmb_batch_autotune(lmb_batch *batch, const uint32_t *seeds, uint32_t first_timestep,
+                       uint32_t number_timesteps, float *best_ms);
+/* The tile plan: Ty[j] x Tz[j] x-rows per block for lattice j. */
+int lmb_batch_plan(lmb_batch *batch, uint32_t *Ty, uint32_t *Tz);
 int lmb_batch_destroy(lmb_batch *batch);
 
 /* ---- serving: continuous batching of solves ------------------------------------

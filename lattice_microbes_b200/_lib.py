@@ -135,6 +135,8 @@ PROTOTYPES = {
     "lmb_batch_run_ranges_async": (C.c_int, [vp, u32p, u32p, u32p, C.c_int]),
     "lmb_batch_set_lattices": (C.c_int, [vp, C.c_uint32, C.POINTER(vp), C.POINTER(vp)]),
     "lmb_batch_destroy": (C.c_int, [vp]),
+    "lmb_batch_autotune": (C.c_int, [vp, u32p, C.c_uint32, C.c_uint32, f32p]),
+    "lmb_batch_plan": (C.c_int, [vp, u32p, u32p]),
     "lmb_server_create": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint32,
                                     C.POINTER(vp)]),
     "lmb_server_destroy": (C.c_int, [vp]),

@@ -11,7 +11,9 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <new>
+#include <tuple>
 #include <vector>
 
 #include "lmb.h"
@@ -1203,9 +1205,14 @@ struct lmb_batch {
     bool pending;
     std::vector<uint32_t> pending_first, pending_n;
     std::vector<int> cur0;
+    // Tiles lmb_batch_autotune chose, by lattice size (X, Y, Z): used for
+    // every member of that size, now and after lmb_batch_set_lattices.
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, std::pair<uint32_t, uint32_t>> tuned;
 };
 
 static const uint32_t BATCH_GRAPH_STEPS = 32;
+
+static std::tuple<uint32_t, uint32_t, uint32_t> size_key(const Geometry &g) { return {g.X, g.Y, g.Z}; }
 
 static void batch_free_arrays(lmb_batch *b)
 {
@@ -1264,6 +1271,13 @@ static int batch_set(lmb_batch *b, uint32_t count, lmb_lattice *const *lattices,
 {
     int rc = batch_reserve(b, count);
     if (rc) return rc;
+    for (uint32_t j = 0; j < count; j++) {
+        const auto it = b->tuned.find(size_key(lattices[j]->g));
+        TileShape t;
+        if (it != b->tuned.end() &&
+            fused_batch_shape_ok(lattices[j]->g, b->bps, b->slots, it->second.first, it->second.second, t))
+            plan[j] = t;
+    }
     b->lats.assign(lattices, lattices + count);
     b->models.assign(models, models + count);
     b->tiles.swap(plan);
@@ -1507,4 +1521,109 @@ extern "C" int lmb_batch_run(lmb_batch *b, const uint32_t *seeds, uint32_t first
     int rc = lmb_batch_run_async(b, seeds, first, n, mode);
     if (rc != LMB_OK) return rc;
     return lmb_batch_wait(b, stats);
+}
+
+extern "C" int lmb_batch_autotune(lmb_batch *b, const uint32_t *seeds, uint32_t first, uint32_t timesteps,
+                                  float *best_ms)
+{
+    // Per lattice size, largest total size first: every tile shape a batch
+    // may use is timed on the whole batch (the launch's shared memory is the
+    // largest any member needs, so the choices interact), each trial from
+    // the same saved states; the fastest stays.  The lattices end where they
+    // started.
+    if (!b || !seeds || timesteps == 0) return LMB_E_ARG;
+    if (b->pending) return LMB_E_STATE;
+    lmb_ctx *c = b->ctx;
+    CK(cudaSetDevice(c->device));
+    const uint32_t count = (uint32_t)b->lats.size();
+    std::vector<size_t> off(count);
+    size_t total = 0;
+    for (uint32_t j = 0; j < count; j++) {
+        off[j] = total;
+        total += (size_t)b->lats[j]->words * b->lats[j]->g.N * sizeof(uint32_t);
+    }
+    uint8_t *save = nullptr;
+    CK(cudaMalloc(&save, total));
+    std::vector<int> cur0(count);
+    for (uint32_t j = 0; j < count; j++) {
+        lmb_lattice *l = b->lats[j];
+        cur0[j] = l->cur;
+        cudaMemcpyAsync(save + off[j], l->buf[l->cur], (size_t)l->words * l->g.N * 4, cudaMemcpyDeviceToDevice,
+                        c->stream);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto restore = [&]() {
+        for (uint32_t j = 0; j < count; j++) {
+            lmb_lattice *l = b->lats[j];
+            l->cur = cur0[j];
+            cudaMemcpyAsync(l->buf[l->cur], save + off[j], (size_t)l->words * l->g.N * 4,
+                            cudaMemcpyDeviceToDevice, c->stream);
+        }
+    };
+    // Time of one trial (the better of two), or a large value when it fails.
+    auto trial = [&]() -> float {
+        float best = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            restore();
+            cudaEventRecord(e0, c->stream);
+            if (batch_run(b, seeds, first, timesteps, nullptr, nullptr, LMB_OVERFLOW_CLASSIC) != LMB_OK) return 1e30f;
+            cudaEventRecord(e1, c->stream);
+            if (lmb_batch_wait(b, nullptr) != LMB_OK) return 1e30f;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) best = ms;
+        }
+        return best;
+    };
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, std::vector<uint32_t>> classes;
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, uint64_t> sites;
+    for (uint32_t j = 0; j < count; j++) {
+        classes[size_key(b->lats[j]->g)].push_back(j);
+        sites[size_key(b->lats[j]->g)] += b->lats[j]->g.N;
+    }
+    std::vector<std::tuple<uint32_t, uint32_t, uint32_t>> order;
+    for (auto &kv : classes) order.push_back(kv.first);
+    std::sort(order.begin(), order.end(), [&](const auto &a, const auto &z) { return sites[a] > sites[z]; });
+    trial();  // warm-up
+    float best = trial();
+    const uint32_t cands[] = {1, 2, 4, 8, 16};
+    for (const auto &key : order) {
+        const std::vector<uint32_t> &members = classes[key];
+        const Geometry g = b->lats[members[0]]->g;
+        TileShape keep = b->tiles[members[0]];
+        for (uint32_t Ty : cands)
+            for (uint32_t Tz : cands) {
+                TileShape t;
+                if (!fused_batch_shape_ok(g, b->bps, b->slots, Ty, Tz, t)) continue;
+                if (t.Ty == keep.Ty && t.Tz == keep.Tz) continue;
+                for (uint32_t j : members) b->tiles[j] = t;
+                const float ms = trial();
+                if (ms < best) {
+                    best = ms;
+                    keep = t;
+                }
+            }
+        for (uint32_t j : members) b->tiles[j] = keep;
+        b->tuned[key] = {keep.Ty, keep.Tz};
+    }
+    restore();
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(save);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (best_ms) *best_ms = best;
+    return LMB_OK;
+}
+
+extern "C" int lmb_batch_plan(lmb_batch *b, uint32_t *Ty, uint32_t *Tz)
+{
+    if (!b || !Ty || !Tz) return LMB_E_ARG;
+    for (size_t j = 0; j < b->tiles.size(); j++) {
+        Ty[j] = b->tiles[j].Ty;
+        Tz[j] = b->tiles[j].Tz;
+    }
+    return LMB_OK;
 }

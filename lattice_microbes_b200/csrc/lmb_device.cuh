@@ -53,6 +53,14 @@ __host__ __device__ __forceinline__ unsigned long long timestep_hash(uint32_t se
     return h;
 }
 
+// Sets rs->step and the four sub-step hashes that go with it.
+__device__ __forceinline__ void set_step(RunState *rs, uint32_t seed, uint32_t step)
+{
+    rs->step = step;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++) rs->th[k] = timestep_hash(seed, step, k);
+}
+
 // Hash-key slot bits (byte_diffusion_1d_dev.cu:51-60).
 template <int S>
 struct CountBits {

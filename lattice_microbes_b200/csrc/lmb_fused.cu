@@ -102,7 +102,7 @@ __device__ __noinline__ SiteWords<BPS, S> react_site_ool(SiteWords<BPS, S> s, ui
                                                          unsigned long long th, const DevTables &m, RunState *rs,
                                                          OverflowEntry *list, uint32_t cap)
 {
-    react_site<BPS, S>(s, t, gi, th, m, rs, list, cap);
+    react_site<BPS, S, 8>(s, t, gi, th, m, rs, list, cap);
     return s;
 }
 
@@ -660,6 +660,15 @@ static cudaError_t ensure_smem_limit(size_t smem)
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) granted[dev] = smem;
     return e;
+}
+
+// A tile a batch may use: it fits, and its region leaves room for the two
+// blocks per SM the batch kernel is built for.
+bool fused_batch_shape_ok(const Geometry &g, int bps, int slots, uint32_t Ty, uint32_t Tz, TileShape &ts)
+{
+    if (!fused_make_shape(g, bps, slots, Ty, Tz, ts)) return false;
+    const uint32_t W = bps == 1 ? slots / 4 : slots;
+    return region_bytes(g.X, Ty, Tz, W) <= FUSED_PREFERRED_SMEM;
 }
 
 // Batch plan: the batch already fills the GPU with many lattices, so each

@@ -49,6 +49,7 @@ cudaError_t launch_fused_batch(int bytes_per_slot, int slots, const FusedJob *jo
 bool fused_make_shape(const Geometry &g, int bytes_per_slot, int slots, uint32_t Ty, uint32_t Tz, TileShape &ts);
 bool fused_default_shape(const Geometry &g, int bytes_per_slot, int slots, TileShape &ts);
 bool fused_batch_shape(const Geometry &g, int bytes_per_slot, int slots, TileShape &ts);
+bool fused_batch_shape_ok(const Geometry &g, int bytes_per_slot, int slots, uint32_t Ty, uint32_t Tz, TileShape &ts);
 size_t fused_smem_bytes(const TileShape &ts, uint32_t X, uint32_t W, uint32_t cap, uint32_t stage_bytes);
 cudaError_t launch_fused(int bytes_per_slot, int slots, const uint32_t *src, uint32_t *dst, const uint8_t *sites,
                          const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,

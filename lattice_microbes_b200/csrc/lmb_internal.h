@@ -90,7 +90,11 @@ struct RunState {
     uint32_t tiles_done;  // fused kernel: blocks finished in this launch
     uint32_t rx_count;    // per-phase schedule: sites the z sweep listed for the reaction step
     uint32_t rx_skip;     // timesteps left to run without the list (it overflowed recently)
+    // timestep_hash(seed, step, k) for the sub-steps k = 0..3 of `step`, set
+    // with every change of step (the per-phase kernels read them here).
+    unsigned long long th[4];
 };
+
 
 // Plane bounds (per-phase schedule, lattices whose X is a multiple of 32):
 // for each segment of 32 consecutive sites (site i in segment i >> PB_SHIFT),

@@ -105,7 +105,7 @@ __device__ __forceinline__ void list_for_reaction(uint32_t n, uint32_t t, uint32
     const float a0 = tload(m.qp0 + t);
     bool need = false;
     if (n != 0 || a0 != 0.0f) {
-        const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
+        const unsigned long long th = rs->th[3];
         need = reaction_may_fire(n, a0, t, hash_float((unsigned long long)i << 1, th), m);
     }
     const uint32_t act = __activemask();
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
     own.clear();
     uint32_t t = 0, tm = 0, tp = 0;
     Code c_own = 0;
-    const unsigned long long th = timestep_hash(rs->seed, rs->step, DIM);
+    const unsigned long long th = rs->th[DIM];
     uint32_t occ = 0;
     if (in) {
         sweep_neighbours<DIM>(g, x, y, z, lid, i, im, ip, lm, lp);
@@ -378,25 +378,43 @@ constexpr int SWEEP_PB_TILE = 16;
 constexpr int SWEEP_PB_YZ_THREADS = 32 * (SWEEP_PB_TILE + 2);
 
 // The rule of sweep_kernel's IntLattice path for lattices that keep plane
-// bounds (X a multiple of 32: every warp holds the 32 sites of one segment of
-// one x row).  A thread moves only the word planes below its segment's bound,
-// in loops whose trip count the whole warp shares: it stages its own site's
-// words in shared memory as they arrive, writes each particle of its new site
-// straight to the destination as it is placed, then clears its planes from
-// its new content up to the larger of the warp's new bound and the
-// destination's old one, and the warp stores its new bound.
+// bounds and whose x rows fit one block (X a multiple of 32, at most 256:
+// every warp holds the 32 sites of one segment of one x row, and an x tile is
+// whole rows).  Work goes by particle, not by site: the warp's particles are
+// spread over its lanes (particle q of the warp, in site then slot order, on
+// lane q % 32) once to draw their choices and once more, after the block has
+// every choice, to place them.  A particle's place in its new site follows
+// from the choice masks alone: a stayer comes after the site's stayers of
+// lower slots; a particle arriving from the minus neighbour after every
+// stayer and that neighbour's PLUS movers of lower slots; one arriving from
+// the plus neighbour after those and the minus neighbour's PLUS movers and
+// its own site's MINUS movers of lower slots (byte_diffusion_1d_dev.cu:
+// 199-269 builds the same order site by site).  Each particle is written
+// straight to the destination by the block that owns its new site (halo
+// rows place what moves into the tile); places past the last slot overflow
+// with the same sequence numbers.  Then each site clears its planes from its
+// new count up to the larger of the warp's new bound and the destination's
+// old one, and the warp stores its new bound.
 template <int S, int DIM, int NT>
-__global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 2)
+__global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     sweep_int_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, const uint8_t *__restrict__ sites,
                      Geometry g, DevTables m, RunState *__restrict__ rs, OverflowEntry *__restrict__ list,
                      uint32_t cap, uint32_t *__restrict__ rx_sites, uint32_t rx_cap,
                      const uint32_t *__restrict__ pb_src, uint32_t *__restrict__ pb_dst)
 {
-    using Code = typename ChoiceCode<S>::type;
     constexpr int CB = CountBits<S>::value;
     constexpr uint32_t LOW = (1u << S) - 1u;
-    __shared__ uint32_t sw[S][NT];
-    __shared__ Code sc[NT];
+    constexpr uint32_t OUT = 1u << 16;  // occupancy word flag: the block writes this site
+    // Dynamic shared memory (sweep_int_smem bytes):
+    //   sw[S][NT]  particles of the tile's sites, planes below the bound
+    //   sc[NT]     choices: bit k MINUS, bit S + k PLUS for slot k
+    //   so[NT]     occupied slots, | OUT for written sites
+    //   pl[NT * S] each warp's particles in site, then slot order: lane << 4 | slot
+    extern __shared__ uint32_t smem_int[];
+    uint32_t(*sw)[NT] = reinterpret_cast<uint32_t(*)[NT]>(smem_int);
+    uint32_t *sc = smem_int + S * NT;
+    uint32_t *so = sc + NT;
+    uint16_t *pl = reinterpret_cast<uint16_t *>(so + NT);
     if (rs->status != LMB_OK) return;
     const bool listing = DIM == 2 && rx_sites && rs->rx_skip == 0;
     uint32_t x, y, z;
@@ -407,7 +425,7 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 2)
     uint32_t i = 0, im = 0, ip = 0;
     int lm = -1, lp = -1;
     uint32_t t = 0, tm = 0, tp = 0, occ = 0;
-    const unsigned long long th = timestep_hash(rs->seed, rs->step, DIM);
+    const unsigned long long th = rs->th[DIM];
     if (in) {
         sweep_neighbours<DIM>(g, x, y, z, lid, i, im, ip, lm, lp);
         const uint32_t npl = planes_at<S>(pb_src, i);
@@ -420,104 +438,112 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 2)
         tm = __ldg(sites + im);
         tp = __ldg(sites + ip);
     }
+    so[lid] = occ | (out ? OUT : 0u);
     sc[lid] = 0;
     __syncwarp();
-    // The warp's particles drawn together, particle q (site, then slot
-    // order) on lane q % 32, as in sweep_kernel.
+    // The warp's particles: prefix counts over the lanes' sites.
+    const uint32_t wbase = (uint32_t)lid & ~31u;
+    const uint32_t cnt = __popc(occ);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - cnt;
+    uint16_t *wpl = pl + wbase * S;
     {
-        const uint32_t wbase = (uint32_t)lid & ~31u;
-        const uint32_t cnt = __popc(occ);
-        uint32_t incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= (uint32_t)o) incl += v;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - cnt;
-        for (uint32_t base = 0; base < total; base += 32) {
-            const uint32_t q = base + lane;
-            uint32_t o = 0;
-#pragma unroll
-            for (uint32_t step = 16; step >= 1; step >>= 1) {
-                const uint32_t e = __shfl_sync(0xffffffffu, excl, (o + step) & 31u);
-                if (o + step < 32 && e <= q) o += step;
+        uint32_t q = excl;
+        for (uint32_t mb = occ; mb; mb &= mb - 1) wpl[q++] = (uint16_t)((lane << 4) | (__ffs(mb) - 1));
+    }
+    __syncwarp();
+    // Particle q of the warp: its site's lane and its slot (lane 0, slot 0
+    // past the last particle).
+    auto particle = [&](uint32_t q, uint32_t &o, uint32_t &k) {
+        const uint32_t e = q < total ? wpl[q] : 0u;
+        o = e >> 4;
+        k = e & 15u;
+    };
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t q = base + lane;
+        uint32_t o, k;
+        particle(q, o, k);
+        const uint32_t t_o = __shfl_sync(0xffffffffu, t, o), tm_o = __shfl_sync(0xffffffffu, tm, o);
+        const uint32_t tp_o = __shfl_sync(0xffffffffu, tp, o), gi_o = __shfl_sync(0xffffffffu, i, o);
+        if (q < total) {
+            const uint32_t sl = wbase + o;
+            const uint32_t p = sw[k][sl];
+            const float rv = hash_float(((unsigned long long)gi_o << CB) | k, th);
+            // PLUS when 0.5 <= r < q(t -> tp) + 0.5, else MINUS when r <
+            // q(t -> tm).  Every q is at most 0.5 (larger ones are refused
+            // when a model is built), so a draw of 0.5 or more cannot move
+            // MINUS and each particle needs one table entry.
+            const bool hi = rv >= 0.5f;
+            const float qv = lookup_T(m, p, t_o, hi ? tp_o : tm_o);
+            uint32_t bit = 0;
+            if (hi) {
+                if (rv < __fadd_rn(qv, 0.5f)) bit = 1u << (S + k);
+            } else if (rv < qv) {
+                bit = 1u << k;
             }
-            const uint32_t occ_o = __shfl_sync(0xffffffffu, occ, o);
-            const uint32_t j = q - __shfl_sync(0xffffffffu, excl, o);
-            const uint32_t t_o = __shfl_sync(0xffffffffu, t, o), tm_o = __shfl_sync(0xffffffffu, tm, o);
-            const uint32_t tp_o = __shfl_sync(0xffffffffu, tp, o), gi_o = __shfl_sync(0xffffffffu, i, o);
-            if (q < total) {
-                uint32_t mbits = occ_o;
-                for (uint32_t r = 0; r < j; r++) mbits &= mbits - 1;
-                const uint32_t k = __ffs(mbits) - 1;
-                const uint32_t so = wbase + o;
-                const uint32_t p = sw[k][so];
-                const float rv = hash_float(((unsigned long long)gi_o << CB) | k, th);
-                Code bit = 0;
-                if ((rv >= 0.5f) && (rv < __fadd_rn(lookup_T(m, p, t_o, tp_o), 0.5f))) bit = (Code)1 << (S + k);
-                else if (rv < lookup_T(m, p, t_o, tm_o)) bit = (Code)1 << k;
-                if (bit) atomicOr(&sc[so], bit);
-            }
+            if (bit) atomicOr(&sc[sl], bit);
         }
     }
     __syncthreads();
-    if (!out) return;
-    const Code c_own = sc[lid];
-    // Neighbours outside the tile (ends of x rows longer than the block):
-    // their occupied slots and choices, drawn here.
-    auto outside = [&](uint32_t idx, uint32_t t_n, uint32_t tm_n, uint32_t tp_n) {
-        const uint32_t npl = planes_at<S>(pb_src, idx);
-        uint32_t o = 0;
-        for (uint32_t k = 0; k < npl; k++) o |= (__ldg(src + (size_t)k * g.N + idx) != 0u ? 1u : 0u) << k;
-        Code c = 0;
-        while (o) {
-            const uint32_t k = __ffs(o) - 1;
-            o &= o - 1;
-            const uint32_t p = __ldg(src + (size_t)k * g.N + idx);
-            const float r = hash_float(((unsigned long long)idx << CB) | k, th);
-            if ((r >= 0.5f) && (r < __fadd_rn(lookup_T(m, p, t_n, tp_n), 0.5f))) c |= (Code)1 << (S + k);
-            else if (r < lookup_T(m, p, t_n, tm_n)) c |= (Code)1 << k;
+    // Tile neighbours of tile site l at x coordinate xl (x tiles are whole
+    // rows, periodic; y and z tiles are 32 sites wide).
+    auto xminus = [&](uint32_t xl) { return xl == 0 ? g.X - 1 : xl - 1; };
+    auto xplus = [&](uint32_t xl) { return xl == g.X - 1 ? 0 : xl + 1; };
+    auto tile_minus = [&](uint32_t l, uint32_t xl) -> uint32_t {
+        if (DIM == 0) return l - xl + xminus(xl);
+        return l - 32u;
+    };
+    auto tile_plus = [&](uint32_t l, uint32_t xl) -> uint32_t {
+        if (DIM == 0) return l - xl + xplus(xl);
+        return l + 32u;
+    };
+    auto stays = [&](uint32_t l) { return so[l] & ~(sc[l] | (sc[l] >> S)) & LOW; };
+    // Place every particle whose new site this block writes.
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t q = base + lane;
+        uint32_t o, k;
+        particle(q, o, k);
+        const uint32_t gi_o = __shfl_sync(0xffffffffu, i, o), im_o = __shfl_sync(0xffffffffu, im, o);
+        const uint32_t ip_o = __shfl_sync(0xffffffffu, ip, o);
+        const uint32_t x_o = DIM == 0 ? __shfl_sync(0xffffffffu, x, o) : 0u;
+        if (q < total) {
+            const uint32_t sl = wbase + o;
+            const uint32_t c = sc[sl];
+            const uint32_t below = (1u << k) - 1u;
+            const uint32_t plus = (c >> (S + k)) & 1u, minus = (c >> k) & 1u;
+            // New site in the tile; a y or z tile's halo rows move particles
+            // out of the tile as well, which other blocks place.
+            const uint32_t row = sl >> 5, rows = DIM == 1 ? blockDim.y : blockDim.z;
+            const bool inside = DIM == 0 || !((plus && row + 1u >= rows) || (minus && row == 0));
+            const uint32_t d = plus ? tile_plus(sl, x_o) : (minus ? tile_minus(sl, x_o) : sl);
+            if (inside && (so[d] & OUT)) {
+                uint32_t gd, pos;
+                if (plus) {  // after the new site's stayers
+                    gd = ip_o;
+                    pos = __popc(stays(d)) + __popc((c >> S) & below);
+                } else if (minus) {  // after its stayers and the PLUS arrivals from its minus side
+                    gd = im_o;
+                    pos = __popc(stays(d)) + __popc((sc[tile_minus(d, xminus(x_o))] >> S) & LOW) +
+                          __popc(c & below);
+                } else {
+                    gd = gi_o;
+                    pos = __popc(stays(sl) & below);
+                }
+                const uint32_t p = sw[k][sl];
+                if (pos < (uint32_t)S) dst[(size_t)pos * g.N + gd] = p;
+                else push_overflow(rs, list, cap, (uint32_t)DIM + 1, gd, pos - (uint32_t)S, p);
+            }
         }
-        return c;
-    };
-    auto outer = [&](uint32_t xn) { return i - x + xn; };
-    Code c_mn, c_pl;
-    if (DIM != 0 || lm >= 0) {
-        c_mn = sc[lm];
-    } else {
-        const uint32_t xm = x == 0 ? g.X - 1 : x - 1;
-        c_mn = outside(im, tm, __ldg(sites + outer(xm == 0 ? g.X - 1 : xm - 1)), t);
     }
-    if (DIM != 0 || lp >= 0) {
-        c_pl = sc[lp];
-    } else {
-        const uint32_t xp = x == g.X - 1 ? 0 : x + 1;
-        c_pl = outside(ip, tp, t, __ldg(sites + outer(xp == g.X - 1 ? 0 : xp + 1)));
-    }
-    uint32_t n = 0;
-    auto push = [&](uint32_t p) {
-        if (n < (uint32_t)S) dst[(size_t)n * g.N + i] = p;
-        else push_overflow(rs, list, cap, (uint32_t)DIM + 1, i, n - (uint32_t)S, p);
-        n++;
-    };
-    uint32_t stay = occ & ~((uint32_t)c_own | (uint32_t)(c_own >> S)) & LOW;
-    while (stay) {
-        const uint32_t k = __ffs(stay) - 1;
-        stay &= stay - 1;
-        push(sw[k][lid]);
-    }
-    uint32_t in_m = (uint32_t)(c_mn >> S) & LOW;
-    while (in_m) {
-        const uint32_t k = __ffs(in_m) - 1;
-        in_m &= in_m - 1;
-        push(DIM != 0 || lm >= 0 ? sw[k][lm] : __ldg(src + (size_t)k * g.N + im));
-    }
-    uint32_t in_p = (uint32_t)c_pl & LOW;
-    while (in_p) {
-        const uint32_t k = __ffs(in_p) - 1;
-        in_p &= in_p - 1;
-        push(DIM != 0 || lp >= 0 ? sw[k][lp] : __ldg(src + (size_t)k * g.N + ip));
-    }
+    if (!out) return;
+    // The site's new count: its stayers and both neighbours' arrivals.
+    const uint32_t n = __popc(stays((uint32_t)lid)) + __popc((sc[tile_minus((uint32_t)lid, x)] >> S) & LOW) +
+                       __popc(sc[tile_plus((uint32_t)lid, x)] & LOW);
     const uint32_t nw = n < (uint32_t)S ? n : (uint32_t)S;
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, nw);
     const uint32_t seg = i >> PB_SHIFT;
@@ -547,7 +573,7 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
     const uint32_t listed = rx_sites && rs->rx_skip == 0 ? rs->rx_count : 0xFFFFFFFFu;
     const bool all = listed > rx_cap;
     const uint32_t n = all ? g.N : listed;
-    const unsigned long long th = timestep_hash(rs->seed, rs->step, 3);
+    const unsigned long long th = rs->th[3];
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         // The z sweep wrote this buffer, so its sites are packed (occupied
         // slots first, whatever the input had): only the planes holding
@@ -566,7 +592,7 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
             t = e.y >> 8;
             s.load_first(lat, g.N, i, BPS == 1 ? (np + 3u) / 4u : np);
         }
-        if (react_site<BPS, S>(s, t, i, th, m, rs, list, cap)) {
+        if (react_site<BPS, S, 0>(s, t, i, th, m, rs, list, cap)) {
             s.store(lat, g.N, i);
             if (pb) {
                 // Products may fill slots above the segment's bound.
@@ -608,7 +634,7 @@ __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__re
 __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode)
 {
     rs->seed = seed;
-    rs->step = first;
+    set_step(rs, seed, first);
     rs->end_step = first + n;
     rs->status = LMB_OK;
     rs->failed_step = 0;
@@ -640,7 +666,7 @@ __global__ void begin_batch_kernel(RunState *const *rs_ptrs, const uint32_t *see
     RunState *rs = rs_ptrs[j];
     const uint32_t f = firsts ? firsts[j] : first;
     rs->seed = seeds[j];
-    rs->step = f;
+    set_step(rs, seeds[j], f);
     rs->end_step = f + (counts ? counts[j] : n);
     rs->status = LMB_OK;
     rs->failed_step = 0;
@@ -857,6 +883,28 @@ bool slots_supported(int bps, int slots)
     return false;
 }
 
+// Dynamic shared memory of sweep_int_kernel<S, *, NT>.
+static size_t sweep_int_smem(int S, int NT) { return (size_t)NT * ((size_t)S * 4 + 8 + (size_t)S * 2); }
+
+// Raises kernel K's dynamic shared-memory limit once per device to the
+// largest size asked for so far (setting it on every launch costs host time).
+// One cache per kernel: instantiations share a function type, not a limit.
+template <auto K>
+static cudaError_t raise_smem_limit(size_t bytes)
+{
+    static size_t granted[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (bytes <= 48 * 1024 || bytes <= granted[dev]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // The whole unified L1 / shared array as shared memory, so that as many
+    // blocks fit as the registers allow.
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess) granted[dev] = bytes;
+    return e;
+}
+
 cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint32_t *dst, const uint8_t *sites,
                          const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
                          uint32_t *rx_sites, uint32_t rx_cap, const uint32_t *pb_src, uint32_t *pb_dst,
@@ -867,7 +915,7 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
     // Plane bounds need each warp on one whole segment of 32 sites.
     if (g.X % 32u != 0) pb_src = pb_dst = nullptr;
     if (!pb_src || !pb_dst) pb_src = pb_dst = nullptr;
-    if (bps == 4 && pb_src) {
+    if (bps == 4 && pb_src && g.X <= (uint32_t)SWEEP_THREADS) {
         // IntLattices with plane bounds: y and z tiles of SWEEP_PB_TILE sites
         // along the axis, one segment across.
         if (dim != 0) {
@@ -883,17 +931,26 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
         }
         count_launch();
         constexpr int YZ = SWEEP_PB_YZ_THREADS;
+        cudaError_t e;
 #define LMB_INT_SWEEP(S_)                                                                                        \
     if (slots == S_) {                                                                                          \
-        if (dim == 0)                                                                                           \
-            sweep_int_kernel<S_, 0, SWEEP_THREADS><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list,  \
-                                                                               cap, nullptr, 0, pb_src, pb_dst); \
-        else if (dim == 1)                                                                                      \
-            sweep_int_kernel<S_, 1, YZ><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap,       \
-                                                                    nullptr, 0, pb_src, pb_dst);                \
-        else                                                                                                    \
-            sweep_int_kernel<S_, 2, YZ><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap,       \
-                                                                    rx_sites, rx_cap, pb_src, pb_dst);          \
+        if (dim == 0) {                                                                                         \
+            const size_t sm = sweep_int_smem(S_, SWEEP_THREADS);                                                \
+            if ((e = raise_smem_limit<sweep_int_kernel<S_, 0, SWEEP_THREADS>>(sm)) != cudaSuccess) return e;     \
+            sweep_int_kernel<S_, 0, SWEEP_THREADS><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, \
+                                                                                cap, nullptr, 0, pb_src,         \
+                                                                                pb_dst);                         \
+        } else if (dim == 1) {                                                                                  \
+            const size_t sm = sweep_int_smem(S_, YZ);                                                           \
+            if ((e = raise_smem_limit<sweep_int_kernel<S_, 1, YZ>>(sm)) != cudaSuccess) return e;               \
+            sweep_int_kernel<S_, 1, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,      \
+                                                                     nullptr, 0, pb_src, pb_dst);               \
+        } else {                                                                                                \
+            const size_t sm = sweep_int_smem(S_, YZ);                                                           \
+            if ((e = raise_smem_limit<sweep_int_kernel<S_, 2, YZ>>(sm)) != cudaSuccess) return e;               \
+            sweep_int_kernel<S_, 2, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,      \
+                                                                     rx_sites, rx_cap, pb_src, pb_dst);         \
+        }                                                                                                       \
         return cudaGetLastError();                                                                              \
     }
         LMB_INT_SWEEP(4)

@@ -113,7 +113,7 @@ __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Ge
     const uint32_t n = *(volatile uint32_t *)&rs->ovf_count;
     const uint32_t carried = rs->carried;
     if (n == 0) {
-        if (tid == 0) rs->step++;
+        if (tid == 0) set_step(rs, rs->seed, rs->step + 1);
         return;
     }
     if (n > cap) {
@@ -183,7 +183,7 @@ __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Ge
         rs->carried = kept;
     }
     __threadfence();
-    rs->step++;
+    set_step(rs, rs->seed, rs->step + 1);
 }
 
 template <int BPS, int S>

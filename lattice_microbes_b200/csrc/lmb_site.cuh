@@ -343,8 +343,6 @@ __device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_
     }
 }
 
-constexpr int MAX_STOICH = 32;
-
 // The first two exits of react_site, for a site of type t holding n
 // particles whose zeroth-order propensity is a0 and whose reaction draw is
 // r0: false when the reaction step cannot change the site.  The reaction
@@ -369,7 +367,10 @@ __device__ __forceinline__ bool reaction_may_fire(uint32_t n, float a0, uint32_t
 
 // Table propensity sum in slot order, double precision probability, at most
 // one reaction; returns true when the site changed (s updated in place).
-template <int BPS, int S>
+// CAP > 0: the reaction's candidates are sorted in a list of CAP registers
+// (nothing in local memory; for kernels whose registers are scarce and whose
+// models have few candidates per site); CAP == 0: in a 64-entry array.
+template <int BPS, int S, int CAP>
 __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uint32_t gi, unsigned long long th,
                                            const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap)
 {
@@ -407,42 +408,77 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
     // determineReactionIndex (byte_reaction_dev.cu:146-176) visits every
     // reaction in index order; a reaction whose propensity is 0 changes
     // nothing, and only the zeroth-order reactions and those whose first
-    // reactant is in the site can have a nonzero one.  So the same steps are
-    // taken over those candidates, merged into index order (the full scan
-    // when there are too many to hold).
-    constexpr int MAX_CAND = 64;
-    uint32_t cand[MAX_CAND];
+    // reactant is in the site can have a nonzero one.  Those candidates are
+    // gathered from the reaction lists of the zeroth-order reactions and of
+    // each species held, sorted, repeats dropped (a species held twice gives
+    // its reactions once), and visited in index order; when there are more
+    // than the list holds, every reaction is visited instead.
+    auto visit = [&](uint32_t rx) {
+        const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
+        if (prop > 0.0f) {
+            if (rp > 0.0f) idx = rx;
+            rp = __fsub_rn(rp, prop);
+        }
+    };
+    constexpr int LEN = CAP > 0 ? CAP : 64;
+    uint32_t cand[LEN];
     int nc = 0;
     bool all = false;
-    {
-        const uint32_t z0 = tload(m.rx_off), z1 = tload(m.rx_off + 1);
-        for (uint32_t e = z0; e < z1 && !all; e++) {
-            if (nc < MAX_CAND) cand[nc++] = tload(m.rx_list + e);
+    // CAP > 0: insertion by compare-and-swap over fixed positions (unused
+    // ones hold ~0u, above every index, so carrying the larger value forward
+    // keeps the list sorted); CAP == 0: appended, sorted below.
+    auto insert = [&](uint32_t v) {
+        if (CAP > 0) {
+            bool dup = false;
+#pragma unroll
+            for (int j = 0; j < LEN; j++) dup |= cand[j] == v;
+            if (dup) return;
+            if (nc == LEN) {
+                all = true;
+                return;
+            }
+            uint32_t carry = v;
+#pragma unroll
+            for (int j = 0; j < LEN; j++) {
+                const uint32_t c = cand[j];
+                const bool sw = c > carry;
+                cand[j] = sw ? carry : c;
+                carry = sw ? c : carry;
+            }
+            nc++;
+        } else {
+            if (nc < LEN) cand[nc++] = v;
             else all = true;
         }
+    };
+    if (CAP > 0) {
+#pragma unroll
+        for (int j = 0; j < LEN; j++) cand[j] = 0xFFFFFFFFu;
+    }
+    {
+        const uint32_t z0 = tload(m.rx_off), z1 = tload(m.rx_off + 1);
+        for (uint32_t e = z0; e < z1 && !all; e++) insert(tload(m.rx_list + e));
 #pragma unroll
         for (int k = 0; k < S; k++) {
             const uint32_t p = s.slot(k);
             if (p > 0 && p <= m.ns && !all) {
                 const uint32_t e0 = tload(m.rx_off + p), e1 = tload(m.rx_off + p + 1);
-                for (uint32_t e = e0; e < e1; e++) {
-                    if (nc < MAX_CAND) cand[nc++] = tload(m.rx_list + e);
-                    else all = true;
-                }
+                for (uint32_t e = e0; e < e1 && !all; e++) insert(tload(m.rx_list + e));
             }
         }
     }
     if (all) {
-        for (uint32_t rx = 0; rx < m.nr; rx++) {
-            const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
-            if (prop > 0.0f) {
-                if (rp > 0.0f) idx = rx;
-                rp = __fsub_rn(rp, prop);
-            }
+        for (uint32_t rx = 0; rx < m.nr; rx++) visit(rx);
+    } else if (CAP > 0) {
+        // Smallest off the front, the rest shifted down.
+        for (int q = 0; q < nc; q++) {
+            const uint32_t rx = cand[0];
+#pragma unroll
+            for (int j = 0; j + 1 < LEN; j++) cand[j] = cand[j + 1];
+            visit(rx);
         }
     } else {
-        // Ascending order (insertion sort of a few entries); a species held
-        // twice contributes its list twice, so repeats are skipped.
+        // Insertion sort of the few entries; repeats skipped.
         for (int a = 1; a < nc; a++) {
             const uint32_t v = cand[a];
             int b = a - 1;
@@ -453,53 +489,80 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
             cand[b + 1] = v;
         }
         for (int q = 0; q < nc; q++) {
-            const uint32_t rx = cand[q];
-            if (q > 0 && rx == cand[q - 1]) continue;
-            const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
-            if (prop > 0.0f) {
-                if (rp > 0.0f) idx = rx;
-                rp = __fsub_rn(rp, prop);
-            }
+            if (q > 0 && cand[q] == cand[q - 1]) continue;
+            visit(cand[q]);
         }
     }
     atomicAdd(&rs->reactions, 1ull);
 
-    // Stoichiometry of the chosen reaction, ascending species.
+    // evaluateReaction (byte_reaction_dev.cu:179-258) with the chosen
+    // reaction's sparse stoichiometry (ascending species): reactants are
+    // taken out in slot order, products appended by ascending species id.
+    // The consumed species are held in two registers (a reaction of order
+    // two or less consumes at most two); a stoichiometry with more negative
+    // entries goes through a per-entry count.
     const uint32_t e0 = tload(m.stoich_off + idx), e1 = tload(m.stoich_off + idx + 1);
-    const int ne = (int)(e1 - e0) < MAX_STOICH ? (int)(e1 - e0) : MAX_STOICH;
-    uint32_t sp[MAX_STOICH];
-    int dlt[MAX_STOICH];
-    for (int e = 0; e < ne; e++) {
-        sp[e] = tload(m.stoich_sp + e0 + e);
-        dlt[e] = tload(m.stoich_d + e0 + e);
+    uint32_t c_sp0 = 0xFFFFFFFFu, c_sp1 = 0xFFFFFFFFu;
+    int c_n0 = 0, c_n1 = 0, negatives = 0;
+    for (uint32_t e = e0; e < e1; e++) {
+        const int d = tload(m.stoich_d + e);
+        if (d < 0) {
+            if (negatives == 0) {
+                c_sp0 = tload(m.stoich_sp + e);
+                c_n0 = -d;
+            } else if (negatives == 1) {
+                c_sp1 = tload(m.stoich_sp + e);
+                c_n1 = -d;
+            }
+            negatives++;
+        }
     }
-    // Survivors in slot order; a consumed reactant bumps its count.
     SiteWords<BPS, S> out;
     out.clear();
     int n = 0;
+    if (negatives <= 2) {
 #pragma unroll
-    for (int k = 0; k < S; k++) {
-        const uint32_t q = s.slot(k);
-        if (q > 0) {
-            bool consumed = false;
-            for (int e = 0; e < ne; e++) {
-                if (sp[e] == q - 1) {
-                    if (dlt[e] < 0) {
-                        dlt[e]++;
-                        consumed = true;
-                    }
-                    break;
-                }
+        for (int k = 0; k < S; k++) {
+            const uint32_t q = s.slot(k);
+            if (q > 0) {
+                if (q - 1 == c_sp0 && c_n0 > 0) c_n0--;
+                else if (q - 1 == c_sp1 && c_n1 > 0) c_n1--;
+                else out.put(n++, q);
             }
-            if (!consumed) out.put(n++, q);
+        }
+    } else {
+        // Any number of consumed species: the entry of each particle's
+        // species is looked up and its remaining count kept in a bit of
+        // `used` per consumed particle (S <= 32 slots, so at most S taken).
+        uint32_t taken_bits = 0;  // bit k: slot k consumed
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            const uint32_t q = s.slot(k);
+            if (q > 0) {
+                int need = 0;
+                for (uint32_t e = e0; e < e1; e++)
+                    if (tload(m.stoich_sp + e) == q - 1) {
+                        need = -tload(m.stoich_d + e);
+                        break;
+                    }
+                // Consumed when fewer of this species than it needs were
+                // taken in the slots before.
+                int before = 0;
+#pragma unroll
+                for (int j = 0; j < k; j++)
+                    if (((taken_bits >> j) & 1u) && s.slot(j) == q) before++;
+                if (need > before) taken_bits |= 1u << k;
+                else out.put(n++, q);
+            }
         }
     }
     // Products by ascending species id; extra ones overflow.  A stoichiometry
     // left negative (reactant missing) adds nothing.
     uint32_t seq = 0;
-    for (int e = 0; e < ne; e++) {
-        for (int j = 0; j < dlt[e]; j++) {
-            const uint32_t p = sp[e] + 1;
+    for (uint32_t e = e0; e < e1; e++) {
+        const int d = tload(m.stoich_d + e);
+        const uint32_t p = tload(m.stoich_sp + e) + 1;
+        for (int j = 0; j < d; j++) {
             if (n < S) out.put(n++, p);
             else push_overflow(rs, list, cap, 4u, gi, seq++, p);
         }

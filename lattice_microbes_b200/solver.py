@@ -288,6 +288,24 @@ class Batch:
                                                    _p(self._counts, L.u32p), overflow_mode),
                 "lmb_batch_run_ranges_async")
 
+    def autotune(self, seeds, first_timestep, timesteps):
+        """Chooses each lattice size's tile shape by timing the whole batch
+        (lmb_batch_autotune); the lattices end where they started.  Returns
+        the best trial's milliseconds."""
+        sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+        ms = C.c_float()
+        L.check(L.lib().lmb_batch_autotune(self.handle, _p(sd, L.u32p), first_timestep, timesteps, C.byref(ms)),
+                "lmb_batch_autotune")
+        return ms.value
+
+    def plan(self):
+        """(Ty, Tz) tile of each lattice."""
+        n = len(self.lattices)
+        ty = np.zeros(n, dtype=np.uint32)
+        tz = np.zeros(n, dtype=np.uint32)
+        L.check(L.lib().lmb_batch_plan(self.handle, _p(ty, L.u32p), _p(tz, L.u32p)), "lmb_batch_plan")
+        return list(zip(ty.tolist(), tz.tolist()))
+
     def set_lattices(self, lattices, models):
         n = len(lattices)
         la = (L.vp * n)(*[l.handle for l in lattices])

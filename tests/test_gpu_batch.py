@@ -67,3 +67,39 @@ def test_batch_failure_is_per_lattice(gpu):
     assert np.array_equal(pb[0].get_native()[0], ref_bad)
     batch.close()
     ctx.close()
+
+
+def test_batch_autotune_keeps_state_and_results(gpu):
+    """lmb_batch_autotune times tile shapes per lattice size from the saved
+    states and leaves every lattice where it was; the batch then runs with the
+    chosen plan and still gives every lattice the oracle's result."""
+    from lattice_microbes_b200.solver import Batch, Context
+    ctx = Context(0)
+    edges = [16, 24, 32, 48, 64, 16, 32]
+    specs = [configs.config0(seed=200 + k, edge=e, nA=int(0.2 * e ** 3), nB=int(0.2 * e ** 3))
+             for k, e in enumerate(edges)]
+    seeds = [77 + k for k in range(len(specs))]
+    pairs = [_make(ctx, s) for s in specs]
+    batch = Batch(ctx, [p[0] for p in pairs], [p[1] for p in pairs])
+    before = [lat.get_native()[0] for lat, _ in pairs]
+    ms = batch.autotune(seeds, 0, 8)
+    assert 0 < ms < 1e6
+    for (lat, _), b in zip(pairs, before):
+        assert np.array_equal(lat.get_native()[0], b)
+    plan = batch.plan()
+    assert len(plan) == len(edges)
+    for e, (ty, tz) in zip(edges, plan):
+        assert ty >= 1 and tz >= 1 and e % ty == 0 and e % tz == 0
+    # Lattices of one size share a plan.
+    assert plan[0] == plan[5] and plan[2] == plan[6]
+    rc, st = batch.run(seeds, 0, 20)
+    assert rc == 0
+    for (lat, m), spec, seed in zip(pairs, specs, seeds):
+        ref, rc_ref, _ = oracle_run(oracle_tables(spec), spec.lattice, spec.sites, seed, 0, 20)
+        assert rc_ref == 0
+        assert np.array_equal(lat.get_native()[0], ref), spec.name
+    batch.close()
+    for lat, m in pairs:
+        lat.close()
+        m.close()
+    ctx.close()
