@@ -428,15 +428,23 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     const unsigned long long th = rs->th[DIM];
     if (in) {
         sweep_neighbours<DIM>(g, x, y, z, lid, i, im, ip, lm, lp);
+        // Planes 0 and 1 are read with the bound rather than after it (a
+        // plane at or above the bound reads as zero, so the early read is
+        // harmless): nearly every segment needs plane 0 and most plane 1,
+        // and the bound's round trip no longer comes first.
         const uint32_t npl = planes_at<S>(pb_src, i);
-        for (uint32_t k = 0; k < npl; k++) {
+        const uint32_t v0 = __ldg(src + i), v1 = __ldg(src + (size_t)g.N + i);
+        t = __ldg(sites + i);
+        tm = __ldg(sites + im);
+        tp = __ldg(sites + ip);
+        sw[0][lid] = v0;
+        sw[1][lid] = v1;
+        occ = (v0 != 0u ? 1u : 0u) | (v1 != 0u ? 2u : 0u);
+        for (uint32_t k = 2; k < npl; k++) {
             const uint32_t v = __ldg(src + (size_t)k * g.N + i);
             sw[k][lid] = v;
             occ |= (v != 0u ? 1u : 0u) << k;
         }
-        t = __ldg(sites + i);
-        tm = __ldg(sites + im);
-        tp = __ldg(sites + ip);
     }
     so[lid] = occ | (out ? OUT : 0u);
     sc[lid] = 0;
