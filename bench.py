@@ -94,7 +94,7 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
-    ap.add_argument("--workload", choices=["crowded", "rodcell", "batch", "cme", "serve", "trajectory"],
+    ap.add_argument("--workload", choices=["crowded", "rodcell", "batch", "cme", "serve", "trajectory", "pair"],
                     default=DEFAULT_WORKLOAD,
                     help="crowded: one 128x128x256 IntLattice-16 (default); rodcell: one 64x64x128 ByteLattice-8; "
                          "batch: 256 bimolecular replicates of "
@@ -985,10 +985,102 @@ def run_serve(a):
     print(json.dumps(line), flush=True)
 
 
+def run_pair(a):
+    """Two large dense serving solves side by side against one after another:
+    the measurement behind the served form's bound.  Each solve is a
+    serving request of the largest kind (edge 128, ByteLattice-16, 2
+    particles per site, 30 species) on the per-phase schedule the server
+    gives large dense solves, T timesteps.  Side by side: two contexts (two
+    streams), both runs enqueued before either is waited for, as the
+    server's two solo streams run them.  One after another: the same two runs,
+    the second enqueued after the first has finished.  Both arms are timed
+    from the first enqueue to the last completion (best of --steps), with each
+    stream's CUDA-event time beside them."""
+    import torch
+
+    from lattice_microbes_b200 import _lib as LL
+    from lattice_microbes_b200 import configs
+    from lattice_microbes_b200.solver import Context, Lattice, Model, compose_seed
+
+    torch.cuda.set_device(0)
+    T = a.timesteps_per_step or 200
+    reqs = [configs.ServeRequest(index=k, arrival=0.0, edge=128, ns=30, density=2.0, timesteps=T, seed=900 + k)
+            for k in range(2)]
+    specs = [_to_byte16(configs.serve_problem(r)) for r in reqs]
+    ctxs = [Context(0), Context(0)]
+    models, lats = [], []
+    for c, sp in zip(ctxs, specs):
+        m = Model.from_spec(c, sp)
+        lat = Lattice(c, sp.X, sp.Y, sp.Z, 16, 1)
+        lat.set_schedule(LL.LMB_SCHEDULE_PHASES)
+        lat.set_native(sp.lattice, sp.sites)
+        models.append(m)
+        lats.append(lat)
+    seeds = [compose_seed(77, k) for k in range(2)]
+    streams = [torch.cuda.ExternalStream(c.stream, device=torch.device("cuda", 0)) for c in ctxs]
+    step = 0
+    for _ in range(max(1, a.warmup)):
+        for lat, m, sd in zip(lats, models, seeds):
+            lat.run(m, sd, step, T)
+        step += T
+
+    def timed(side_by_side):
+        nonlocal step
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(2)]
+        torch.cuda.synchronize(0)
+        t0 = time.perf_counter()
+        for k in range(2):
+            with torch.cuda.stream(streams[k]):
+                ev[k][0].record(streams[k])
+                lats[k].run_async(models[k], seeds[k], step, T)
+                ev[k][1].record(streams[k])
+            if not side_by_side:
+                lats[k].wait()
+        for k in range(2):
+            if side_by_side:
+                lats[k].wait()
+        wall = time.perf_counter() - t0
+        step += T
+        per = [e0.elapsed_time(e1) for e0, e1 in ev]
+        return wall, per
+
+    seq = [timed(False) for _ in range(a.steps)]
+    par = [timed(True) for _ in range(a.steps)]
+    seq_ms = min(w * 1e3 for w, _ in seq)
+    par_ms = min(w * 1e3 for w, _ in par)
+    sites = specs[0].nsites
+    line = {
+        "metric": "site-steps/s",
+        "value": 2 * sites * T / (par_ms / 1e3),
+        "unit": "site-steps/s",
+        "n_gpus": 1,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": par_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (two seeded serving requests, lattice_microbes_b200.configs.serve_problem)",
+        "config": {"workload": "two 128^3 ByteLattice-16 serving solves, 2 particles per site, 30 species, "
+                               "per-phase schedule, %d timesteps each" % T},
+        "one_after_another": {"ms": seq_ms, "site_steps_per_s": 2 * sites * T / (seq_ms / 1e3),
+                              "ms_per_solve": [p for p in seq[-1][1]]},
+        "side_by_side": {"ms_wall": par_ms, "ms_per_stream": par[-1][1]},
+        "gain": seq_ms / par_ms,
+    }
+    print(json.dumps(line), flush=True)
+    for lat, m in zip(lats, models):
+        lat.close()
+        m.close()
+    for c in ctxs:
+        c.close()
+
+
 def run_trajectory(a):
     """The rod-cell model as a trajectory with output: each bench step is 500
-    timesteps in runs of 100, after each run the species counts and a lattice
-    frame go to a `.lm` file (lmb_lmfile_append_lattice_device: GPU transpose,
+    timesteps in runs of 100, after each run the species counts (taken inside
+    the run) and a lattice frame go to a `.lm` file (lmb_lmfile_append_lattice_device: GPU transpose,
     copy to pinned memory, gzip-1 16^3 chunks on the writer thread), and the
     timed region ends when the file is flushed.  The same loop without the
     file is timed beside it; both are wall-clock (host calls included)."""
@@ -1012,15 +1104,19 @@ def run_trajectory(a):
     tmp = tempfile.mkdtemp()
 
     def loop(writer, first, steps):
+        # With output: each run takes the species totals in its own work
+        # (lmb_run_counts_async); without: the runs alone.
         t = first
         for _ in range(steps):
             for _ in range(T // every):
-                lat.run(model, 7, t, every)
-                t += every
-                c = lat.species_counts(spec.ns)
                 if writer is not None:
+                    _, _, c = lat.run_counts(model, 7, t, every, spec.ns)
+                    t += every
                     writer.append_species_counts(0, [t * spec.tau], np.asarray(c[1:], np.int32)[None, :])
                     writer.append_lattice_device(0, t * spec.tau, lat)
+                else:
+                    lat.run(model, 7, t, every)
+                    t += every
         if writer is not None:
             writer.flush()
         return t
@@ -1098,6 +1194,8 @@ if __name__ == "__main__":
         run_cme(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "pair":
+        run_pair(args)
     elif args.workload == "trajectory":
         run_trajectory(args)
     else:

@@ -218,6 +218,20 @@ int lmb_run(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_
 int lmb_run_async(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
                   uint32_t number_timesteps, int overflow_mode);
 int lmb_run_wait(lmb_lattice *lattice, lmb_run_stats *stats);
+/* lmb_run_async that also takes the lattice's species totals at the end of
+ * the run (recordSpeciesCounts, MpdRdmeSolver.cu:933-942, with
+ * ByteLattice::getParticleCounts, ByteLattice.cpp:495-520) inside the run's
+ * own work: on the fused schedule the last timestep's kernel adds the
+ * particles of the sites each block stores into per-block histograms, one
+ * atomic per species, and the overflow resolution adds those it puts back;
+ * on the per-phase schedule one pass after the last timestep reads only the
+ * word planes below each segment's plane bound.  The totals come back with
+ * the run state: lmb_run_counts_wait returns them, counts[0..number_species]
+ * as lmb_lattice_species_counts gives them, with no further launch or
+ * synchronization. */
+int lmb_run_counts_async(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
+                         uint32_t number_timesteps, int overflow_mode, uint32_t number_species);
+int lmb_run_counts_wait(lmb_lattice *lattice, lmb_run_stats *stats, uint64_t *counts);
 
 /* lmb_run with a CUDA event pair around every kernel on the lattice's
  * stream; phase_ms[6] / phase_launches[6] receive the summed device time and

@@ -257,7 +257,11 @@ public:
             ev = std::min<uint64_t>(ev, nextCounts > step ? nextCounts : step + 1);
             ev = std::min<uint64_t>(ev, nextLattice > step ? nextLattice : step + 1);
             if (hookEnabled) ev = std::min<uint64_t>(ev, nextHook > step ? nextHook : step + 1);
-            run(step, (uint32_t)(ev - step));
+            // A step whose records need the species totals, with no hook that
+            // could change the lattice first, takes them in the run's own work.
+            const bool records = ev >= nextCounts || ev >= nextLattice;
+            const bool hooks = hookEnabled && ev >= nextHook;
+            run(step, (uint32_t)(ev - step), records && !hooks);
             step = (uint32_t)ev;
             time = step * tau_;
             if (step >= nextLattice || step >= nextCounts || (hookEnabled && step >= nextHook)) {
@@ -347,10 +351,28 @@ private:
         return d;
     }
 
-    void run(uint32_t first, uint32_t n)
+    void run(uint32_t first, uint32_t n, bool withCounts = false)
     {
-        const int rc = lmb_run(lattice_, model_, seed_, first, n, overflow_, &stats_);
+        int rc;
+        if (withCounts) {
+            runCounts_.assign(ns_ + 1, 0);
+            rc = lmb_run_counts_async(lattice_, model_, seed_, first, n, overflow_, ns_);
+            if (rc == LMB_OK) rc = lmb_run_counts_wait(lattice_, &stats_, runCounts_.data());
+        } else {
+            rc = lmb_run(lattice_, model_, seed_, first, n, overflow_, &stats_);
+        }
+        runCountsValid_ = withCounts && rc == LMB_OK;
         if (rc != LMB_OK) throw Exception(rc, "runTimestep");
+    }
+
+    /* The lattice's species totals: those the last run took, unless the
+     * lattice was changed since. */
+    std::vector<uint64_t> speciesCounts()
+    {
+        if (runCountsValid_) return runCounts_;
+        std::vector<uint64_t> c(ns_ + 1);
+        check(lmb_lattice_species_counts(lattice_, ns_, c.data()), "recordSpeciesCounts");
+        return c;
     }
 
     void download()
@@ -364,12 +386,12 @@ private:
     {
         check(lmb_lattice_set_native(lattice_, host_.particles.data(), withSites ? host_.sites.data() : nullptr),
               "copyToGPU");
+        runCountsValid_ = false;
     }
 
     void recordSpeciesCounts(double time)
     {
-        std::vector<uint64_t> c(ns_ + 1);
-        check(lmb_lattice_species_counts(lattice_, ns_, c.data()), "recordSpeciesCounts");
+        std::vector<uint64_t> c = speciesCounts();
         c.erase(c.begin());  // species ids are 1-based
         if (out_) {
             std::vector<int32_t> row(c.begin(), c.end());
@@ -382,8 +404,7 @@ private:
      * the frame. */
     void writeLatticeRecord(double time)
     {
-        std::vector<uint64_t> c(ns_ + 1);
-        check(lmb_lattice_species_counts(lattice_, ns_, c.data()), "writeLatticeData");
+        const std::vector<uint64_t> c = speciesCounts();
         for (uint32_t s = 1; s <= ns_; s++)
             if (c[s] > maxParticleCounts_[s]) maxParticleCounts_[s] = (uint32_t)c[s];
         if (out_) check(lmb_lmfile_append_lattice_device(out_, replicate_, time, lattice_), "writeLatticeData");
@@ -471,6 +492,8 @@ private:
     double spacing_ = 0.0, tau_ = 0.0;
     HostLattice host_;
     lmb_run_stats stats_{};
+    std::vector<uint64_t> runCounts_;  // species totals the last run took
+    bool runCountsValid_ = false;      // and the lattice is unchanged since
     bool stop_ = false;
     std::vector<uint32_t> maxParticleCounts_, maxSiteCounts_;
     lmb_lmfile *out_ = nullptr;

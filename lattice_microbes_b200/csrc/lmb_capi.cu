@@ -76,6 +76,11 @@ struct lmb_lattice {
     uint32_t nseg;
     unsigned long long *counts_dev;
     uint32_t counts_len;
+    // Species counts of the last lmb_run_counts_async (pinned), and the
+    // species count they were taken for (~0u: none pending).
+    unsigned long long *counts_host;
+    uint32_t counts_host_len;
+    uint32_t pending_count_ns;
     bool validated;
     uint32_t max_species, max_site_type;
     // Schedule: fused tile kernel (one launch per timestep) or per-phase kernels.
@@ -675,6 +680,7 @@ extern "C" int lmb_lattice_destroy(lmb_lattice *l)
     if (l->rx_sites) cudaFree(l->rx_sites);
     if (l->pb) cudaFree(l->pb);
     if (l->counts_dev) cudaFree(l->counts_dev);
+    if (l->counts_host) cudaFreeHost(l->counts_host);
     if (l->rs_host) cudaFreeHost(l->rs_host);
     for (auto &gr : l->graph)
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
@@ -795,18 +801,26 @@ extern "C" int lmb_lattice_device_buffers(lmb_lattice *l, void **particles, void
     return LMB_OK;
 }
 
-extern "C" int lmb_lattice_species_counts(lmb_lattice *l, uint32_t ns, uint64_t *counts)
+// Device counters for ns + 1 species totals (kept between calls).
+static int ensure_counts_dev(lmb_lattice *l, uint32_t ns)
 {
-    if (!l || !counts) return LMB_E_ARG;
-    if (l->pending) return LMB_E_STATE;
-    lmb_ctx *c = l->ctx;
-    CK(cudaSetDevice(c->device));
     if (!l->counts_dev || l->counts_len < ns + 1) {
         if (l->counts_dev) cudaFree(l->counts_dev);
         l->counts_dev = nullptr;
         CK(cudaMalloc(&l->counts_dev, sizeof(unsigned long long) * (ns + 1)));
         l->counts_len = ns + 1;
     }
+    return LMB_OK;
+}
+
+extern "C" int lmb_lattice_species_counts(lmb_lattice *l, uint32_t ns, uint64_t *counts)
+{
+    if (!l || !counts) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    int rc = ensure_counts_dev(l, ns);
+    if (rc) return rc;
     CK(cudaMemsetAsync(l->counts_dev, 0, sizeof(unsigned long long) * (ns + 1), c->stream));
     CK(launch_counts((int)l->bps, (int)l->slots, l->buf[l->cur], l->g, ns, l->counts_dev, c->stream));
     CK(cudaMemcpyAsync(counts, l->counts_dev, sizeof(uint64_t) * (ns + 1), cudaMemcpyDeviceToHost, c->stream));
@@ -938,7 +952,10 @@ static int validate_for_model(lmb_lattice *l, const lmb_model *m)
     return LMB_OK;
 }
 
-extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_t first, uint32_t n, int mode)
+// count_ns ~0u: no species count; otherwise the lattice's species totals at
+// the end of the run are taken in the run's own work (lmb_run_counts_async).
+static int run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_t first, uint32_t n, int mode,
+                     uint32_t count_ns)
 {
     if (!l || !mc) return LMB_E_ARG;
     if (l->pending) return LMB_E_STATE;
@@ -954,7 +971,23 @@ extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed,
     }
     int rc = validate_for_model(l, m);
     if (rc) return rc;
-    CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream));
+    const bool counting = count_ns != ~0u;
+    // The fused kernel counts in its last launch when its work list can hold
+    // the histogram; otherwise one pass over the final lattice follows the run.
+    const bool in_kernel = counting && n > 0 && l->schedule == LMB_SCHEDULE_FUSED && count_ns + 1 <= l->tile.R;
+    if (counting) {
+        rc = ensure_counts_dev(l, count_ns);
+        if (rc) return rc;
+        if (!l->counts_host || l->counts_host_len < count_ns + 1) {
+            if (l->counts_host) cudaFreeHost(l->counts_host);
+            l->counts_host = nullptr;
+            CK(cudaMallocHost(&l->counts_host, sizeof(unsigned long long) * (count_ns + 1)));
+            l->counts_host_len = count_ns + 1;
+        }
+        CK(cudaMemsetAsync(l->counts_dev, 0, sizeof(unsigned long long) * (count_ns + 1), c->stream));
+    }
+    CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream, in_kernel ? first + n - 1 : ~0u, count_ns,
+                        l->counts_dev));
     CK(reset_plane_bounds(l, c->stream));
     l->pending_cur0 = l->cur;
     uint32_t done = 0;
@@ -969,11 +1002,46 @@ extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed,
         }
     }
     for (; done < n; done++) CK(enqueue_step(l, m, c->stream));
+    if (counting) {
+        if (!in_kernel) {
+            // After a per-phase run the current buffer's plane bounds hold:
+            // only the planes below them are read.
+            const uint32_t *pb = l->schedule == LMB_SCHEDULE_PHASES && n > 0 ? plane_bounds(l, l->cur) : nullptr;
+            CK(launch_counts((int)l->bps, (int)l->slots, l->buf[l->cur], l->g, count_ns, l->counts_dev, c->stream,
+                             pb));
+        }
+        CK(cudaMemcpyAsync(l->counts_host, l->counts_dev, sizeof(unsigned long long) * (count_ns + 1),
+                           cudaMemcpyDeviceToHost, c->stream));
+    }
     CK(cudaMemcpyAsync(l->rs_host, l->rs, sizeof(RunState), cudaMemcpyDeviceToHost, c->stream));
     l->pending = true;
     l->pending_first = first;
     l->pending_n = n;
+    l->pending_count_ns = count_ns;
     return LMB_OK;
+}
+
+extern "C" int lmb_run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_t first, uint32_t n, int mode)
+{
+    return run_async(l, mc, seed, first, n, mode, ~0u);
+}
+
+extern "C" int lmb_run_counts_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_t first, uint32_t n,
+                                    int mode, uint32_t number_species)
+{
+    if (number_species == ~0u) return LMB_E_ARG;
+    return run_async(l, mc, seed, first, n, mode, number_species);
+}
+
+extern "C" int lmb_run_counts_wait(lmb_lattice *l, lmb_run_stats *st, uint64_t *counts)
+{
+    if (!l || !counts) return LMB_E_ARG;
+    if (!l->pending || l->pending_count_ns == ~0u) return LMB_E_STATE;
+    const uint32_t ns = l->pending_count_ns;
+    const int rc = lmb_run_wait(l, st);
+    for (uint32_t s = 0; s <= ns; s++) counts[s] = l->counts_host[s];
+    counts[0] = 0;
+    return rc;
 }
 
 extern "C" int lmb_run_wait(lmb_lattice *l, lmb_run_stats *st)

@@ -482,6 +482,35 @@ __device__ __forceinline__ void tile_store(uint32_t *__restrict__ dst, const Geo
     }
 }
 
+// Species counts of the tile's owned rows from (w, o), added to counts[0..ns]
+// (a species id above ns goes to entry 0): a shared-memory histogram in the
+// work list (R >= ns + 1 entries, free after the timestep), then one global
+// atomic per species the tile holds.
+template <int BPS, int S>
+__device__ __forceinline__ void tile_count(const Geometry &g, const TileShape &ts, const TileSmem &t,
+                                           const uint32_t *w, const uint32_t *o, uint32_t ns,
+                                           unsigned long long *counts)
+{
+    const uint32_t X = g.X, R = ts.R, MW = ts.MW, orows = ts.Ty * ts.Tz, tid = threadIdx.x, nthr = blockDim.x;
+    uint32_t *hist = t.work;
+    for (uint32_t b = tid; b <= ns; b += nthr) hist[b] = 0;
+    __syncthreads();
+    for (uint32_t i = tid; i < orows * X; i += nthr) {
+        const uint32_t q = i / X, x = i - q * X, r = t.zrow[q];
+        if (!((o[r * MW + (x >> 5)] >> (x & 31u)) & 1u)) continue;
+        SiteWords<BPS, S> s;
+        load_smem<BPS, S>(w, R, r * X + x, s);
+#pragma unroll
+        for (int k = 0; k < S; k++) {
+            const uint32_t p = s.slot(k);
+            if (p) atomicAdd(&hist[p <= ns ? p : 0u], 1u);
+        }
+    }
+    __syncthreads();
+    for (uint32_t b = tid; b <= ns; b += nthr)
+        if (hist[b]) atomicAdd(counts + b, (unsigned long long)hist[b]);
+}
+
 // One timestep of one tile (`tile` of the lattice's `ntiles`), run by the
 // whole block.  The block is flat (FUSED_THREADS threads); the tile's
 // logical bx x by layout (bx a multiple of 32, so a warp is 32 consecutive x
@@ -520,6 +549,9 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     tile_timestep<BPS, S, ROWS>(g, s_mt, rs, list, cap, ts, t, src_w, dst_w, src_o, dst_o, seed, step,
                                 with_reaction);
     tile_store<BPS, S>(dst, g, ts, t, src_w, src_o);
+    // The run's species count, at the timestep it was asked for.
+    const bool counting = step == rs->count_step;
+    if (counting) tile_count<BPS, S>(g, ts, t, src_w, src_o, rs->count_ns, rs->counts);
 
     // The last block to finish resolves the overflow queue and advances the
     // step counter.
@@ -533,7 +565,8 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     if (s_last) {
         __threadfence();
         if (tid == 0) rs->tiles_done = 0;
-        resolve_block_flat<BPS, S>(dst, sites, g, rs, list, cap, (OverflowEntry *)smem, tid, nthr, nullptr);
+        resolve_block_flat<BPS, S>(dst, sites, g, rs, list, cap, (OverflowEntry *)smem, tid, nthr, nullptr,
+                                   counting ? rs->counts : nullptr);
     }
 }
 

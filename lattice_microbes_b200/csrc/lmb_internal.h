@@ -93,6 +93,13 @@ struct RunState {
     // timestep_hash(seed, step, k) for the sub-steps k = 0..3 of `step`, set
     // with every change of step (the per-phase kernels read them here).
     unsigned long long th[4];
+    // Species counts taken inside the run: at timestep count_step the fused
+    // kernel adds the particles of the sites it stores (and the overflow
+    // resolution those it puts back) into counts[0..count_ns]; count_step is
+    // ~0u when no count is asked for.
+    uint32_t count_step;
+    uint32_t count_ns;
+    unsigned long long *counts;
 };
 
 
@@ -132,14 +139,20 @@ cudaError_t launch_resolve(int bytes_per_slot, int slots, uint32_t *lat, const u
                            uint32_t *pb, cudaStream_t stream);
 // Sets `count` plane bounds to `planes`.
 cudaError_t launch_fill_bounds(uint32_t *pb, uint32_t count, uint32_t planes, cudaStream_t stream);
+// count_step / count_ns / counts: RunState's in-run species count (count_step
+// ~0u: none).
 cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
-                             cudaStream_t stream);
+                             cudaStream_t stream, uint32_t count_step = ~0u, uint32_t count_ns = 0,
+                             unsigned long long *counts = nullptr);
 cudaError_t launch_begin_batch(RunState *const *rs_ptrs, const uint32_t *seeds, uint32_t count, uint32_t first,
                                uint32_t n, const uint32_t *firsts, const uint32_t *counts, uint32_t mode,
                                cudaStream_t stream);
 cudaError_t launch_gather_states(RunState *const *rs_ptrs, uint32_t count, RunState *out, cudaStream_t stream);
+// pb: the plane bounds of `lat` (only the planes below them are read), or
+// null.
 cudaError_t launch_counts(int bytes_per_slot, int slots, const uint32_t *lat, const Geometry &g,
-                          uint32_t ns, unsigned long long *counts, cudaStream_t stream);
+                          uint32_t ns, unsigned long long *counts, cudaStream_t stream,
+                          const uint32_t *pb = nullptr);
 cudaError_t launch_validate(int bytes_per_slot, int slots, const uint32_t *lat, const uint8_t *sites,
                             const Geometry &g, RunState *rs, cudaStream_t stream);
 cudaError_t launch_row_major_to_native(int bytes_per_slot, int slots, const void *rm_particles,

@@ -639,8 +639,12 @@ __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__re
 
 // Sets the run state for a new run without a host round trip.  The relaxed
 // handler's queue survives across runs; the classic one starts empty.
-__global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode)
+__global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
+                                 uint32_t count_step, uint32_t count_ns, unsigned long long *counts)
 {
+    rs->count_step = count_step;
+    rs->count_ns = count_ns;
+    rs->counts = counts;
     rs->seed = seed;
     set_step(rs, seed, first);
     rs->end_step = first + n;
@@ -673,6 +677,7 @@ __global__ void begin_batch_kernel(RunState *const *rs_ptrs, const uint32_t *see
     if (j >= count) return;
     RunState *rs = rs_ptrs[j];
     const uint32_t f = firsts ? firsts[j] : first;
+    rs->count_step = ~0u;
     rs->seed = seeds[j];
     set_step(rs, seeds[j], f);
     rs->end_step = f + (counts ? counts[j] : n);
@@ -724,10 +729,10 @@ cudaError_t launch_fill_bounds(uint32_t *pb, uint32_t count, uint32_t planes, cu
 }
 
 cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32_t n, uint32_t mode,
-                             cudaStream_t stream)
+                             cudaStream_t stream, uint32_t count_step, uint32_t count_ns, unsigned long long *counts)
 {
     count_launch();
-    begin_run_kernel<<<1, 1, 0, stream>>>(rs, seed, first, n, mode);
+    begin_run_kernel<<<1, 1, 0, stream>>>(rs, seed, first, n, mode, count_step, count_ns, counts);
     return cudaGetLastError();
 }
 
@@ -737,8 +742,9 @@ cudaError_t launch_begin_run(RunState *rs, uint32_t seed, uint32_t first, uint32
 
 template <int BPS, int S>
 __global__ void counts_kernel(const uint32_t *__restrict__ lat, Geometry g, uint32_t ns,
-                              unsigned long long *__restrict__ counts)
+                              unsigned long long *__restrict__ counts, const uint32_t *__restrict__ pb)
 {
+    constexpr int W = SiteWords<BPS, S>::W;
     extern __shared__ unsigned int hist[];
     const bool use_shared = ns + 1 <= 8192;
     if (use_shared)
@@ -746,7 +752,7 @@ __global__ void counts_kernel(const uint32_t *__restrict__ lat, Geometry g, uint
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.N; i += gridDim.x * blockDim.x) {
         SiteWords<BPS, S> s;
-        s.load(lat, g.N, i);
+        s.load_planes(lat, g.N, i, planes_at<W>(pb, i));
         if (s.empty()) continue;
 #pragma unroll
         for (int k = 0; k < S; k++) {
@@ -1018,14 +1024,14 @@ cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sit
 }
 
 cudaError_t launch_counts(int bps, int slots, const uint32_t *lat, const Geometry &g, uint32_t ns,
-                          unsigned long long *counts, cudaStream_t stream)
+                          unsigned long long *counts, cudaStream_t stream, const uint32_t *pb)
 {
     const uint32_t threads = 256;
     uint32_t blocks = (g.N + threads - 1) / threads;
     if (blocks > 148 * 8) blocks = 148 * 8;
     const size_t smem = ns + 1 <= 8192 ? (ns + 1) * sizeof(unsigned int) : 0;
     count_launch();
-    LMB_DISPATCH_ALL(counts_kernel<BPS, S><<<blocks, threads, smem, stream>>>(lat, g, ns, counts))
+    LMB_DISPATCH_ALL(counts_kernel<BPS, S><<<blocks, threads, smem, stream>>>(lat, g, ns, counts, pb))
 }
 
 cudaError_t launch_validate(int bps, int slots, const uint32_t *lat, const uint8_t *sites, const Geometry &g,

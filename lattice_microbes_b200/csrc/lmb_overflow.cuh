@@ -104,11 +104,13 @@ __host__ __device__ __forceinline__ uint32_t pow2_at_least(uint32_t n)
 // Resolves the step's overflow queue with the whole block (thread `tid` of
 // `nthreads`); `sh` holds pow2_at_least(cap) entries.  On success the step
 // counter advances.  pb: the lattice's plane bounds, raised for every slot
-// filled here (null when it keeps none).
+// filled here (null when it keeps none).  counts (when not null): species
+// counts of the lattice being taken, to which every particle put back is
+// added.
 template <int BPS, int S>
 __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Geometry &g, RunState *rs,
                                    OverflowEntry *list, uint32_t cap, OverflowEntry *sh, uint32_t tid,
-                                   uint32_t nthreads, uint32_t *pb)
+                                   uint32_t nthreads, uint32_t *pb, unsigned long long *counts = nullptr)
 {
     const uint32_t n = *(volatile uint32_t *)&rs->ovf_count;
     const uint32_t carried = rs->carried;
@@ -165,6 +167,7 @@ __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Ge
                 rs->failed_step = rs->step;
                 return;
             }
+            if (counts) atomicAdd(counts + sh[e].particle, 1ull);
         }
         rs->ovf_count = 0;
         rs->carried = 0;
@@ -177,6 +180,8 @@ __device__ void resolve_block_flat(uint32_t *lat, const uint8_t *sites, const Ge
                 OverflowEntry o = sh[e];
                 o.key = (unsigned long long)kept;  // phase 0, list order
                 list[kept++] = o;
+            } else if (counts) {
+                atomicAdd(counts + sh[e].particle, 1ull);
             }
         }
         rs->ovf_count = kept;

@@ -232,6 +232,7 @@ class MpdRdmeSolver:
         self.maxParticleCounts = None  # per species id (index 0 unused)
         self.maxSiteCounts = None      # per site type (type 0 not counted)
         self.lastRunStats = None
+        self._run_counts = None       # species totals the last run took (None: take them anew)
         self.output = None            # lmfile.LMFileWriter the trajectory goes to
         self._write_inputs = False
         self.checkpointInterval = 0.0  # seconds between checkpoints of the output file (0: none)
@@ -375,9 +376,17 @@ class MpdRdmeSolver:
 
     def _upload(self, with_sites):
         self.lat.set_native(self.lattice.particles, self.lattice.sites if with_sites else None)
+        self._run_counts = None
+
+    def _species_counts(self):
+        """The lattice's species totals: those the last run took, unless the
+        lattice was changed since."""
+        if self._run_counts is not None:
+            return self._run_counts.copy()
+        return self.lat.species_counts(self._ns)
 
     def _record_counts(self, time):
-        c = self.lat.species_counts(self._ns)
+        c = self._species_counts()
         self.writeSpeciesCounts(time, np.asarray(c[1:], dtype=np.uint64))
         if self.output is not None:
             self.output.append_species_counts(self.replicate, [time],
@@ -387,7 +396,7 @@ class MpdRdmeSolver:
     def _write_lattice(self, time):
         # writeLatticeData (MpdRdmeSolver.cu:854-883): the particle maxima,
         # then the frame.
-        c = np.asarray(self.lat.species_counts(self._ns), dtype=np.uint32)
+        c = np.asarray(self._species_counts(), dtype=np.uint32)
         c[0] = 0
         np.maximum(self._max_particles, c, out=self._max_particles)
         if self.output is not None:
@@ -433,6 +442,7 @@ class MpdRdmeSolver:
         hook_interval = int(float(p["hookInterval"])) if p.get("hookInterval", "") != "" else None
         max_time = float(p.get("maxTime", "0") or 0)
         self._stop = False
+        self._run_counts = None
         self._download()
         self.onBeginTrajectory(self.lattice)
         self._upload(True)
@@ -451,7 +461,13 @@ class MpdRdmeSolver:
         for step, hook, lat, cnt in trajectory_events(total, counts_interval, lattice_interval, hook_interval):
             if self._stop:
                 break
-            _, self.lastRunStats = self.lat.run(self.model, self.seed, done, step - done, self.overflow_mode)
+            if (cnt or lat) and not hook:
+                # The totals a record needs, taken in the run's own work.
+                _, self.lastRunStats, self._run_counts = self.lat.run_counts(
+                    self.model, self.seed, done, step - done, self._ns, self.overflow_mode)
+            else:
+                _, self.lastRunStats = self.lat.run(self.model, self.seed, done, step - done, self.overflow_mode)
+                self._run_counts = None
             done = step
             t = step * self.tau
             if hook:

@@ -212,6 +212,20 @@ class Lattice:
             L.check(rc, "lmb_run")
         return rc, st
 
+    def run_counts(self, model, seed, first_timestep, timesteps, number_species,
+                   overflow_mode=L.LMB_OVERFLOW_CLASSIC, check=True):
+        """lmb_run with the species totals at the end of the run taken in the
+        run's own work (lmb_run_counts_async / lmb_run_counts_wait); returns
+        (status, stats, counts[0..number_species])."""
+        L.check(L.lib().lmb_run_counts_async(self.handle, model.handle, seed, first_timestep, timesteps,
+                                             overflow_mode, number_species), "lmb_run_counts_async")
+        st = L.RunStats()
+        c = np.zeros(number_species + 1, dtype=np.uint64)
+        rc = L.lib().lmb_run_counts_wait(self.handle, C.byref(st), _p(c, L.u64p))
+        if check:
+            L.check(rc, "lmb_run_counts_wait")
+        return rc, st, c
+
     def run_profiled(self, model, seed, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
         """Runs with CUDA events around every kernel; returns (stats, phase
         milliseconds [x, y, z, reaction, overflow, fused], launches per phase)."""

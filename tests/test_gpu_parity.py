@@ -451,3 +451,39 @@ def test_plane_bounds_across_runs_and_edits(ctx, slots, bps):
     assert rc == rc_ref == 0
     assert out.any()
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
+@pytest.mark.parametrize("case", ["sparse", "storm", "relaxed", "zero_steps"])
+def test_run_counts_equal_separate_counts(ctx, schedule, case):
+    """lmb_run_counts_async takes the species totals inside the run (the fused
+    kernel's last launch and its overflow resolution, or one bounded pass
+    after a per-phase run): they equal lmb_lattice_species_counts of the final
+    lattice and the oracle's, overflow storms and the relaxed handler's
+    unresolved particles (left out of the lattice) included."""
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import Lattice, Model
+    if case == "sparse":
+        spec = configs.random_problem(51, X=64, Y=16, Z=16, slots=8, bytes_per_slot=1, density=0.3, nst=3)
+    else:
+        spec = configs.random_problem(52, X=32, Y=8, Z=8, slots=8, bytes_per_slot=1, density=5.0, nst=2)
+    mode = L.LMB_OVERFLOW_RELAXED if case == "relaxed" else L.LMB_OVERFLOW_CLASSIC
+    n = 0 if case == "zero_steps" else 9
+    t = oracle_tables(spec)
+    model = Model.from_tables(ctx, t)
+    lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
+    if schedule == "phases":
+        lat.set_schedule(L.LMB_SCHEDULE_PHASES)
+    else:
+        lat.set_schedule(L.LMB_SCHEDULE_FUSED)
+    lat.set_native(spec.lattice, spec.sites)
+    rc, st, counts = lat.run_counts(model, 17, 0, n, spec.ns, mode, check=False)
+    ref, rc_ref, _ = oracle_run(t, spec.lattice, spec.sites, 17, 0, n, mode)
+    assert rc == rc_ref
+    if rc == 0:
+        out, _ = lat.get_native()
+        assert np.array_equal(out, ref)
+        assert np.array_equal(counts, lat.species_counts(spec.ns))
+        assert np.array_equal(counts, oracle_counts(t, ref))
+    lat.close()
+    model.close()
