@@ -487,7 +487,7 @@ def run_ours(a):
         alg_bytes = N * B_STEP                 # site-steps per launch x per-site-step bytes
         own_bytes = N * B_SWEEP                # its own dataflow: read slots + site type, write slots
     else:
-        kern = "sweep_int_kernel / sweep_kernel (x, y, z hop sweeps)"
+        kern = "sweep_pp_kernel (x, y, z hop sweeps by particle)"
         sweep_share = float(phase_ms[:3].sum()) / total_ms
         launch_ms = step_ms * sweep_share / max(1, int(phase_n[:3].sum()))
         alg_bytes = N * B_SWEEP

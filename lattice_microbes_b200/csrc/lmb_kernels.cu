@@ -377,10 +377,10 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
 constexpr int SWEEP_PB_TILE = 16;
 constexpr int SWEEP_PB_YZ_THREADS = 32 * (SWEEP_PB_TILE + 2);
 
-// The rule of sweep_kernel's IntLattice path for lattices that keep plane
-// bounds and whose x rows fit one block (X a multiple of 32, at most 256:
-// every warp holds the 32 sites of one segment of one x row, and an x tile is
-// whole rows).  Work goes by particle, not by site: the warp's particles are
+// The sweep rule by particle, for lattices that keep plane bounds and whose
+// x rows fit one block (X a multiple of 32, at most 256: every warp holds
+// the 32 sites of one segment of one x row, and an x tile is whole rows);
+// IntLattices and ByteLattices of up to 16 slots.  The warp's particles are
 // spread over its lanes (particle q of the warp, in site then slot order, on
 // lane q % 32) once to draw their choices and once more, after the block has
 // every choice, to place them.  A particle's place in its new site follows
@@ -389,32 +389,38 @@ constexpr int SWEEP_PB_YZ_THREADS = 32 * (SWEEP_PB_TILE + 2);
 // stayer and that neighbour's PLUS movers of lower slots; one arriving from
 // the plus neighbour after those and the minus neighbour's PLUS movers and
 // its own site's MINUS movers of lower slots (byte_diffusion_1d_dev.cu:
-// 199-269 builds the same order site by site).  Each particle is written
-// straight to the destination by the block that owns its new site (halo
-// rows place what moves into the tile); places past the last slot overflow
-// with the same sequence numbers.  Then each site clears its planes from its
-// new count up to the larger of the warp's new bound and the destination's
-// old one, and the warp stores its new bound.
-template <int S, int DIM, int NT>
+// 199-269 builds the same order site by site).  Each particle is placed by
+// the block that owns its new site (halo rows place what moves into the
+// tile): an IntLattice particle straight into the destination word, a
+// ByteLattice particle into its byte of the site's words assembled in shared
+// memory and stored whole after a barrier.  Places past the last slot
+// overflow with the same sequence numbers.  Each site clears its words from
+// its new content up to the larger of the warp's new bound and the
+// destination's old one, and the warp stores its new bound.
+template <int BPS, int S, int DIM, int NT>
 __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
-    sweep_int_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, const uint8_t *__restrict__ sites,
-                     Geometry g, DevTables m, RunState *__restrict__ rs, OverflowEntry *__restrict__ list,
-                     uint32_t cap, uint32_t *__restrict__ rx_sites, uint32_t rx_cap,
-                     const uint32_t *__restrict__ pb_src, uint32_t *__restrict__ pb_dst)
+    sweep_pp_kernel(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, const uint8_t *__restrict__ sites,
+                    Geometry g, DevTables m, RunState *__restrict__ rs, OverflowEntry *__restrict__ list,
+                    uint32_t cap, uint32_t *__restrict__ rx_sites, uint32_t rx_cap,
+                    const uint32_t *__restrict__ pb_src, uint32_t *__restrict__ pb_dst)
 {
+    static_assert(S <= 16, "slot masks and list entries hold 16 slots");
+    constexpr int W = SiteWords<BPS, S>::W;
     constexpr int CB = CountBits<S>::value;
     constexpr uint32_t LOW = (1u << S) - 1u;
     constexpr uint32_t OUT = 1u << 16;  // occupancy word flag: the block writes this site
-    // Dynamic shared memory (sweep_int_smem bytes):
-    //   sw[S][NT]  particles of the tile's sites, planes below the bound
+    // Dynamic shared memory (sweep_pp_smem bytes):
+    //   sw[W][NT]  words of the tile's sites, planes below the bound
     //   sc[NT]     choices: bit k MINUS, bit S + k PLUS for slot k
     //   so[NT]     occupied slots, | OUT for written sites
     //   pl[NT * S] each warp's particles in site, then slot order: lane << 4 | slot
-    extern __shared__ uint32_t smem_int[];
-    uint32_t(*sw)[NT] = reinterpret_cast<uint32_t(*)[NT]>(smem_int);
-    uint32_t *sc = smem_int + S * NT;
+    //   ow[W][NT]  (ByteLattices) the written sites' new words
+    extern __shared__ uint32_t smem_pp[];
+    uint32_t(*sw)[NT] = reinterpret_cast<uint32_t(*)[NT]>(smem_pp);
+    uint32_t *sc = smem_pp + W * NT;
     uint32_t *so = sc + NT;
     uint16_t *pl = reinterpret_cast<uint16_t *>(so + NT);
+    uint32_t(*ow)[NT] = reinterpret_cast<uint32_t(*)[NT]>(pl + NT * S);
     if (rs->status != LMB_OK) return;
     const bool listing = DIM == 2 && rx_sites && rs->rx_skip == 0;
     uint32_t x, y, z;
@@ -426,28 +432,43 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     int lm = -1, lp = -1;
     uint32_t t = 0, tm = 0, tp = 0, occ = 0;
     const unsigned long long th = rs->th[DIM];
+    // Occupied slots of word k of a site.
+    auto word_slots = [](uint32_t v, uint32_t k) -> uint32_t {
+        if (BPS == 4) return (v != 0u ? 1u : 0u) << k;
+        const uint32_t hi = (v | ((v & 0x7F7F7F7Fu) + 0x7F7F7F7Fu)) & 0x80808080u;
+        return ((((hi >> 7) * 0x10204080u) >> 28) & 0xFu) << (4 * k);
+    };
     if (in) {
         sweep_neighbours<DIM>(g, x, y, z, lid, i, im, ip, lm, lp);
         // Planes 0 and 1 are read with the bound rather than after it (a
         // plane at or above the bound reads as zero, so the early read is
         // harmless): nearly every segment needs plane 0 and most plane 1,
         // and the bound's round trip no longer comes first.
-        const uint32_t npl = planes_at<S>(pb_src, i);
-        const uint32_t v0 = __ldg(src + i), v1 = __ldg(src + (size_t)g.N + i);
+        constexpr uint32_t EARLY = W < 2 ? W : 2;
+        const uint32_t npl = planes_at<W>(pb_src, i);
+        uint32_t v[EARLY];
+#pragma unroll
+        for (uint32_t k = 0; k < EARLY; k++) v[k] = __ldg(src + (size_t)k * g.N + i);
         t = __ldg(sites + i);
         tm = __ldg(sites + im);
         tp = __ldg(sites + ip);
-        sw[0][lid] = v0;
-        sw[1][lid] = v1;
-        occ = (v0 != 0u ? 1u : 0u) | (v1 != 0u ? 2u : 0u);
-        for (uint32_t k = 2; k < npl; k++) {
-            const uint32_t v = __ldg(src + (size_t)k * g.N + i);
-            sw[k][lid] = v;
-            occ |= (v != 0u ? 1u : 0u) << k;
+#pragma unroll
+        for (uint32_t k = 0; k < EARLY; k++) {
+            sw[k][lid] = v[k];
+            occ |= word_slots(v[k], k);
+        }
+        for (uint32_t k = EARLY; k < npl; k++) {
+            const uint32_t vk = __ldg(src + (size_t)k * g.N + i);
+            sw[k][lid] = vk;
+            occ |= word_slots(vk, k);
         }
     }
     so[lid] = occ | (out ? OUT : 0u);
     sc[lid] = 0;
+    if (BPS == 1) {
+#pragma unroll
+        for (int k = 0; k < W; k++) ow[k][lid] = 0u;
+    }
     __syncwarp();
     // The warp's particles: prefix counts over the lanes' sites.
     const uint32_t wbase = (uint32_t)lid & ~31u;
@@ -455,8 +476,8 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     uint32_t incl = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (uint32_t)o) incl += v;
+        const uint32_t vv = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += vv;
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31), excl = incl - cnt;
     uint16_t *wpl = pl + wbase * S;
@@ -472,6 +493,11 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
         o = e >> 4;
         k = e & 15u;
     };
+    // The particle in slot k of tile site sl.
+    auto slot_value = [&](uint32_t sl, uint32_t k) -> uint32_t {
+        if (BPS == 4) return sw[k][sl];
+        return (sw[k >> 2][sl] >> (8u * (k & 3u))) & 0xFFu;
+    };
     for (uint32_t base = 0; base < total; base += 32) {
         const uint32_t q = base + lane;
         uint32_t o, k;
@@ -480,7 +506,7 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
         const uint32_t tp_o = __shfl_sync(0xffffffffu, tp, o), gi_o = __shfl_sync(0xffffffffu, i, o);
         if (q < total) {
             const uint32_t sl = wbase + o;
-            const uint32_t p = sw[k][sl];
+            const uint32_t p = slot_value(sl, k);
             const float rv = hash_float(((unsigned long long)gi_o << CB) | k, th);
             // PLUS when 0.5 <= r < q(t -> tp) + 0.5, else MINUS when r <
             // q(t -> tm).  Every q is at most 0.5 (larger ones are refused
@@ -542,25 +568,32 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
                     gd = gi_o;
                     pos = __popc(stays(sl) & below);
                 }
-                const uint32_t p = sw[k][sl];
-                if (pos < (uint32_t)S) dst[(size_t)pos * g.N + gd] = p;
-                else push_overflow(rs, list, cap, (uint32_t)DIM + 1, gd, pos - (uint32_t)S, p);
+                const uint32_t p = slot_value(sl, k);
+                if (pos >= (uint32_t)S) push_overflow(rs, list, cap, (uint32_t)DIM + 1, gd, pos - (uint32_t)S, p);
+                else if (BPS == 4) dst[(size_t)pos * g.N + gd] = p;
+                else reinterpret_cast<uint8_t *>(&ow[pos >> 2][d])[pos & 3u] = (uint8_t)p;
             }
         }
     }
+    if (BPS == 1) __syncthreads();  // every byte of the written sites placed
     if (!out) return;
     // The site's new count: its stayers and both neighbours' arrivals.
     const uint32_t n = __popc(stays((uint32_t)lid)) + __popc((sc[tile_minus((uint32_t)lid, x)] >> S) & LOW) +
                        __popc(sc[tile_plus((uint32_t)lid, x)] & LOW);
-    const uint32_t nw = n < (uint32_t)S ? n : (uint32_t)S;
+    const uint32_t held = n < (uint32_t)S ? n : (uint32_t)S;  // particles the site holds
+    const uint32_t nw = BPS == 4 ? held : (held + 3u) >> 2;    // words they fill
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, nw);
     const uint32_t seg = i >> PB_SHIFT;
     const uint32_t old = pb_dst[seg];
-    const uint32_t lim = wmax > old ? wmax : (old < (uint32_t)S ? old : (uint32_t)S);
-    for (uint32_t k = nw; k < lim; k++) dst[(size_t)k * g.N + i] = 0u;
+    const uint32_t lim = wmax > old ? wmax : (old < (uint32_t)W ? old : (uint32_t)W);
+    if (BPS == 4) {
+        for (uint32_t k = nw; k < lim; k++) dst[(size_t)k * g.N + i] = 0u;
+    } else {
+        for (uint32_t k = 0; k < lim; k++) dst[(size_t)k * g.N + i] = k < nw ? ow[k][lid] : 0u;
+    }
     __syncwarp();
     if (lane == 0) pb_dst[seg] = wmax;
-    if (listing) list_for_reaction(nw, t, i, lid, m, rs, rx_sites, rx_cap);
+    if (listing) list_for_reaction(held, t, i, lid, m, rs, rx_sites, rx_cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -897,8 +930,12 @@ bool slots_supported(int bps, int slots)
     return false;
 }
 
-// Dynamic shared memory of sweep_int_kernel<S, *, NT>.
-static size_t sweep_int_smem(int S, int NT) { return (size_t)NT * ((size_t)S * 4 + 8 + (size_t)S * 2); }
+// Dynamic shared memory of sweep_pp_kernel<BPS, S, *, NT>.
+static size_t sweep_pp_smem(int BPS, int S, int NT)
+{
+    const size_t W = BPS == 1 ? (size_t)S / 4 : (size_t)S;
+    return (size_t)NT * (W * 4 + 8 + (size_t)S * 2 + (BPS == 1 ? W * 4 : 0));
+}
 
 // Raises kernel K's dynamic shared-memory limit once per device to the
 // largest size asked for so far (setting it on every launch costs host time).
@@ -929,9 +966,9 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
     // Plane bounds need each warp on one whole segment of 32 sites.
     if (g.X % 32u != 0) pb_src = pb_dst = nullptr;
     if (!pb_src || !pb_dst) pb_src = pb_dst = nullptr;
-    if (bps == 4 && pb_src && g.X <= (uint32_t)SWEEP_THREADS) {
-        // IntLattices with plane bounds: y and z tiles of SWEEP_PB_TILE sites
-        // along the axis, one segment across.
+    if (pb_src && g.X <= (uint32_t)SWEEP_THREADS && slots <= 16 && (bps == 4 || slots >= 4)) {
+        // Plane-bounded lattices whose rows fit a block: by particle, y and z
+        // tiles of SWEEP_PB_TILE sites along the axis, one segment across.
         if (dim != 0) {
             const uint32_t A = dim == 1 ? g.Y : g.Z;
             const uint32_t L = A < (uint32_t)SWEEP_PB_TILE ? A : (uint32_t)SWEEP_PB_TILE;
@@ -946,31 +983,33 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
         count_launch();
         constexpr int YZ = SWEEP_PB_YZ_THREADS;
         cudaError_t e;
-#define LMB_INT_SWEEP(S_)                                                                                        \
-    if (slots == S_) {                                                                                          \
-        if (dim == 0) {                                                                                         \
-            const size_t sm = sweep_int_smem(S_, SWEEP_THREADS);                                                \
-            if ((e = raise_smem_limit<sweep_int_kernel<S_, 0, SWEEP_THREADS>>(sm)) != cudaSuccess) return e;     \
-            sweep_int_kernel<S_, 0, SWEEP_THREADS><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, \
-                                                                                cap, nullptr, 0, pb_src,         \
-                                                                                pb_dst);                         \
-        } else if (dim == 1) {                                                                                  \
-            const size_t sm = sweep_int_smem(S_, YZ);                                                           \
-            if ((e = raise_smem_limit<sweep_int_kernel<S_, 1, YZ>>(sm)) != cudaSuccess) return e;               \
-            sweep_int_kernel<S_, 1, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,      \
-                                                                     nullptr, 0, pb_src, pb_dst);               \
-        } else {                                                                                                \
-            const size_t sm = sweep_int_smem(S_, YZ);                                                           \
-            if ((e = raise_smem_limit<sweep_int_kernel<S_, 2, YZ>>(sm)) != cudaSuccess) return e;               \
-            sweep_int_kernel<S_, 2, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,      \
-                                                                     rx_sites, rx_cap, pb_src, pb_dst);         \
-        }                                                                                                       \
-        return cudaGetLastError();                                                                              \
+#define LMB_PP_SWEEP(BPS_, S_)                                                                                     \
+    if (bps == BPS_ && slots == S_) {                                                                             \
+        if (dim == 0) {                                                                                           \
+            const size_t sm = sweep_pp_smem(BPS_, S_, SWEEP_THREADS);                                             \
+            if ((e = raise_smem_limit<sweep_pp_kernel<BPS_, S_, 0, SWEEP_THREADS>>(sm)) != cudaSuccess) return e;  \
+            sweep_pp_kernel<BPS_, S_, 0, SWEEP_THREADS><<<grid, block, sm, stream>>>(                               \
+                src, dst, sites, g, m, rs, list, cap, nullptr, 0, pb_src, pb_dst);                                \
+        } else if (dim == 1) {                                                                                    \
+            const size_t sm = sweep_pp_smem(BPS_, S_, YZ);                                                        \
+            if ((e = raise_smem_limit<sweep_pp_kernel<BPS_, S_, 1, YZ>>(sm)) != cudaSuccess) return e;            \
+            sweep_pp_kernel<BPS_, S_, 1, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,   \
+                                                                          nullptr, 0, pb_src, pb_dst);            \
+        } else {                                                                                                  \
+            const size_t sm = sweep_pp_smem(BPS_, S_, YZ);                                                        \
+            if ((e = raise_smem_limit<sweep_pp_kernel<BPS_, S_, 2, YZ>>(sm)) != cudaSuccess) return e;            \
+            sweep_pp_kernel<BPS_, S_, 2, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,   \
+                                                                          rx_sites, rx_cap, pb_src, pb_dst);      \
+        }                                                                                                         \
+        return cudaGetLastError();                                                                                \
     }
-        LMB_INT_SWEEP(4)
-        LMB_INT_SWEEP(8)
-        LMB_INT_SWEEP(16)
-#undef LMB_INT_SWEEP
+        LMB_PP_SWEEP(4, 4)
+        LMB_PP_SWEEP(4, 8)
+        LMB_PP_SWEEP(4, 16)
+        LMB_PP_SWEEP(1, 4)
+        LMB_PP_SWEEP(1, 8)
+        LMB_PP_SWEEP(1, 16)
+#undef LMB_PP_SWEEP
         return cudaErrorInvalidValue;
     }
     count_launch();

@@ -112,6 +112,26 @@ def test_sweep_tiles_vs_oracle(ctx, shape, slots, bps):
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("slots,bps", VARIANTS)
+@pytest.mark.parametrize("shape,per_slot", [((32, 20, 7), 0.3), ((64, 16, 33), 0.05), ((256, 3, 18), 0.12),
+                                             ((96, 1, 1), 0.2), ((32, 17, 16), 0.25)])
+def test_particle_sweep_vs_oracle(ctx, shape, per_slot, slots, bps):
+    """Per-phase runs on lattices whose x rows are whole segments of 32 sites
+    and fit one block, which sweep by particle with plane bounds (IntLattices
+    and ByteLattices of up to 16 slots; ByteLattice-32 keeps the sweep by
+    site): y and z tiles cut off by the end of the axis, axes of one site,
+    sparse sites whose bounds stay low and full sites that overflow (up to
+    2,962 overflows in six timesteps)."""
+    X, Y, Z = shape
+    spec = configs.random_problem(61, X=X, Y=Y, Z=Z, slots=slots, bytes_per_slot=bps, density=per_slot * slots,
+                                  nst=3)
+    t = oracle_tables(spec)
+    ref, rc_ref, _ = oracle_run(t, spec.lattice, spec.sites, 17, 2, 6)
+    out, rc, _ = _gpu_run(ctx, t, spec.lattice, spec.sites, 17, 2, 6, schedule="phases")
+    assert rc == rc_ref
+    assert np.array_equal(out, ref)
+
+
 @pytest.mark.parametrize("slots,bps", [(8, 1), (16, 4)])
 @pytest.mark.parametrize("shape,per_slot", [((64, 32, 32), 0.03), ((64, 32, 32), 0.15), ((64, 64, 32), 0.3)])
 def test_reaction_site_list_vs_oracle(ctx, shape, per_slot, slots, bps):
