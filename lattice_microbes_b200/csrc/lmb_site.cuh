@@ -318,15 +318,17 @@ __device__ __forceinline__ SiteWords<BPS, S> sweep_site(const SiteWords<BPS, S> 
 
 // Per-reaction propensity from FP32 counts (byte_reaction_dev.cu:62-102,
 // MPD_GLOBAL_R_MATRIX branch: the self reaction is rate*n*(n-1)).
+// hi: slots at and above it are empty (an unrolled loop stops there).
 template <int BPS, int S>
 __device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_t t, const SiteWords<BPS, S> &s,
-                                                     uint32_t rx)
+                                                     uint32_t rx, int hi)
 {
     if (!tload(m.RL + (size_t)rx * m.nst + t)) return 0.0f;
     const uint32_t d1 = tload(m.D1 + rx), d2 = tload(m.D2 + rx);
     float n1 = 0.0f, n2 = 0.0f;
 #pragma unroll
     for (int k = 0; k < S; k++) {
+        if (k >= hi) break;
         const uint32_t p = s.slot(k);
         if (p > 0) {
             n1 = __fadd_rn(n1, p == d1 ? 1.0f : 0.0f);
@@ -379,15 +381,22 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
     // The table sums and the double exp are evaluated only for draws below
     // the bound of reaction_may_fire.
     const float r0 = hash_float(((unsigned long long)gi << 1) | 0ull, th);
-    if (!reaction_may_fire((uint32_t)__popc(occupied_slots<BPS, S>(s)), a, t, r0, m)) return false;
+    const uint32_t occ = occupied_slots<BPS, S>(s);
+    if (!reaction_may_fire((uint32_t)__popc(occ), a, t, r0, m)) return false;
+    // Every slot loop below stops at the highest occupied slot: the slots
+    // above it add nothing (sites are packed after a sweep, so this is the
+    // particle count, which keeps the unrolled loops short).
+    const int hi = 32 - __clz((int)occ);
     const size_t o1 = (size_t)t * m.ns, o2 = (size_t)t * m.ns * m.ns;
 #pragma unroll
     for (int k = 0; k < S; k++) {
+        if (k >= hi) break;
         const uint32_t p1 = s.slot(k);
         if (p1 > 0) {
             a = __fadd_rn(a, tload(m.qp1 + o1 + (p1 - 1)));
 #pragma unroll
             for (int j = k + 1; j < S; j++) {
+                if (j >= hi) break;
                 const uint32_t p2 = s.slot(j);
                 if (p2 > 0) a = __fadd_rn(a, tload(m.qp2 + o2 + (size_t)(p1 - 1) * m.ns + (p2 - 1)));
             }
@@ -414,7 +423,7 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
     // its reactions once), and visited in index order; when there are more
     // than the list holds, every reaction is visited instead.
     auto visit = [&](uint32_t rx) {
-        const float prop = reaction_propensity<BPS, S>(m, t, s, rx);
+        const float prop = reaction_propensity<BPS, S>(m, t, s, rx, hi);
         if (prop > 0.0f) {
             if (rp > 0.0f) idx = rx;
             rp = __fsub_rn(rp, prop);
@@ -460,6 +469,7 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
         for (uint32_t e = z0; e < z1 && !all; e++) insert(tload(m.rx_list + e));
 #pragma unroll
         for (int k = 0; k < S; k++) {
+            if (k >= hi) break;
             const uint32_t p = s.slot(k);
             if (p > 0 && p <= m.ns && !all) {
                 const uint32_t e0 = tload(m.rx_off + p), e1 = tload(m.rx_off + p + 1);
@@ -523,6 +533,7 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
     if (negatives <= 2) {
 #pragma unroll
         for (int k = 0; k < S; k++) {
+            if (k >= hi) break;
             const uint32_t q = s.slot(k);
             if (q > 0) {
                 if (q - 1 == c_sp0 && c_n0 > 0) c_n0--;
@@ -537,6 +548,7 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
         uint32_t taken_bits = 0;  // bit k: slot k consumed
 #pragma unroll
         for (int k = 0; k < S; k++) {
+            if (k >= hi) break;
             const uint32_t q = s.slot(k);
             if (q > 0) {
                 int need = 0;
