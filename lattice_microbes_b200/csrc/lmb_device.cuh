@@ -12,6 +12,19 @@
 
 namespace lmb {
 
+// Programmatic dependent launch between the kernels of a timestep.  Every
+// kernel of the chain starts with chain_enter(): it waits until the kernel
+// before it in the stream has finished and its writes are visible (at once
+// when that kernel was not launched as part of a chain), then lets the next
+// kernel of the chain be launched, so that its blocks are scheduled while
+// this kernel's last blocks run instead of after them.  Nothing is read or
+// written before the wait.
+__device__ __forceinline__ void chain_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Model-table read.  The tables live in global memory, or in shared memory
 // when a kernel stages them there, so the load is a generic one.
 template <typename T>

@@ -583,6 +583,7 @@ __global__ void __launch_bounds__(FUSED_THREADS, MINB) fused_step_kernel(const u
                                                                    const __grid_constant__ TileShape ts,
                                                                    int with_reaction)
 {
+    chain_enter();
     fused_tile<BPS, S, true>(src, dst, sites, g, m, rs, list, cap, ts, with_reaction, blockIdx.x, gridDim.x);
 }
 
@@ -597,6 +598,7 @@ template <int BPS, int S>
 __global__ void __launch_bounds__(FUSED_THREADS, 2) fused_batch_kernel(const FusedJob *__restrict__ jobs,
                                                                     uint32_t njobs, uint32_t parity)
 {
+    chain_enter();
     uint32_t lo = 0, hi = njobs;
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) / 2;
@@ -737,9 +739,8 @@ static cudaError_t fused_launch(dim3 grid, dim3 block, size_t smem, cudaStream_t
 {
     cudaError_t e = ensure_smem_limit<BPS, S, MINB>(smem);
     if (e != cudaSuccess) return e;
-    fused_step_kernel<BPS, S, MINB><<<grid, block, smem, stream>>>(src, dst, sites, g, m, rs, list, cap, ts,
-                                                                   with_reaction);
-    return cudaGetLastError();
+    return launch_chain(fused_step_kernel<BPS, S, MINB>, grid, block, smem, stream, src, dst, sites, g, m, rs, list,
+                        cap, ts, with_reaction);
 }
 
 #define FUSED_DISPATCH(BPS_, S_)                                                                            \
@@ -794,8 +795,8 @@ static cudaError_t ensure_batch_smem_limit(size_t smem)
     if (bps == BPS_ && slots == S_) {                                                                 \
         cudaError_t e = ensure_batch_smem_limit<BPS_, S_>(smem);                                      \
         if (e != cudaSuccess) return e;                                                               \
-        fused_batch_kernel<BPS_, S_><<<total_tiles, FUSED_THREADS, smem, stream>>>(jobs, njobs, parity); \
-        return cudaGetLastError();                                                                    \
+        return launch_chain(fused_batch_kernel<BPS_, S_>, dim3(total_tiles), dim3(FUSED_THREADS), smem, stream, \
+                            jobs, njobs, parity);                                                     \
     }
 
 cudaError_t launch_fused_batch(int bps, int slots, const FusedJob *jobs, uint32_t njobs, uint32_t total_tiles,

@@ -165,6 +165,26 @@ cudaError_t launch_native_to_row_major(int bytes_per_slot, int slots, const uint
 bool slots_supported(int bytes_per_slot, int slots);
 void count_launch(uint64_t n = 1);
 
+// Launches kernel k as a link of the timestep chain (programmatic stream
+// serialization): the kernel must begin with chain_enter(), which waits for
+// the kernel before it, so only the launch itself overlaps that kernel's end.
+template <typename... KArgs, typename... Args>
+static inline cudaError_t launch_chain(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                       Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Read-only view of a lattice for code outside the C ABI file (the .lm
 // writer): its context, geometry, layout and current device buffers.
 struct LatticeView {

@@ -99,15 +99,13 @@ __device__ __forceinline__ void sweep_neighbours(const Geometry &g, uint32_t x, 
 // atomic per group of converged lanes.  An entry is the pair (i, t << 8 |
 // n).  Entries past rx_cap are dropped but counted, which sends the reaction
 // step over every site.
-__device__ __forceinline__ void list_for_reaction(uint32_t n, uint32_t t, uint32_t i, int lid, const DevTables &m,
-                                                  RunState *rs, uint32_t *rx_sites, uint32_t rx_cap)
+// rb: the bound's inputs for type t; th: the reaction sub-step's hash.
+__device__ __forceinline__ void list_for_reaction(uint32_t n, uint32_t t, uint32_t i, int lid, const ReactBound &rb,
+                                                  unsigned long long th, RunState *rs, uint32_t *rx_sites,
+                                                  uint32_t rx_cap)
 {
-    const float a0 = tload(m.qp0 + t);
     bool need = false;
-    if (n != 0 || a0 != 0.0f) {
-        const unsigned long long th = rs->th[3];
-        need = reaction_may_fire(n, a0, t, hash_float((unsigned long long)i << 1, th), m);
-    }
+    if (n != 0 || rb.a0 != 0.0f) need = reaction_may_fire(n, rb, hash_float((unsigned long long)i << 1, th));
     const uint32_t act = __activemask();
     const uint32_t want = __ballot_sync(act, need);
     if (!need) return;
@@ -164,6 +162,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
     constexpr int NT = DIM == 0 ? SWEEP_THREADS : SWEEP_MAX_THREADS;
     __shared__ uint32_t sw[W][NT];
     __shared__ Code sc[NT];
+    chain_enter();
     if (rs->status != LMB_OK) return;
     // The z sweep lists reaction sites unless the list overflowed recently.
     const bool listing = DIM == 2 && rs->rx_skip == 0;
@@ -338,7 +337,8 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
             for (int k = 0; k < S; k++) dst[(size_t)k * g.N + i] = (uint32_t)k < n ? so[k][oid] : 0u;
         }
         if (DIM == 2 && rx_sites && listing)
-            list_for_reaction(n < (uint32_t)S ? n : (uint32_t)S, t, i, lid, m, rs, rx_sites, rx_cap);
+            list_for_reaction(n < (uint32_t)S ? n : (uint32_t)S, t, i, lid, react_bound(t, m), rs->th[3], rs,
+                              rx_sites, rx_cap);
     } else {
         // The neighbours: from the tile, or loaded with their choices drawn here.
         SiteWords<BPS, S> mn, pl;
@@ -364,7 +364,8 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
         const uint32_t n_out = (uint32_t)__popc(occupied_slots<BPS, S>(out));
         if (pb_dst) store_bounded<W>(dst, pb_dst, g.N, i, (n_out + 3u) >> 2, [&](int k) { return out.w[k]; });
         else out.store(dst, g.N, i);
-        if (DIM == 2 && rx_sites && listing) list_for_reaction(n_out, t, i, lid, m, rs, rx_sites, rx_cap);
+        if (DIM == 2 && rx_sites && listing)
+            list_for_reaction(n_out, t, i, lid, react_bound(t, m), rs->th[3], rs, rx_sites, rx_cap);
     }
 }
 
@@ -421,6 +422,7 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     uint32_t *so = sc + NT;
     uint16_t *pl = reinterpret_cast<uint16_t *>(so + NT);
     uint32_t(*ow)[NT] = reinterpret_cast<uint32_t(*)[NT]>(pl + NT * S);
+    chain_enter();
     if (rs->status != LMB_OK) return;
     const bool listing = DIM == 2 && rx_sites && rs->rx_skip == 0;
     uint32_t x, y, z;
@@ -432,6 +434,11 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     int lm = -1, lp = -1;
     uint32_t t = 0, tm = 0, tp = 0, occ = 0;
     const unsigned long long th = rs->th[DIM];
+    // The destination's old plane bound, loaded here rather than where it is
+    // used, so that its round trip to L2 (the previous sweep wrote it from
+    // another SM) is not on the critical path of the warp's tail; no other
+    // warp writes it.
+    uint32_t old_pb = 0;
     // Occupied slots of word k of a site.
     auto word_slots = [](uint32_t v, uint32_t k) -> uint32_t {
         if (BPS == 4) return (v != 0u ? 1u : 0u) << k;
@@ -452,6 +459,7 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
         t = __ldg(sites + i);
         tm = __ldg(sites + im);
         tp = __ldg(sites + ip);
+        if (out) old_pb = pb_dst[i >> PB_SHIFT];
 #pragma unroll
         for (uint32_t k = 0; k < EARLY; k++) {
             sw[k][lid] = v[k];
@@ -584,8 +592,7 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     const uint32_t nw = BPS == 4 ? held : (held + 3u) >> 2;    // words they fill
     const uint32_t wmax = __reduce_max_sync(0xffffffffu, nw);
     const uint32_t seg = i >> PB_SHIFT;
-    const uint32_t old = pb_dst[seg];
-    const uint32_t lim = wmax > old ? wmax : (old < (uint32_t)W ? old : (uint32_t)W);
+    const uint32_t lim = wmax > old_pb ? wmax : (old_pb < (uint32_t)W ? old_pb : (uint32_t)W);
     if (BPS == 4) {
         for (uint32_t k = nw; k < lim; k++) dst[(size_t)k * g.N + i] = 0u;
     } else {
@@ -593,7 +600,7 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     }
     __syncwarp();
     if (lane == 0) pb_dst[seg] = wmax;
-    if (listing) list_for_reaction(held, t, i, lid, m, rs, rx_sites, rx_cap);
+    if (listing) list_for_reaction(held, t, i, lid, react_bound(t, m), rs->th[3], rs, rx_sites, rx_cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -608,6 +615,7 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
                                                        uint32_t *__restrict__ pb)
 {
     constexpr int W = SiteWords<BPS, S>::W;
+    chain_enter();
     if (rs->status != LMB_OK) return;
     // The sites the z sweep listed, or every site when it listed none or
     // more than the list holds.
@@ -658,6 +666,7 @@ __global__ void __launch_bounds__(RESOLVE_THREADS) resolve_kernel(uint32_t *__re
                                                                   uint32_t rx_cap, uint32_t *__restrict__ pb)
 {
     extern __shared__ OverflowEntry sh[];
+    chain_enter();
     if (rs->status != LMB_OK) return;
     // The reaction step of this timestep has read its site list.  A list
     // that overflowed is not built for the next 31 timesteps (the reaction
@@ -988,20 +997,20 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
         if (dim == 0) {                                                                                           \
             const size_t sm = sweep_pp_smem(BPS_, S_, SWEEP_THREADS);                                             \
             if ((e = raise_smem_limit<sweep_pp_kernel<BPS_, S_, 0, SWEEP_THREADS>>(sm)) != cudaSuccess) return e;  \
-            sweep_pp_kernel<BPS_, S_, 0, SWEEP_THREADS><<<grid, block, sm, stream>>>(                               \
-                src, dst, sites, g, m, rs, list, cap, nullptr, 0, pb_src, pb_dst);                                \
+            e = launch_chain(sweep_pp_kernel<BPS_, S_, 0, SWEEP_THREADS>, grid, block, sm, stream, src, dst, sites, \
+                             g, m, rs, list, cap, nullptr, 0u, pb_src, pb_dst);                                   \
         } else if (dim == 1) {                                                                                    \
             const size_t sm = sweep_pp_smem(BPS_, S_, YZ);                                                        \
             if ((e = raise_smem_limit<sweep_pp_kernel<BPS_, S_, 1, YZ>>(sm)) != cudaSuccess) return e;            \
-            sweep_pp_kernel<BPS_, S_, 1, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,   \
-                                                                          nullptr, 0, pb_src, pb_dst);            \
+            e = launch_chain(sweep_pp_kernel<BPS_, S_, 1, YZ>, grid, block, sm, stream, src, dst, sites, g, m, rs, \
+                             list, cap, nullptr, 0u, pb_src, pb_dst);                                             \
         } else {                                                                                                  \
             const size_t sm = sweep_pp_smem(BPS_, S_, YZ);                                                        \
             if ((e = raise_smem_limit<sweep_pp_kernel<BPS_, S_, 2, YZ>>(sm)) != cudaSuccess) return e;            \
-            sweep_pp_kernel<BPS_, S_, 2, YZ><<<grid, block, sm, stream>>>(src, dst, sites, g, m, rs, list, cap,   \
-                                                                          rx_sites, rx_cap, pb_src, pb_dst);      \
+            e = launch_chain(sweep_pp_kernel<BPS_, S_, 2, YZ>, grid, block, sm, stream, src, dst, sites, g, m, rs, \
+                             list, cap, rx_sites, rx_cap, pb_src, pb_dst);                                        \
         }                                                                                                         \
-        return cudaGetLastError();                                                                                \
+        return e;                                                                                                 \
     }
         LMB_PP_SWEEP(4, 4)
         LMB_PP_SWEEP(4, 8)
@@ -1015,14 +1024,14 @@ cudaError_t launch_sweep(int bps, int slots, int dim, const uint32_t *src, uint3
     count_launch();
     LMB_DISPATCH_ALL({
         if (dim == 0)
-            sweep_kernel<BPS, S, 0><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0,
-                                                                pb_src, pb_dst);
+            return launch_chain(sweep_kernel<BPS, S, 0>, grid, block, 0, stream, src, dst, sites, g, m, rs, list, cap,
+                                nullptr, 0u, pb_src, pb_dst);
         else if (dim == 1)
-            sweep_kernel<BPS, S, 1><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, nullptr, 0,
-                                                                pb_src, pb_dst);
+            return launch_chain(sweep_kernel<BPS, S, 1>, grid, block, 0, stream, src, dst, sites, g, m, rs, list, cap,
+                                nullptr, 0u, pb_src, pb_dst);
         else
-            sweep_kernel<BPS, S, 2><<<grid, block, 0, stream>>>(src, dst, sites, g, m, rs, list, cap, rx_sites,
-                                                                rx_cap, pb_src, pb_dst);
+            return launch_chain(sweep_kernel<BPS, S, 2>, grid, block, 0, stream, src, dst, sites, g, m, rs, list, cap,
+                                rx_sites, rx_cap, pb_src, pb_dst);
     })
 }
 
@@ -1038,8 +1047,8 @@ cudaError_t launch_reaction(int bps, int slots, uint32_t *lat, const uint8_t *si
     if (blocks > 148 * 8) blocks = 148 * 8;
     if (g.X % 32u != 0) pb = nullptr;
     count_launch();
-    LMB_DISPATCH_ALL(reaction_kernel<BPS, S><<<blocks, threads, 0, stream>>>(lat, sites, g, m, rs, list, cap,
-                                                                             rx_sites, rx_cap, pb))
+    LMB_DISPATCH_ALL(return launch_chain(reaction_kernel<BPS, S>, dim3(blocks), dim3(threads), 0, stream, lat, sites,
+                                         g, m, rs, list, cap, rx_sites, rx_cap, pb))
 }
 
 cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sites, const Geometry &g, RunState *rs,
@@ -1058,7 +1067,8 @@ cudaError_t launch_resolve(int bps, int slots, uint32_t *lat, const uint8_t *sit
             cudaFuncSetAttribute(resolve_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             raised[dev] = true;
         }
-        resolve_kernel<BPS, S><<<1, RESOLVE_THREADS, smem, stream>>>(lat, sites, g, rs, list, cap, rx_cap, pb);
+        return launch_chain(resolve_kernel<BPS, S>, dim3(1), dim3(RESOLVE_THREADS), smem, stream, lat, sites, g, rs,
+                            list, cap, rx_cap, pb);
     })
 }
 

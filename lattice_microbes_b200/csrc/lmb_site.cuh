@@ -356,15 +356,32 @@ __device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_
 // cannot react.  The z sweep evaluates the same function on the site it has
 // just assembled, so the sites it leaves out are exactly those react_site
 // would leave unchanged.
+// The per-type inputs of the bound: qp0, max qp1 and max qp2 of type t (a
+// kernel may load them ahead of the site's count).
+struct ReactBound {
+    float a0, q1, q2;
+};
+
+__device__ __forceinline__ ReactBound react_bound(uint32_t t, const DevTables &m)
+{
+    return ReactBound{tload(m.qp0 + t), tload(m.qpmax + t), tload(m.qpmax + m.nst + t)};
+}
+
+__device__ __forceinline__ bool reaction_may_fire(uint32_t n, const ReactBound &b, float r0)
+{
+    if (n == 0 && b.a0 == 0.0f) return false;
+    const float nf = (float)n;
+    const float pairs = __fmul_rn(nf, __fmul_rn(__fsub_rn(nf, 1.0f), 0.5f));
+    float u = __fadd_ru(b.a0, __fmul_ru(nf, b.q1));
+    u = __fadd_ru(u, __fmul_ru(pairs, b.q2));
+    u = __fmul_ru(u, 1.0001f);
+    return !(r0 > __fadd_ru(__fmul_ru(u, 1.00000095367431640625f), 8.67361738e-19f));
+}
+
 __device__ __forceinline__ bool reaction_may_fire(uint32_t n, float a0, uint32_t t, float r0, const DevTables &m)
 {
     if (n == 0 && a0 == 0.0f) return false;
-    const float nf = (float)n;
-    const float pairs = __fmul_rn(nf, __fmul_rn(__fsub_rn(nf, 1.0f), 0.5f));
-    float u = __fadd_ru(a0, __fmul_ru(nf, tload(m.qpmax + t)));
-    u = __fadd_ru(u, __fmul_ru(pairs, tload(m.qpmax + m.nst + t)));
-    u = __fmul_ru(u, 1.0001f);
-    return !(r0 > __fadd_ru(__fmul_ru(u, 1.00000095367431640625f), 8.67361738e-19f));
+    return reaction_may_fire(n, ReactBound{a0, tload(m.qpmax + t), tload(m.qpmax + m.nst + t)}, r0);
 }
 
 // Table propensity sum in slot order, double precision probability, at most
@@ -430,12 +447,22 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
         }
     };
     constexpr int LEN = CAP > 0 ? CAP : 64;
+    // CAP == 0, models of up to BMW * 32 reactions: the candidates are the
+    // set bits of a bitmap indexed by reaction, which keeps them sorted and
+    // drops repeats whatever their number (a full site of one species, say).
+    constexpr uint32_t BMW = CAP > 0 ? 1 : 128;
+    const bool bitmap = CAP == 0 && m.nr <= BMW * 32;
+    // Only its first nbw words are used, each cleared below before any bit
+    // is set (the compiler cannot see that the two conditions agree).
+#pragma nv_diag_suppress 549
+    uint32_t bm[BMW];
     uint32_t cand[LEN];
     int nc = 0;
     bool all = false;
     // CAP > 0: insertion by compare-and-swap over fixed positions (unused
     // ones hold ~0u, above every index, so carrying the larger value forward
-    // keeps the list sorted); CAP == 0: appended, sorted below.
+    // keeps the list sorted); CAP == 0 without the bitmap: appended, sorted
+    // below.
     auto insert = [&](uint32_t v) {
         if (CAP > 0) {
             bool dup = false;
@@ -455,6 +482,8 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
                 carry = sw ? c : carry;
             }
             nc++;
+        } else if (bitmap) {
+            bm[v >> 5] |= 1u << (v & 31u);
         } else {
             if (nc < LEN) cand[nc++] = v;
             else all = true;
@@ -464,6 +493,9 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
 #pragma unroll
         for (int j = 0; j < LEN; j++) cand[j] = 0xFFFFFFFFu;
     }
+    const uint32_t nbw = (m.nr + 31u) / 32u;
+    if (bitmap)
+        for (uint32_t w = 0; w < nbw; w++) bm[w] = 0u;
     {
         const uint32_t z0 = tload(m.rx_off), z1 = tload(m.rx_off + 1);
         for (uint32_t e = z0; e < z1 && !all; e++) insert(tload(m.rx_list + e));
@@ -487,6 +519,15 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
             for (int j = 0; j + 1 < LEN; j++) cand[j] = cand[j + 1];
             visit(rx);
         }
+    } else if (bitmap) {
+        for (uint32_t w = 0; w < nbw; w++) {
+            uint32_t bits = bm[w];
+            while (bits) {
+                const uint32_t k = __ffs(bits) - 1;
+                bits &= bits - 1;
+                visit(w * 32u + k);
+            }
+        }
     } else {
         // Insertion sort of the few entries; repeats skipped.
         for (int a = 1; a < nc; a++) {
@@ -503,6 +544,7 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
             visit(cand[q]);
         }
     }
+#pragma nv_diag_default 549
     atomicAdd(&rs->reactions, 1ull);
 
     // evaluateReaction (byte_reaction_dev.cu:179-258) with the chosen

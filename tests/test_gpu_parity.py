@@ -346,13 +346,13 @@ def test_graph_replay_long_run_vs_oracle(ctx, schedule):
     assert np.array_equal(out, ref)
 
 
-def _busy_problem(seed, promiscuous):
+def _busy_problem(seed, promiscuous, ns=60, nr=150):
     """Many species and reactions on a small Int-16 lattice, with fast
     reactions so that sites react every few timesteps: exercises the
-    candidate-reaction scan (and, when `promiscuous`, its full-scan fallback:
-    one species is the first reactant of 80 reactions) and the propensity
-    bound of the reaction step."""
-    spec = configs.config2(seed=seed, X=32, Y=16, Z=16, ns=60, nr=150, nparticles=12000, nst=4,
+    candidate-reaction scan (and, when `promiscuous`, sites with more
+    candidate reactions than a short list holds: one species is the first
+    reactant of 80 reactions) and the propensity bound of the reaction step."""
+    spec = configs.config2(seed=seed, X=32, Y=16, Z=16, ns=ns, nr=nr, nparticles=12000, nst=4,
                            obstacle_fraction=0.1)
     spec.tau = 2e-4  # larger rates per timestep
     if promiscuous:
@@ -380,6 +380,21 @@ def test_many_reactions_vs_oracle(ctx, schedule, promiscuous):
     out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 4242, 0, 12, schedule=schedule)
     assert rc == rc_ref == 0
     assert st_ref.reactions > 50  # the reaction step really fires
+    assert st[0].reactions == st_ref.reactions
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("schedule", SCHEDULES)
+def test_reactions_past_the_candidate_bitmap_vs_oracle(ctx, schedule):
+    """4200 reactions, more than the per-phase reaction step's candidate
+    bitmap covers (4096): its candidates go through the 64-entry list, and
+    the full scan of every reaction when a site has more."""
+    spec = _busy_problem(21, True, ns=120, nr=4200)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 4242, 0, 12)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 4242, 0, 12, schedule=schedule)
+    assert rc == rc_ref == 0
+    assert st_ref.reactions > 50
     assert st[0].reactions == st_ref.reactions
     assert np.array_equal(out, ref)
 
