@@ -623,7 +623,12 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
     const bool all = listed > rx_cap;
     const uint32_t n = all ? g.N : listed;
     const unsigned long long th = rs->th[3];
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    // Listed sites go round the blocks (entry j to block j % gridDim.x), so
+    // that the few thousand entries spread over every SM; a pass over every
+    // site keeps neighbouring sites on neighbouring lanes.
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t j0 = all ? blockIdx.x * blockDim.x + threadIdx.x : threadIdx.x * gridDim.x + blockIdx.x;
+    for (uint32_t j = j0; j < n; j += stride) {
         // The z sweep wrote this buffer, so its sites are packed (occupied
         // slots first, whatever the input had): only the planes holding
         // particles are read.
@@ -1042,9 +1047,10 @@ cudaError_t launch_reaction(int bps, int slots, uint32_t *lat, const uint8_t *si
                             const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
                             const uint32_t *rx_sites, uint32_t rx_cap, uint32_t *pb, cudaStream_t stream)
 {
+    // One wave: four blocks per SM fit every instantiation's registers.
     const uint32_t threads = 256;
     uint32_t blocks = (g.N + threads - 1) / threads;
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks > 148 * 4) blocks = 148 * 4;
     if (g.X % 32u != 0) pb = nullptr;
     count_launch();
     LMB_DISPATCH_ALL(return launch_chain(reaction_kernel<BPS, S>, dim3(blocks), dim3(threads), 0, stream, lat, sites,
