@@ -499,24 +499,39 @@ def run_ours(a):
         sweep_fraction = alg_bytes / (launch_ms / 1e3) / 1e9 / peak
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     # ---- end to end through the public API with host buffers ----
+    # Every step is one solve: its input lattice and site types copied from
+    # pinned host memory, T timesteps, the final lattice copied back into
+    # pinned host memory (lmb_run_native_async).  The solves alternate
+    # between two lattices on two contexts (streams), each step's solve
+    # queued while the one before runs, so that one solve's copies overlap
+    # the other's timesteps; the clock runs from the first call to the last
+    # solve's end (wall clock).
     words = spec.words * N
     h_lat = torch.from_numpy(spec.lattice.copy()).pin_memory()
     h_sites = torch.from_numpy(spec.sites.copy()).pin_memory()
-    h_out = torch.empty(words, dtype=torch.int32).pin_memory()
-    import ctypes as C
-    from lattice_microbes_b200 import _lib as L
-    e2e_ms = []
+    h_out = [torch.empty(words, dtype=torch.int32).pin_memory() for _ in range(2)]
+    ctx2 = Context(device)
+    lat2 = Lattice(ctx2, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+    lat2.set_schedule(*sched)
+    lat2.set_native(spec.lattice, spec.sites)
+    pair = [lat, lat2]
+    for k in range(2):  # graphs captured and buffers touched before the clock starts
+        pair[k].run_native_async(model, seed, 0, T, h_lat.data_ptr(), h_sites.data_ptr(), h_out[k].data_ptr())
+        pair[k].wait()
+    torch.cuda.synchronize(device)
     ranks.barrier()
-    for _ in range(a.steps):
-        torch.cuda.synchronize(device)
-        t0 = time.perf_counter()
-        L.check(L.lib().lmb_lattice_set_native(lat.handle, C.cast(h_lat.data_ptr(), L.u32p),
-                                               C.cast(h_sites.data_ptr(), L.u8p)))
-        lat.run(model, seed, 0, T)
-        L.check(L.lib().lmb_lattice_get_native(lat.handle, C.cast(h_out.data_ptr(), L.u32p), None))
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_total = ranks.max(sum(e2e_ms), device)
+    t0 = time.perf_counter()
+    for k in range(a.steps):
+        if k >= 2:
+            pair[k % 2].wait()
+        pair[k % 2].run_native_async(model, seed, 0, T, h_lat.data_ptr(), h_sites.data_ptr(),
+                                     h_out[k % 2].data_ptr())
+    for k in range(min(2, a.steps)):
+        pair[(a.steps - 1 - k) % 2].wait()
+    e2e_total = ranks.max((time.perf_counter() - t0) * 1e3, device)
     e2e_value = aggregate_rate(N * T * a.steps, e2e_total, world)
+    lat2.close()
+    ctx2.close()
 
     if rank == 0:
         line = {
@@ -573,6 +588,10 @@ def run_ours(a):
                 "unit": METRIC,
                 "h2d_bytes_per_step": int(words * 4 + N),
                 "d2h_bytes_per_step": int(words * 4),
+                "what": "one solve per step through lmb_run_native_async (input lattice and site types from "
+                        "pinned host memory, %d timesteps, final lattice to pinned host memory), solves "
+                        "alternating between two lattices on two streams so that copies overlap timesteps; "
+                        "wall clock" % T,
             },
             "gpu_launches": int(launches),
             "clocks": clock_info,

@@ -218,6 +218,20 @@ int lmb_run(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_
 int lmb_run_async(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
                   uint32_t number_timesteps, int overflow_mode);
 int lmb_run_wait(lmb_lattice *lattice, lmb_run_stats *stats);
+/* One solve queued as a whole on the lattice's stream: new native contents
+ * (lmb_lattice_set_native; either pointer NULL keeps that part), the run
+ * (lmb_run_async), and the final particles copied to out_particles (NULL:
+ * not copied) -- the copyToGPU / timesteps / copyFromGPU of a trajectory
+ * (MpdRdmeSolver.cu:485-668, CudaByteLattice.cu:128-140) with no host wait
+ * between them except the check of the new contents' species ids and site
+ * types, which waits for their upload.  lmb_run_wait ends the solve; the host
+ * buffers must stay valid until then, and pinned host buffers let the copies
+ * overlap work on other streams (two lattices on two contexts pipeline their
+ * solves this way).  After a failed run out_particles is not the partial
+ * lattice: lmb_lattice_get_native after lmb_run_wait gives it. */
+int lmb_run_native_async(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
+                         uint32_t number_timesteps, int overflow_mode, const uint32_t *in_particles,
+                         const uint8_t *in_sites, uint32_t *out_particles);
 /* lmb_run_async that also takes the lattice's species totals at the end of
  * the run (recordSpeciesCounts, MpdRdmeSolver.cu:933-942, with
  * ByteLattice::getParticleCounts, ByteLattice.cpp:495-520) inside the run's

@@ -126,6 +126,7 @@ PROTOTYPES = {
     "lmb_run": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(RunStats)]),
     "lmb_run_async": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int]),
     "lmb_run_wait": (C.c_int, [vp, C.POINTER(RunStats)]),
+    "lmb_run_native_async": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp, vp, vp]),
     "lmb_run_counts_async": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32]),
     "lmb_run_counts_wait": (C.c_int, [vp, C.POINTER(RunStats), u64p]),
     "lmb_run_profiled": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, f32p, u32p,

@@ -1044,6 +1044,33 @@ extern "C" int lmb_run_counts_wait(lmb_lattice *l, lmb_run_stats *st, uint64_t *
     return rc;
 }
 
+extern "C" int lmb_run_native_async(lmb_lattice *l, const lmb_model *m, uint32_t seed, uint32_t first, uint32_t n,
+                                    int mode, const uint32_t *in_particles, const uint8_t *in_sites,
+                                    uint32_t *out_particles)
+{
+    if (!l || !m) return LMB_E_ARG;
+    if (l->pending) return LMB_E_STATE;
+    lmb_ctx *c = l->ctx;
+    CK(cudaSetDevice(c->device));
+    const size_t bytes = (size_t)l->words * l->g.N * 4;
+    if (in_particles || in_sites) {
+        // As lmb_lattice_set_native, without its wait: the run's check of the
+        // new contents (validate_for_model) waits for the upload.
+        if (in_particles) CK(cudaMemcpyAsync(l->buf[l->cur], in_particles, bytes, cudaMemcpyHostToDevice, c->stream));
+        if (in_sites) CK(cudaMemcpyAsync(l->sites, in_sites, l->g.N, cudaMemcpyHostToDevice, c->stream));
+        reset_overflow_queue(l);
+        CK(cudaMemcpyAsync(l->rs, l->rs_host, sizeof(RunState), cudaMemcpyHostToDevice, c->stream));
+        l->validated = false;
+    }
+    int rc = run_async(l, m, seed, first, n, mode, ~0u);
+    if (rc) return rc;
+    // The buffer the run ends in when it succeeds (run_async tracks the
+    // parity as it queues the timesteps).
+    if (out_particles)
+        CK(cudaMemcpyAsync(out_particles, l->buf[l->cur], bytes, cudaMemcpyDeviceToHost, c->stream));
+    return LMB_OK;
+}
+
 extern "C" int lmb_run_wait(lmb_lattice *l, lmb_run_stats *st)
 {
     if (!l) return LMB_E_ARG;

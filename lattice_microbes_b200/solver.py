@@ -239,6 +239,16 @@ class Lattice:
     def run_async(self, model, seed, first_timestep, timesteps, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
         L.check(L.lib().lmb_run_async(self.handle, model.handle, seed, first_timestep, timesteps, overflow_mode))
 
+    def run_native_async(self, model, seed, first_timestep, timesteps, particles_in=0, sites_in=0,
+                         particles_out=0, overflow_mode=L.LMB_OVERFLOW_CLASSIC):
+        """lmb_run_native_async: upload, run and download queued as one solve
+        on the lattice's stream; wait() ends it.  The buffers are host
+        addresses (ints, e.g. a pinned tensor's data_ptr(); 0 for none) of
+        words * N uint32 particles and N uint8 site types, valid until wait()."""
+        L.check(L.lib().lmb_run_native_async(self.handle, model.handle, seed, first_timestep, timesteps,
+                                             overflow_mode, particles_in or None, sites_in or None,
+                                             particles_out or None), "lmb_run_native_async")
+
     def wait(self, check=True):
         st = L.RunStats()
         rc = L.lib().lmb_run_wait(self.handle, C.byref(st))

@@ -229,6 +229,60 @@ def test_autotune_keeps_state_and_result(ctx):
     m.close()
 
 
+@pytest.mark.parametrize("slots,bps,schedule", [(16, 4, "phases"), (8, 1, "fused"), (8, 1, "phases")])
+def test_run_native_async_pipelined(ctx, slots, bps, schedule):
+    """lmb_run_native_async on two lattices of two contexts, their solves
+    pipelined (the next solve of one queued while the other runs), each from
+    new contents and with its own seed: every result equals
+    lmb_lattice_set_native + lmb_run + lmb_lattice_get_native of the same
+    solve, and the first one the oracle's."""
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import Context, Lattice, Model
+    spec = configs.random_problem(71, X=64, Y=16, Z=24, slots=slots, bytes_per_slot=bps, density=0.05 * slots,
+                                  nst=3)  # ~20 K overflows resolved over the 70 timesteps, none exhausted
+    t = oracle_tables(spec)
+    sched = L.LMB_SCHEDULE_PHASES if schedule == "phases" else L.LMB_SCHEDULE_FUSED
+    ctx2 = Context(0)
+    models = [Model.from_tables(ctx, t), Model.from_tables(ctx2, t)]
+    lats = [Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot),
+            Lattice(ctx2, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)]
+    for lat in lats:
+        lat.set_schedule(sched)
+    rng = np.random.default_rng(5)
+    inputs = []
+    for k in range(5):
+        lat_k = spec.lattice.copy()
+        if k:  # other contents: the same particles, shuffled over the sites
+            N = spec.nsites
+            perm = rng.permutation(N)
+            lat_k = lat_k.reshape(-1, N)[:, perm].reshape(-1).copy()
+        inputs.append(np.ascontiguousarray(lat_k, dtype=np.uint32))
+    sites = np.ascontiguousarray(spec.sites, dtype=np.uint8)
+    outs = [np.zeros_like(x) for x in inputs]
+    T = 70  # two captured graphs of 32 timesteps and six single launches
+    for k in range(5):
+        lat = lats[k % 2]
+        if k >= 2:
+            lat.wait()
+        lat.run_native_async(models[k % 2], 100 + k, 3, T, inputs[k].ctypes.data, sites.ctypes.data,
+                             outs[k].ctypes.data)
+    for lat in lats:
+        lat.wait()
+    ref, rc_ref, _ = oracle_run(t, inputs[0], sites, 100, 3, T)
+    assert rc_ref == 0
+    assert np.array_equal(outs[0], ref)
+    solo = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
+    solo.set_schedule(sched)
+    for k in range(1, 5):
+        solo.set_native(inputs[k], sites)
+        solo.run(models[0], 100 + k, 3, T)
+        got, _ = solo.get_native()
+        assert np.array_equal(outs[k], got), k
+    for obj in [solo] + lats + models:
+        obj.close()
+    ctx2.close()
+
+
 def test_chunked_run_equals_single_run(ctx):
     spec = configs.random_problem(8, X=32, Y=16, Z=8, density=0.7)
     t = oracle_tables(spec)
