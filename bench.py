@@ -47,6 +47,12 @@ L2_FLUSH_BYTES = 256 << 20    # larger than the 126 MB L2
 # schedule moves B_sweep = 2 S b + 1 bytes per site per sweep and
 # B_step = 7 S b + 4 per site-step (three sweeps + the reaction read).
 WORKLOADS = {
+    "bimolecular": dict(
+        desc="bimolecular A + B <-> C, 32x32x32 ByteLattice-8, 1 site type, 1000 A + 1000 B, "
+             "10,000 timesteps of 50 us per step",
+        config="config0", S=8, b=1, tau=50e-6, dtype="u8", timesteps_per_step=10000, ref_timesteps=1000,
+        nsm_seg=0.25, nsm_segments=8, ref_mpd_timesteps=600,
+        l2="flushed between timed steps (256 MB write); working set 0.3 MB is L2-resident within a step"),
     "rodcell": dict(
         desc="rod-cell 64x64x128 ByteLattice-8, 3 site types, 5 species, 8 reactions, 5400 particles",
         config="config1", S=8, b=1, tau=25e-6, dtype="u8", timesteps_per_step=500, ref_timesteps=1000,
@@ -94,9 +100,11 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
-    ap.add_argument("--workload", choices=["crowded", "rodcell", "batch", "cme", "serve", "trajectory", "pair"],
+    ap.add_argument("--workload", choices=["crowded", "rodcell", "bimolecular", "batch", "cme", "serve", "trajectory",
+                                           "pair"],
                     default=DEFAULT_WORKLOAD,
                     help="crowded: one 128x128x256 IntLattice-16 (default); rodcell: one 64x64x128 ByteLattice-8; "
+                         "bimolecular: the plain 32x32x32 A + B <-> C run, 10,000 timesteps per step; "
                          "batch: 256 bimolecular replicates of "
                          "uneven size in one launch per timestep; cme: 65,536 two-state gene replicates "
                          "(direct method) to t = 3600 s; serve: a Poisson stream of solve requests; trajectory: "
@@ -577,8 +585,9 @@ def run_ours(a):
                           "planes that can hold particles, so own_dataflow_frac (ncu DRAM bytes per launch) is far "
                           "below it and the sweeps are bound by instruction issue and latency, not HBM") +
                          "; launch times are the device-timed step x the kernel's share of device time in an "
-                         "event-bracketed run" + ("; working set 9 MB is L2-resident" if a.workload == "rodcell"
-                                                  else "")),
+                         "event-bracketed run" + {"rodcell": "; working set 9 MB is L2-resident",
+                                                 "bimolecular": "; working set 0.3 MB is L2-resident"}.get(
+                                                     a.workload, "")),
                 "phases": phases,
                 "sweep_fraction": sweep_fraction,
                 "step_fraction_reference_schedule": value * B_STEP / (peak * 1e9),
@@ -626,7 +635,7 @@ def run_reference(a):
     if value is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return
-    spec_sites = {"rodcell": 64 * 64 * 128, "crowded": 128 * 128 * 256}[wname]
+    spec_sites = make_spec(wname, 1).nsites
     T = a.timesteps_per_step or w["timesteps_per_step"]
     line = {
         "impl": "reference",
