@@ -99,7 +99,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
-    ap.add_argument("--schedule", choices=["auto", "fused", "phases"], default="auto")
+    ap.add_argument("--schedule", choices=["auto", "fused", "phases", "cluster"], default="auto")
     ap.add_argument("--workload", choices=["crowded", "rodcell", "bimolecular", "batch", "cme", "serve", "trajectory",
                                            "pair"],
                     default=DEFAULT_WORKLOAD,
@@ -437,12 +437,16 @@ def run_ours(a):
     tuned = None
     if a.schedule == "phases":
         lat.set_schedule(LL.LMB_SCHEDULE_PHASES)
+    elif a.schedule == "cluster":
+        lat.set_schedule(LL.LMB_SCHEDULE_CLUSTER)
     elif a.schedule == "fused" or a.no_autotune:
         lat.set_schedule(LL.LMB_SCHEDULE_FUSED)
     else:
         tuned = lat.autotune(model, seed, 0, 100)
     sched = lat.schedule()
-    sched_name = ("fused Ty=%d Tz=%d" % (sched[1], sched[2])) if sched[0] == LL.LMB_SCHEDULE_FUSED else "phases"
+    sched_name = {LL.LMB_SCHEDULE_FUSED: "fused Ty=%d Tz=%d" % (sched[1], sched[2]),
+                  LL.LMB_SCHEDULE_CLUSTER: "cluster (whole lattice in one thread-block cluster, one launch per run)"
+                  }.get(sched[0], "phases")
 
     step = 0
     for _ in range(a.warmup):
@@ -492,7 +496,9 @@ def run_ours(a):
     peak, peak_kind = measured_peak_hbm()
     sweep_fraction = None
     if phase_n[5] > 0:
-        kern = "fused_step_kernel (x, y, z sweeps + reaction + overflow, one timestep)"
+        kern = ("cluster_run_kernel (every timestep of the run in one launch; per timestep)"
+                if sched[0] == LL.LMB_SCHEDULE_CLUSTER else
+                "fused_step_kernel (x, y, z sweeps + reaction + overflow, one timestep)")
         launch_ms = phases["fused_step"]["ms_per_launch"]
         alg_bytes = N * B_STEP                 # site-steps per launch x per-site-step bytes
         own_bytes = N * B_SWEEP                # its own dataflow: read slots + site type, write slots

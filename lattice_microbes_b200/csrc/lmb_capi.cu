@@ -648,6 +648,14 @@ extern "C" int lmb_lattice_set_schedule(lmb_lattice *l, int schedule, uint32_t T
         l->schedule = schedule;
         return LMB_OK;
     }
+    if (schedule == LMB_SCHEDULE_CLUSTER) {
+        // The plan is checked with the largest staged tables (8 KiB).
+        uint32_t C = 0, P = 0;
+        CK(cudaSetDevice(l->ctx->device));
+        if (!cluster_plan(l->g, (int)l->bps, (int)l->slots, l->cap, 8 * 1024, C, P)) return LMB_E_UNSUPPORTED;
+        l->schedule = schedule;
+        return LMB_OK;
+    }
     if (schedule != LMB_SCHEDULE_FUSED) return LMB_E_ARG;
     TileShape t;
     bool ok = (Ty == 0 && Tz == 0) ? fused_default_shape(l->g, (int)l->bps, (int)l->slots, t)
@@ -986,11 +994,20 @@ static int run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_
         }
         CK(cudaMemsetAsync(l->counts_dev, 0, sizeof(unsigned long long) * (count_ns + 1), c->stream));
     }
+    // The cluster-resident schedule resolves overflows the classic way only.
+    if (l->schedule == LMB_SCHEDULE_CLUSTER && mode != LMB_OVERFLOW_CLASSIC) return LMB_E_UNSUPPORTED;
     CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream, in_kernel ? first + n - 1 : ~0u, count_ns,
                         l->counts_dev));
     CK(reset_plane_bounds(l, c->stream));
     l->pending_cur0 = l->cur;
     uint32_t done = 0;
+    if (l->schedule == LMB_SCHEDULE_CLUSTER && n > 0) {
+        // Every timestep in one launch, ending in the buffer n's parity gives.
+        CK(launch_cluster_run((int)l->bps, (int)l->slots, l->buf[l->cur], l->buf[l->cur ^ 1], l->sites, l->g,
+                              m->dev, l->rs, l->list, l->cap, c->stream));
+        l->cur ^= (int)(n & 1u);
+        done = n;
+    }
     // Whole graphs of GRAPH_STEPS timesteps, then single launches.
     // A stream that cannot be captured (the legacy default stream) runs
     // every timestep as single launches.
@@ -1120,10 +1137,23 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
     for (auto &e : ev) CK(cudaEventCreate(&e));
     const int bps = (int)l->bps, S = (int)l->slots;
     const int cur0 = l->cur;
-    const bool fused = l->schedule == LMB_SCHEDULE_FUSED;
+    const bool cluster = l->schedule == LMB_SCHEDULE_CLUSTER;
+    const bool fused = l->schedule == LMB_SCHEDULE_FUSED || cluster;
+    if (cluster && mode != LMB_OVERFLOW_CLASSIC) return LMB_E_UNSUPPORTED;
     for (uint32_t s = 0; s < n; s++) {
         uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
         cudaEvent_t *E = &ev[(size_t)s * 12];
+        if (cluster) {
+            // One launch runs every timestep; its time counts under the
+            // fused-timestep entry, one launch per timestep.
+            CK(cudaEventRecord(E[10], c->stream));
+            if (s == 0) {
+                CK(launch_cluster_run(bps, S, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+                l->cur ^= (int)(n & 1u);
+            }
+            CK(cudaEventRecord(E[11], c->stream));
+            continue;
+        }
         if (fused) {
             CK(cudaEventRecord(E[10], c->stream));
             CK(launch_fused(bps, S, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, l->tile, m->nr > 0,
@@ -1215,7 +1245,7 @@ extern "C" int lmb_lattice_autotune(lmb_lattice *l, const lmb_model *m, uint32_t
     const int sched0 = l->schedule;
     const TileShape tile0 = l->tile;
     struct Cand { int sched; uint32_t ty, tz; };
-    std::vector<Cand> cands = {{LMB_SCHEDULE_PHASES, 0, 0}};
+    std::vector<Cand> cands = {{LMB_SCHEDULE_PHASES, 0, 0}, {LMB_SCHEDULE_CLUSTER, 0, 0}};
     const uint32_t dims[] = {1, 2, 4, 8, 16};
     for (uint32_t ty : dims)
         for (uint32_t tz : dims) {
@@ -1236,6 +1266,12 @@ extern "C" int lmb_lattice_autotune(lmb_lattice *l, const lmb_model *m, uint32_t
             cudaMemcpyAsync(l->buf[l->cur], save, wbytes, cudaMemcpyDeviceToDevice, c->stream);
             cudaEventRecord(e0, c->stream);
             rc = lmb_run_async(l, m, seed, first, timesteps, LMB_OVERFLOW_CLASSIC);
+            if (rc != LMB_OK && cd.sched == LMB_SCHEDULE_CLUSTER && rc == LMB_E_CUDA) {
+                // A cluster the device would not launch: not a candidate.
+                cudaGetLastError();
+                rc = LMB_OK;
+                break;
+            }
             if (rc != LMB_OK) break;
             cudaEventRecord(e1, c->stream);
             lmb_run_stats st;

@@ -17,6 +17,7 @@
 // only the owner of a site queues its overflows.  The last block of a launch
 // to finish resolves the overflow queue (lmb_overflow.cuh), so a timestep is a
 // single launch.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -809,6 +810,326 @@ cudaError_t launch_fused_batch(int bps, int slots, const FusedJob *jobs, uint32_
     BATCH_DISPATCH(4, 4)
     BATCH_DISPATCH(4, 8)
     BATCH_DISPATCH(4, 16)
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// Cluster-resident runs of small lattices
+// ---------------------------------------------------------------------------
+//
+// A lattice whose two buffers fit in the shared memory of one thread-block
+// cluster runs a whole run in one launch.  CTA `rank` of the C in the cluster
+// holds z planes rank * P .. rank * P + P - 1 (both buffers and the site
+// types), so the x and y sweeps read only its own shared memory and the z
+// sweep reads the neighbouring CTA's edge plane through distributed shared
+// memory.  Hardware cluster barriers replace the launches between phases:
+// one before the z sweep (the other CTAs' y output complete) and one after
+// it (their z reads done before the next x sweep overwrites that buffer).
+// Every site belongs to exactly one CTA, so sweep_site records its
+// overflows once; the reaction runs on each site right after its z sweep.
+// A timestep in which any site of the cluster ended full may have queued
+// overflows: then the state goes to global memory, CTA 0 resolves the queue
+// there (the same resolve_block_flat, step counter included), and every
+// CTA reloads its planes.  The sweep rules, hashes and orders are those of
+// the fused and per-phase kernels, so the result is theirs bit for bit.
+//
+// All CTAs run the same number of timesteps and take every branch that
+// holds a cluster barrier together: the loop bounds come from the run state
+// written before the launch, and the two decisions inside the loop (a full
+// site somewhere, a failed resolution) are read by all CTAs from the same
+// place after a barrier.
+constexpr uint32_t CLUSTER_THREADS = 1024;
+
+template <int BPS, int S>
+__device__ __forceinline__ bool site_full(const SiteWords<BPS, S> &s)
+{
+    return __popc(occupied_slots<BPS, S>(s)) == S;
+}
+
+template <int BPS, int S>
+__global__ void __launch_bounds__(CLUSTER_THREADS, 1)
+    cluster_run_kernel(uint32_t *__restrict__ buf0, uint32_t *__restrict__ buf1, const uint8_t *__restrict__ sites,
+                       Geometry g, const __grid_constant__ DevTables m, RunState *__restrict__ rs,
+                       OverflowEntry *__restrict__ list, uint32_t cap, uint32_t P, uint32_t words_at,
+                       uint32_t tables_at)
+{
+    namespace cg = cooperative_groups;
+    constexpr int W = SiteWords<BPS, S>::W;
+    cg::cluster_group cl = cg::this_cluster();
+    const uint32_t rank = cl.block_rank(), C = cl.num_blocks();
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x;
+    const uint32_t X = g.X, Y = g.Y, XY = g.XY, n = P * XY, z0 = rank * P;
+    // Dynamic shared memory: the site types T[n]; at words_at the two
+    // buffers' words A[W][n], B[W][n], a region that CTA 0's overflow sort
+    // reuses (the state is in global memory then) and that is sized for it;
+    // the staged model tables at tables_at.
+    extern __shared__ __align__(16) uint32_t smem[];
+    uint8_t *T = reinterpret_cast<uint8_t *>(smem);
+    uint32_t *A = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(smem) + words_at);
+    uint32_t *B = A + (size_t)W * n;
+    OverflowEntry *sort = reinterpret_cast<OverflowEntry *>(A);
+    uint8_t *tab = reinterpret_cast<uint8_t *>(smem) + tables_at;
+    __shared__ uint32_t s_flag[2];  // CTA 0's: a site of the cluster ended full, by timestep parity
+    __shared__ uint32_t s_full, s_go;
+    __shared__ DevTables s_mt;
+    const uint32_t seed = rs->seed, first = rs->step, end = rs->end_step;
+    if (rs->status != LMB_OK || first >= end) return;  // the same for every CTA
+    {
+        const DevTables staged = m.stage_bytes ? stage_tables(m, tab, tid, nthr) : m;
+        if (tid == 0) {
+            s_mt = staged;
+            s_flag[0] = s_flag[1] = 0;
+            s_full = 0;
+        }
+    }
+    for (uint32_t k = 0; k < (uint32_t)W; k++)
+        for (uint32_t l = tid; l < n; l += nthr) A[k * n + l] = __ldcg(buf0 + (size_t)k * g.N + (size_t)z0 * XY + l);
+    for (uint32_t l = tid; l < n; l += nthr) T[l] = sites[(size_t)z0 * XY + l];
+    bool zeroth = false;
+    for (uint32_t q = 0; q < m.nst; q++) zeroth |= m.qp0[q] != 0.0f;
+    const bool reacting = m.nr > 0;
+    cl.sync();  // every CTA's planes and flags in place before any remote access
+    const DevTables &mt = s_mt;
+    const TableSet tabs{&mt};
+    const uint32_t rm = rank == 0 ? C - 1 : rank - 1, rp = rank == C - 1 ? 0 : rank + 1;
+    uint32_t parity = 0;  // the global buffer a copy of the current state belongs in: buf0 or buf1
+    for (uint32_t step = first; step < end; step++) {
+        uint32_t full = 0;
+        // x sweep, A -> B.
+        {
+            const unsigned long long th = timestep_hash(seed, step, 0);
+            for (uint32_t l = tid; l < n; l += nthr) {
+                const uint32_t x = l % X, xm = x == 0 ? X - 1 : x - 1, xp = x == X - 1 ? 0 : x + 1;
+                const uint32_t lm = l - x + xm, lp = l - x + xp, gi = z0 * XY + l;
+                SiteWords<BPS, S> own, mn, pl;
+                load_smem<BPS, S>(A, n, l, own);
+                load_smem<BPS, S>(A, n, lm, mn);
+                load_smem<BPS, S>(A, n, lp, pl);
+                own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], gi, gi - x + xm, gi - x + xp, th, tabs,
+                                         true, 1u, rs, list, cap);
+                store_smem<BPS, S>(B, n, l, own);
+                full |= site_full<BPS, S>(own) ? 1u : 0u;
+            }
+        }
+        __syncthreads();
+        // y sweep, B -> A.
+        {
+            const unsigned long long th = timestep_hash(seed, step, 1);
+            for (uint32_t l = tid; l < n; l += nthr) {
+                const uint32_t p = l / XY, r = l - p * XY, y = r / X;
+                const uint32_t ym = y == 0 ? Y - 1 : y - 1, yp = y == Y - 1 ? 0 : y + 1;
+                const uint32_t lm = l - y * X + ym * X, lp = l - y * X + yp * X, gi = z0 * XY + l;
+                SiteWords<BPS, S> own, mn, pl;
+                load_smem<BPS, S>(B, n, l, own);
+                load_smem<BPS, S>(B, n, lm, mn);
+                load_smem<BPS, S>(B, n, lp, pl);
+                own = sweep_site<BPS, S>(own, mn, pl, T[l], T[lm], T[lp], gi, gi - y * X + ym * X,
+                                         gi - y * X + yp * X, th, tabs, true, 2u, rs, list, cap);
+                store_smem<BPS, S>(A, n, l, own);
+                full |= site_full<BPS, S>(own) ? 1u : 0u;
+            }
+        }
+        cl.sync();  // every CTA's y output in place before the z sweep reads edge planes
+        // z sweep, A -> B, and the reaction of each site right after it.
+        {
+            const unsigned long long th = timestep_hash(seed, step, 2), th_rx = timestep_hash(seed, step, 3);
+            const uint32_t *Am = cl.map_shared_rank(A, rm), *Ap = cl.map_shared_rank(A, rp);
+            const uint8_t *Tm = cl.map_shared_rank(T, rm), *Tp = cl.map_shared_rank(T, rp);
+            for (uint32_t l = tid; l < n; l += nthr) {
+                const uint32_t p = l / XY, r = l - p * XY, z = z0 + p;
+                const uint32_t zm = z == 0 ? g.Z - 1 : z - 1, zp = z == g.Z - 1 ? 0 : z + 1;
+                const uint32_t gi = z * XY + r;
+                SiteWords<BPS, S> own, mn, pl;
+                load_smem<BPS, S>(A, n, l, own);
+                uint32_t tm, tp;
+                if (p > 0) {
+                    load_smem<BPS, S>(A, n, l - XY, mn);
+                    tm = T[l - XY];
+                } else {  // plane P - 1 of the CTA before (periodic)
+                    load_smem<BPS, S>(Am, n, (P - 1) * XY + r, mn);
+                    tm = Tm[(P - 1) * XY + r];
+                }
+                if (p + 1 < P) {
+                    load_smem<BPS, S>(A, n, l + XY, pl);
+                    tp = T[l + XY];
+                } else {  // plane 0 of the CTA after
+                    load_smem<BPS, S>(Ap, n, r, pl);
+                    tp = Tp[r];
+                }
+                own = sweep_site<BPS, S>(own, mn, pl, T[l], tm, tp, gi, zm * XY + r, zp * XY + r, th, tabs, true,
+                                         3u, rs, list, cap);
+                if (reacting && (zeroth || !own.empty())) {
+                    const uint32_t ts = T[l];
+                    const float a0 = tload(mt.qp0 + ts);
+                    if (!own.empty() || a0 != 0.0f) {
+                        const float r0 = hash_float((unsigned long long)gi << 1, th_rx);
+                        if (reaction_may_fire((uint32_t)__popc(occupied_slots<BPS, S>(own)), a0, ts, r0, mt))
+                            own = react_site_ool<BPS, S>(own, ts, gi, th_rx, mt, rs, list, cap);
+                    }
+                }
+                store_smem<BPS, S>(B, n, l, own);
+                full |= site_full<BPS, S>(own) ? 1u : 0u;
+            }
+        }
+        if (full) atomicOr(&s_full, 1u);
+        __syncthreads();
+        if (tid == 0 && s_full) atomicOr(cl.map_shared_rank(&s_flag[step & 1u], 0), 1u);
+        cl.sync();  // every z output and every flag in place
+        if (tid == 0) {
+            s_go = *cl.map_shared_rank(&s_flag[step & 1u], 0);
+            s_full = 0;
+            if (rank == 0) s_flag[(step + 1u) & 1u] = 0;  // the next timestep's flag, unused until then
+        }
+        __syncthreads();
+        parity ^= 1u;
+        if (s_go) {
+            // Overflows may be queued: resolve them in global memory as the
+            // per-phase and fused schedules do.
+            uint32_t *gb = parity ? buf1 : buf0;
+            for (uint32_t k = 0; k < (uint32_t)W; k++)
+                for (uint32_t l = tid; l < n; l += nthr) gb[(size_t)k * g.N + (size_t)z0 * XY + l] = B[k * n + l];
+            __threadfence();
+            cl.sync();  // the whole state in gb; no remote reads of shared memory remain
+            if (rank == 0) {
+                if (tid == 0) rs->step = step;
+                __syncthreads();
+                resolve_block_flat<BPS, S>(gb, sites, g, rs, list, cap, sort, tid, nthr, nullptr);
+                __threadfence();
+            }
+            cl.sync();  // the resolution (or its failure) visible to every CTA
+            if (*(volatile int32_t *)&rs->status != LMB_OK) return;  // the partial lattice is in gb
+            for (uint32_t k = 0; k < (uint32_t)W; k++)
+                for (uint32_t l = tid; l < n; l += nthr) B[k * n + l] = __ldcg(gb + (size_t)k * g.N + (size_t)z0 * XY + l);
+            __syncthreads();
+        }
+        uint32_t *t0 = A;
+        A = B;
+        B = t0;
+    }
+    // The final state, in the buffer the timestep count's parity gives.
+    uint32_t *gb = parity ? buf1 : buf0;
+    for (uint32_t k = 0; k < (uint32_t)W; k++)
+        for (uint32_t l = tid; l < n; l += nthr) gb[(size_t)k * g.N + (size_t)z0 * XY + l] = A[k * n + l];
+    if (rank == 0 && tid == 0) set_step(rs, seed, end);
+    cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// Plan of a cluster-resident run: C CTAs (the largest of 16, 8, 4, 2, 1 that
+// divides Z and that the device can place) of P = Z / C planes each, and the
+// dynamic shared memory of a CTA.  False when the lattice does not fit.
+// Byte offsets in a CTA's dynamic shared memory: the buffers' words (and the
+// overflow sort) at words_at, after the site types; the tables at tables_at.
+static void cluster_layout(const Geometry &g, uint32_t W, uint32_t P, uint32_t cap, size_t &words_at,
+                           size_t &tables_at)
+{
+    const size_t n = (size_t)P * g.XY;
+    words_at = (n + 15) & ~(size_t)15;
+    const size_t words = 2 * (size_t)W * n * 4;
+    const size_t sort = (size_t)pow2_at_least(cap) * sizeof(OverflowEntry);
+    tables_at = words_at + ((words > sort ? words : sort) + 15 & ~(size_t)15);
+}
+
+template <int BPS, int S>
+static bool cluster_plan_t(const Geometry &g, uint32_t cap, uint32_t stage_bytes, uint32_t &C, uint32_t &P,
+                           size_t &words_at, size_t &tables_at, size_t &smem)
+{
+    const uint32_t W = SiteWords<BPS, S>::W;
+    for (uint32_t c = 16; c >= 1; c >>= 1) {
+        if (g.Z % c) continue;
+        const uint32_t p = g.Z / c;
+        size_t wa = 0, ta = 0;
+        cluster_layout(g, W, p, cap, wa, ta);
+        const size_t sm = ta + stage_bytes;
+        if (sm > 200 * 1024) continue;
+        if (cudaFuncSetAttribute(cluster_run_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(cluster_run_kernel<BPS, S>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(CLUSTER_THREADS);
+        cfg.dynamicSmemBytes = sm;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, cluster_run_kernel<BPS, S>, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (clusters < 1) continue;
+        C = c;
+        P = p;
+        words_at = wa;
+        tables_at = ta;
+        smem = sm;
+        return true;
+    }
+    return false;
+}
+
+#define CLUSTER_DISPATCH(BPS_, S_, ...) \
+    if (bps == BPS_ && slots == S_) {   \
+        __VA_ARGS__;                    \
+    }
+
+bool cluster_plan(const Geometry &g, int bps, int slots, uint32_t cap, uint32_t stage_bytes, uint32_t &C,
+                  uint32_t &P)
+{
+    size_t words_at = 0, tables_at = 0, smem = 0;
+    if (slots > 16) return false;
+    CLUSTER_DISPATCH(1, 4, return cluster_plan_t<1, 4>(g, cap, stage_bytes, C, P, words_at, tables_at, smem))
+    CLUSTER_DISPATCH(1, 8, return cluster_plan_t<1, 8>(g, cap, stage_bytes, C, P, words_at, tables_at, smem))
+    CLUSTER_DISPATCH(1, 16, return cluster_plan_t<1, 16>(g, cap, stage_bytes, C, P, words_at, tables_at, smem))
+    CLUSTER_DISPATCH(4, 4, return cluster_plan_t<4, 4>(g, cap, stage_bytes, C, P, words_at, tables_at, smem))
+    CLUSTER_DISPATCH(4, 8, return cluster_plan_t<4, 8>(g, cap, stage_bytes, C, P, words_at, tables_at, smem))
+    CLUSTER_DISPATCH(4, 16, return cluster_plan_t<4, 16>(g, cap, stage_bytes, C, P, words_at, tables_at, smem))
+    return false;
+}
+
+template <int BPS, int S>
+static cudaError_t cluster_launch_t(uint32_t *buf0, uint32_t *buf1, const uint8_t *sites, const Geometry &g,
+                                    const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
+                                    cudaStream_t stream)
+{
+    uint32_t C = 0, P = 0;
+    size_t words_at = 0, tables_at = 0, smem = 0;
+    if (!cluster_plan_t<BPS, S>(g, cap, m.stage_bytes, C, P, words_at, tables_at, smem))
+        return cudaErrorInvalidConfiguration;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(CLUSTER_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    count_launch();
+    return cudaLaunchKernelEx(&cfg, cluster_run_kernel<BPS, S>, buf0, buf1, sites, g, m, rs, list, cap, P,
+                              (uint32_t)words_at, (uint32_t)tables_at);
+}
+
+cudaError_t launch_cluster_run(int bps, int slots, uint32_t *buf0, uint32_t *buf1, const uint8_t *sites,
+                               const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
+                               cudaStream_t stream)
+{
+    CLUSTER_DISPATCH(1, 4, return cluster_launch_t<1, 4>(buf0, buf1, sites, g, m, rs, list, cap, stream))
+    CLUSTER_DISPATCH(1, 8, return cluster_launch_t<1, 8>(buf0, buf1, sites, g, m, rs, list, cap, stream))
+    CLUSTER_DISPATCH(1, 16, return cluster_launch_t<1, 16>(buf0, buf1, sites, g, m, rs, list, cap, stream))
+    CLUSTER_DISPATCH(4, 4, return cluster_launch_t<4, 4>(buf0, buf1, sites, g, m, rs, list, cap, stream))
+    CLUSTER_DISPATCH(4, 8, return cluster_launch_t<4, 8>(buf0, buf1, sites, g, m, rs, list, cap, stream))
+    CLUSTER_DISPATCH(4, 16, return cluster_launch_t<4, 16>(buf0, buf1, sites, g, m, rs, list, cap, stream))
     return cudaErrorInvalidValue;
 }
 

@@ -55,4 +55,17 @@ cudaError_t launch_fused(int bytes_per_slot, int slots, const uint32_t *src, uin
                          const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
                          const TileShape &ts, int with_reaction, cudaStream_t stream);
 
+// Cluster-resident runs of small lattices (lmb_fused.cu): the whole lattice
+// in the shared memory of one thread-block cluster of C CTAs (P = Z / C z
+// planes each), every timestep of a run in one launch.  cluster_plan is
+// false when the lattice does not fit or the device cannot place the cluster
+// (it sets the kernel's attributes on the current device).  The run starts
+// from buf0 and ends in buf0 or buf1 by the parity of its timestep count (of
+// the failing timestep + 1 when it fails), as alternating launches would.
+bool cluster_plan(const Geometry &g, int bytes_per_slot, int slots, uint32_t cap, uint32_t stage_bytes, uint32_t &C,
+                  uint32_t &P);
+cudaError_t launch_cluster_run(int bytes_per_slot, int slots, uint32_t *buf0, uint32_t *buf1, const uint8_t *sites,
+                               const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
+                               cudaStream_t stream);
+
 }  // namespace lmb

@@ -36,6 +36,8 @@ def _gpu_run(ctx, tables_or_spec, lattice, sites, seed, step0, nsteps, mode=0, f
     lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
     if schedule == "phases":
         lat.set_schedule(L.LMB_SCHEDULE_PHASES)
+    elif schedule == "cluster":
+        lat.set_schedule(L.LMB_SCHEDULE_CLUSTER)
     else:
         lat.set_schedule(L.LMB_SCHEDULE_FUSED, *tile)
     lat.set_native(lattice, sites)
@@ -281,6 +283,45 @@ def test_run_native_async_pipelined(ctx, slots, bps, schedule):
     for obj in [solo] + lats + models:
         obj.close()
     ctx2.close()
+
+
+@pytest.mark.parametrize("shape,slots,bps,per_slot,nsteps", [
+    ((32, 32, 32), 8, 1, 0.01, 40),    # the plain bimolecular size: 16 CTAs of two planes
+    ((16, 16, 16), 4, 1, 0.2, 40),     # one plane per CTA: both z neighbours remote
+    ((24, 20, 48), 16, 1, 0.05, 30),   # odd plane sizes, three planes per CTA
+    ((32, 16, 32), 4, 4, 0.15, 30),    # IntLattice
+    ((32, 8, 16), 8, 1, 0.5, 20),      # dense: overflows resolved in global memory most timesteps
+    ((32, 8, 12), 8, 1, 0.9, 10),      # denser still: four CTAs, the run may fail as the oracle's does
+])
+def test_cluster_schedule_vs_oracle(ctx, shape, slots, bps, per_slot, nsteps):
+    """The cluster-resident schedule (the whole lattice in one thread-block
+    cluster, every timestep of the run in one launch) against the oracle: the
+    same status, statistics and lattice, including timesteps whose overflows
+    go through global memory and runs that stop at a failed resolution."""
+    X, Y, Z = shape
+    spec = configs.random_problem(81, X=X, Y=Y, Z=Z, slots=slots, bytes_per_slot=bps, density=per_slot * slots,
+                                  nst=3)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 31, 5, nsteps)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 31, 5, nsteps, schedule="cluster",
+                           chunks=[nsteps // 2, nsteps - nsteps // 2])
+    assert rc == rc_ref
+    if rc == 0:
+        assert sum(x.overflows for x in st) == st_ref.overflows
+        assert sum(x.reactions for x in st) == st_ref.reactions
+    assert np.array_equal(out, ref)
+
+
+def test_cluster_schedule_bimolecular_vs_oracle(ctx):
+    """The plain 32^3 bimolecular model on the cluster-resident schedule,
+    300 timesteps in three runs, against the oracle."""
+    spec = configs.config0(seed=3)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 77, 0, 300)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 77, 0, 300, schedule="cluster", chunks=[100, 100, 100])
+    assert rc == rc_ref == 0
+    assert sum(x.reactions for x in st) == st_ref.reactions > 0
+    assert np.array_equal(out, ref)
 
 
 def test_chunked_run_equals_single_run(ctx):
