@@ -529,9 +529,11 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     __shared__ uint16_t yrow[FUSED_MAX_ROWS], zrow[FUSED_MAX_ROWS];
     __shared__ uint8_t rowflag[FUSED_MAX_ROWS];
     // A failed run stops; in a batch, a lattice whose own timestep range is
-    // done sits out the remaining launches.
-    if (rs->status != LMB_OK || rs->step >= rs->end_step) return;
-    const uint32_t seed = rs->seed, step = rs->step;
+    // done sits out the remaining launches.  The run state is loaded now and
+    // checked after the region load (before the first write), so that its
+    // round trip overlaps the loads.
+    const int32_t status = rs->status;
+    const uint32_t seed = rs->seed, step = rs->step, end_step = rs->end_step;
     const uint32_t tid = threadIdx.x, nthr = blockDim.x;
     const TileSmem t = tile_smem<BPS, S>(smem, ts, rowbase, yrow, zrow, rowflag, s_cnt);
     // The model tables, from shared memory when they are small; the table set
@@ -545,6 +547,7 @@ __device__ __forceinline__ void fused_tile(const uint32_t *__restrict__ src, uin
     tile_rows(g, ts, tile, t);
     __syncthreads();
     tile_load<BPS, S, false>(src, sites, g, ts, t, t.A, t.occA, false, true);
+    if (status != LMB_OK || step >= end_step) return;  // the same for the whole block
 
     uint32_t *src_w = t.A, *dst_w = t.B, *src_o = t.occA, *dst_o = t.occB;
     tile_timestep<BPS, S, ROWS>(g, s_mt, rs, list, cap, ts, t, src_w, dst_w, src_o, dst_o, seed, step,

@@ -163,7 +163,10 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
     __shared__ uint32_t sw[W][NT];
     __shared__ Code sc[NT];
     chain_enter();
-    if (rs->status != LMB_OK) return;
+    // The run state's status is loaded with everything else and checked
+    // before the first write (a failed run's kernels do nothing), so that
+    // its round trip does not come first.
+    const int32_t status = rs->status;
     // The z sweep lists reaction sites unless the list overflowed recently.
     const bool listing = DIM == 2 && rs->rx_skip == 0;
     uint32_t x, y, z;
@@ -196,6 +199,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_THREADS) sweep_kernel(const uint32_t
             for (int k = 0; k < W; k++) sw[k][lid] = own.w[k];
         }
     }
+    if (status != LMB_OK) return;  // the same for the whole block
     sc[lid] = 0;
     __syncwarp();
     // The warp's particles drawn together: particle q of the warp (in site,
@@ -423,7 +427,9 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
     uint16_t *pl = reinterpret_cast<uint16_t *>(so + NT);
     uint32_t(*ow)[NT] = reinterpret_cast<uint32_t(*)[NT]>(pl + NT * S);
     chain_enter();
-    if (rs->status != LMB_OK) return;
+    // Checked before the first write, loaded with everything else (as in
+    // sweep_kernel).
+    const int32_t status = rs->status;
     const bool listing = DIM == 2 && rx_sites && rs->rx_skip == 0;
     uint32_t x, y, z;
     bool in, out;
@@ -471,6 +477,7 @@ __global__ void __launch_bounds__(NT, DIM == 0 ? 4 : 3)
             occ |= word_slots(vk, k);
         }
     }
+    if (status != LMB_OK) return;  // the same for the whole block
     so[lid] = occ | (out ? OUT : 0u);
     sc[lid] = 0;
     if (BPS == 1) {
@@ -616,10 +623,13 @@ __global__ void __launch_bounds__(256) reaction_kernel(uint32_t *__restrict__ la
 {
     constexpr int W = SiteWords<BPS, S>::W;
     chain_enter();
-    if (rs->status != LMB_OK) return;
+    // The status, the list's state and the hash in one round trip.
+    const int32_t status = rs->status;
+    const uint32_t rx_skip = rs->rx_skip, rx_count = rs->rx_count;
+    if (status != LMB_OK) return;
     // The sites the z sweep listed, or every site when it listed none or
     // more than the list holds.
-    const uint32_t listed = rx_sites && rs->rx_skip == 0 ? rs->rx_count : 0xFFFFFFFFu;
+    const uint32_t listed = rx_sites && rx_skip == 0 ? rx_count : 0xFFFFFFFFu;
     const bool all = listed > rx_cap;
     const uint32_t n = all ? g.N : listed;
     const unsigned long long th = rs->th[3];
