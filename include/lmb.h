@@ -228,8 +228,10 @@ int lmb_run_wait(lmb_lattice *lattice, lmb_run_stats *stats);
  * (lmb_run_async), and the final particles copied to out_particles (NULL:
  * not copied) -- the copyToGPU / timesteps / copyFromGPU of a trajectory
  * (MpdRdmeSolver.cu:485-668, CudaByteLattice.cu:128-140) with no host wait
- * between them except the check of the new contents' species ids and site
- * types, which waits for their upload.  lmb_run_wait ends the solve; the host
+ * between them.  New contents are checked on the device ahead of the
+ * timesteps: a species id above the model's or a site type beyond it fails
+ * the solve with LMB_E_ARG (from lmb_run_wait, no timestep run, the uploaded
+ * contents left in place).  lmb_run_wait ends the solve; the host
  * buffers must stay valid until then, and pinned host buffers let the copies
  * overlap work on other streams (two lattices on two contexts pipeline their
  * solves this way).  After a failed run out_particles is not the partial

@@ -100,6 +100,7 @@ struct lmb_lattice {
     bool pending;
     int pending_cur0;
     uint32_t pending_first, pending_n;
+    bool pending_check;  // its new contents are checked on the device (lmb_run_native_async)
 };
 
 #define CK(call)                                      \
@@ -962,8 +963,12 @@ static int validate_for_model(lmb_lattice *l, const lmb_model *m)
 
 // count_ns ~0u: no species count; otherwise the lattice's species totals at
 // the end of the run are taken in the run's own work (lmb_run_counts_async).
+// device_check: the lattice's contents were just uploaded in the same
+// stream; they are checked by kernels queued ahead of the timesteps (a bad
+// species id or site type fails the run with LMB_E_ARG) instead of by a host
+// round trip.
 static int run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_t first, uint32_t n, int mode,
-                     uint32_t count_ns)
+                     uint32_t count_ns, bool device_check = false)
 {
     if (!l || !mc) return LMB_E_ARG;
     if (l->pending) return LMB_E_STATE;
@@ -977,7 +982,7 @@ static int run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_
         int rc = upload_model(m);
         if (rc) return rc;
     }
-    int rc = validate_for_model(l, m);
+    int rc = device_check ? LMB_OK : validate_for_model(l, m);
     if (rc) return rc;
     const bool counting = count_ns != ~0u;
     // The fused kernel counts in its last launch when its work list can hold
@@ -998,8 +1003,13 @@ static int run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_
     if (l->schedule == LMB_SCHEDULE_CLUSTER && mode != LMB_OVERFLOW_CLASSIC) return LMB_E_UNSUPPORTED;
     CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream, in_kernel ? first + n - 1 : ~0u, count_ns,
                         l->counts_dev));
+    if (device_check) {
+        CK(launch_validate((int)l->bps, (int)l->slots, l->buf[l->cur], l->sites, l->g, l->rs, c->stream));
+        CK(launch_check_contents(l->rs, m->ns, m->nst, c->stream));
+    }
     CK(reset_plane_bounds(l, c->stream));
     l->pending_cur0 = l->cur;
+    l->pending_check = device_check;
     uint32_t done = 0;
     if (l->schedule == LMB_SCHEDULE_CLUSTER && n > 0) {
         // Every timestep in one launch, ending in the buffer n's parity gives.
@@ -1071,15 +1081,15 @@ extern "C" int lmb_run_native_async(lmb_lattice *l, const lmb_model *m, uint32_t
     CK(cudaSetDevice(c->device));
     const size_t bytes = (size_t)l->words * l->g.N * 4;
     if (in_particles || in_sites) {
-        // As lmb_lattice_set_native, without its wait: the run's check of the
-        // new contents (validate_for_model) waits for the upload.
+        // As lmb_lattice_set_native, without its wait; the new contents are
+        // checked on the device ahead of the timesteps.
         if (in_particles) CK(cudaMemcpyAsync(l->buf[l->cur], in_particles, bytes, cudaMemcpyHostToDevice, c->stream));
         if (in_sites) CK(cudaMemcpyAsync(l->sites, in_sites, l->g.N, cudaMemcpyHostToDevice, c->stream));
         reset_overflow_queue(l);
         CK(cudaMemcpyAsync(l->rs, l->rs_host, sizeof(RunState), cudaMemcpyHostToDevice, c->stream));
         l->validated = false;
     }
-    int rc = run_async(l, m, seed, first, n, mode, ~0u);
+    int rc = run_async(l, m, seed, first, n, mode, ~0u, in_particles || in_sites);
     if (rc) return rc;
     // The buffer the run ends in when it succeeds (run_async tracks the
     // parity as it queues the timesteps).
@@ -1098,7 +1108,19 @@ extern "C" int lmb_run_wait(lmb_lattice *l, lmb_run_stats *st)
     CK(cudaStreamSynchronize(c->stream));
     const RunState &h = *l->rs_host;
     uint32_t done = h.status == LMB_OK ? l->pending_n : h.failed_step - l->pending_first;
-    if (h.status != LMB_OK) {
+    const bool refused = l->pending_check && h.status == LMB_E_ARG;
+    if (l->pending_check) {
+        // The device's check of the contents, kept as the host's would be.
+        l->max_species = h.max_species;
+        l->max_site_type = h.max_site_type;
+        l->validated = true;
+        l->pending_check = false;
+    }
+    if (refused) {
+        // Refused before the first timestep: the lattice is where it was.
+        done = 0;
+        l->cur = l->pending_cur0;
+    } else if (h.status != LMB_OK) {
         // Kernels after the failing step did nothing: the lattice sits in the
         // buffer reached after done + 1 steps (each step flips once).
         l->cur = l->pending_cur0 ^ (int)((done + 1) & 1u);

@@ -153,6 +153,9 @@ cudaError_t launch_gather_states(RunState *const *rs_ptrs, uint32_t count, RunSt
 cudaError_t launch_counts(int bytes_per_slot, int slots, const uint32_t *lat, const Geometry &g,
                           uint32_t ns, unsigned long long *counts, cudaStream_t stream,
                           const uint32_t *pb = nullptr);
+// Fails the run (LMB_E_ARG) when the maxima launch_validate left in the run
+// state exceed the model's species or site types.
+cudaError_t launch_check_contents(RunState *rs, uint32_t ns, uint32_t nst, cudaStream_t stream);
 cudaError_t launch_validate(int bytes_per_slot, int slots, const uint32_t *lat, const uint8_t *sites,
                             const Geometry &g, RunState *rs, cudaStream_t stream);
 cudaError_t launch_row_major_to_native(int bytes_per_slot, int slots, const void *rm_particles,

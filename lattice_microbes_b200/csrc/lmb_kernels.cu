@@ -719,6 +719,24 @@ __global__ void begin_run_kernel(RunState *rs, uint32_t seed, uint32_t first, ui
     }
 }
 
+// A run whose lattice holds a species id above ns or a site type of nst or
+// more (validate_kernel's maxima) fails before its first timestep with
+// LMB_E_ARG, as the host check of a synchronous run refuses it.
+__global__ void check_contents_kernel(RunState *rs, uint32_t ns, uint32_t nst)
+{
+    if (rs->max_species > ns || rs->max_site_type >= nst) {
+        rs->status = LMB_E_ARG;
+        rs->failed_step = rs->step;
+    }
+}
+
+cudaError_t launch_check_contents(RunState *rs, uint32_t ns, uint32_t nst, cudaStream_t stream)
+{
+    count_launch();
+    check_contents_kernel<<<1, 1, 0, stream>>>(rs, ns, nst);
+    return cudaGetLastError();
+}
+
 __global__ void fill_bounds_kernel(uint32_t *pb, uint32_t count, uint32_t planes)
 {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x) pb[j] = planes;

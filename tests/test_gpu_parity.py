@@ -324,6 +324,41 @@ def test_cluster_schedule_bimolecular_vs_oracle(ctx):
     assert np.array_equal(out, ref)
 
 
+@pytest.mark.parametrize("schedule", ["phases", "fused", "cluster"])
+def test_run_native_async_refuses_bad_contents(ctx, schedule):
+    """New contents given to lmb_run_native_async are checked on the device
+    ahead of the timesteps: a species id above the model's fails the solve
+    with LMB_E_ARG before its first timestep and leaves the uploaded lattice
+    as it is, as lmb_lattice_set_native + lmb_run does; the next solve with
+    good contents runs as usual."""
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import Lattice, Model
+    spec = configs.random_problem(91, X=32, Y=16, Z=16, slots=8, bytes_per_slot=1, density=0.1, nst=3)
+    t = oracle_tables(spec)
+    sched = {"phases": L.LMB_SCHEDULE_PHASES, "fused": L.LMB_SCHEDULE_FUSED, "cluster": L.LMB_SCHEDULE_CLUSTER}
+    model = Model.from_tables(ctx, t)
+    lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
+    lat.set_schedule(sched[schedule])
+    good = np.ascontiguousarray(spec.lattice, dtype=np.uint32)
+    sites = np.ascontiguousarray(spec.sites, dtype=np.uint8)
+    bad = good.copy()
+    bad[7] = (bad[7] & ~np.uint32(0xFF)) | np.uint32(spec.ns + 5)  # slot 0 of site 7: no such species
+    out = np.zeros_like(good)
+    lat.run_native_async(model, 9, 0, 70, bad.ctypes.data, sites.ctypes.data, out.ctypes.data)
+    rc, st = lat.wait(check=False)
+    assert rc == L.LMB_E_ARG and st.steps_done == 0
+    now, _ = lat.get_native()
+    assert np.array_equal(now, bad)
+    lat.run_native_async(model, 9, 0, 70, good.ctypes.data, sites.ctypes.data, out.ctypes.data)
+    rc, _ = lat.wait(check=False)
+    assert rc == 0
+    ref, rc_ref, _ = oracle_run(t, good, sites, 9, 0, 70)
+    assert rc_ref == 0
+    assert np.array_equal(out, ref)
+    lat.close()
+    model.close()
+
+
 def test_chunked_run_equals_single_run(ctx):
     spec = configs.random_problem(8, X=32, Y=16, Z=8, density=0.7)
     t = oracle_tables(spec)
