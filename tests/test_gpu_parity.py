@@ -618,7 +618,7 @@ def test_plane_bounds_across_runs_and_edits(ctx, slots, bps):
     assert np.array_equal(out, ref)
 
 
-@pytest.mark.parametrize("schedule", SCHEDULES)
+@pytest.mark.parametrize("schedule", SCHEDULES + ["cluster"])
 @pytest.mark.parametrize("case", ["sparse", "storm", "relaxed", "zero_steps"])
 def test_run_counts_equal_separate_counts(ctx, schedule, case):
     """lmb_run_counts_async takes the species totals inside the run (the fused
@@ -639,9 +639,19 @@ def test_run_counts_equal_separate_counts(ctx, schedule, case):
     lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
     if schedule == "phases":
         lat.set_schedule(L.LMB_SCHEDULE_PHASES)
+    elif schedule == "cluster":
+        lat.set_schedule(L.LMB_SCHEDULE_CLUSTER)
     else:
         lat.set_schedule(L.LMB_SCHEDULE_FUSED)
     lat.set_native(spec.lattice, spec.sites)
+    if schedule == "cluster" and mode == L.LMB_OVERFLOW_RELAXED:
+        # The cluster-resident schedule resolves overflows the classic way only.
+        with pytest.raises(L.LmbError) as err:
+            lat.run_counts(model, 17, 0, n, spec.ns, mode, check=False)
+        assert err.value.status == L.LMB_E_UNSUPPORTED
+        lat.close()
+        model.close()
+        return
     rc, st, counts = lat.run_counts(model, 17, 0, n, spec.ns, mode, check=False)
     ref, rc_ref, _ = oracle_run(t, spec.lattice, spec.sites, 17, 0, n, mode)
     assert rc == rc_ref
