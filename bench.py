@@ -677,6 +677,7 @@ def run_batch(a):
     edge, over the same timesteps."""
     import torch
 
+    from lattice_microbes_b200 import _lib as LL
     from lattice_microbes_b200 import configs
     from lattice_microbes_b200.solver import Batch, Context, Lattice, Model, compose_seed, kernel_launches
 
@@ -773,7 +774,8 @@ def run_batch(a):
         "site_steps_per_s": sites_total / (ms_step / 1e3),
         "sequential_plain": {"value": seq_rep_per_s, "unit": "replicates/s",
                              "what": "all %d replicates, one after another, %d timesteps each" % (len(lats), T),
-                             "schedule_by_edge": {str(e): ("fused %dx%d" % (v[1], v[2]) if v[0] == 0 else "phases")
+                             "schedule_by_edge": {str(e): ("fused %dx%d" % (v[1], v[2]) if v[0] == LL.LMB_SCHEDULE_FUSED else
+                                                           "cluster" if v[0] == LL.LMB_SCHEDULE_CLUSTER else "phases")
                                                   for e, v in sched.items()}},
         "speedup_vs_sequential": rep_per_s / seq_rep_per_s,
         "gpu_launches": int(launches),
