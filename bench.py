@@ -99,7 +99,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
-    ap.add_argument("--schedule", choices=["auto", "fused", "phases", "cluster"], default="auto")
+    ap.add_argument("--schedule", choices=["auto", "fused", "phases", "cluster", "grid"], default="auto")
     ap.add_argument("--workload", choices=["crowded", "rodcell", "bimolecular", "batch", "cme", "serve", "trajectory",
                                            "pair"],
                     default=DEFAULT_WORKLOAD,
@@ -439,13 +439,17 @@ def run_ours(a):
         lat.set_schedule(LL.LMB_SCHEDULE_PHASES)
     elif a.schedule == "cluster":
         lat.set_schedule(LL.LMB_SCHEDULE_CLUSTER)
+    elif a.schedule == "grid":
+        lat.set_schedule(LL.LMB_SCHEDULE_GRID)
     elif a.schedule == "fused" or a.no_autotune:
         lat.set_schedule(LL.LMB_SCHEDULE_FUSED)
     else:
         tuned = lat.autotune(model, seed, 0, 100)
     sched = lat.schedule()
     sched_name = {LL.LMB_SCHEDULE_FUSED: "fused Ty=%d Tz=%d" % (sched[1], sched[2]),
-                  LL.LMB_SCHEDULE_CLUSTER: "cluster (whole lattice in one thread-block cluster, one launch per run)"
+                  LL.LMB_SCHEDULE_CLUSTER: "cluster (whole lattice in one thread-block cluster, one launch per run)",
+                  LL.LMB_SCHEDULE_GRID: "grid Ty=%d Tz=%d (every fused tile resident at once, one launch per run)"
+                                        % (sched[1], sched[2]),
                   }.get(sched[0], "phases")
 
     step = 0
@@ -498,6 +502,8 @@ def run_ours(a):
     if phase_n[5] > 0:
         kern = ("cluster_run_kernel (every timestep of the run in one launch; per timestep)"
                 if sched[0] == LL.LMB_SCHEDULE_CLUSTER else
+                "fused_grid_kernel (every timestep of the run in one launch; per timestep)"
+                if sched[0] == LL.LMB_SCHEDULE_GRID else
                 "fused_step_kernel (x, y, z sweeps + reaction + overflow, one timestep)")
         launch_ms = phases["fused_step"]["ms_per_launch"]
         alg_bytes = N * B_STEP                 # site-steps per launch x per-site-step bytes
@@ -775,7 +781,9 @@ def run_batch(a):
         "sequential_plain": {"value": seq_rep_per_s, "unit": "replicates/s",
                              "what": "all %d replicates, one after another, %d timesteps each" % (len(lats), T),
                              "schedule_by_edge": {str(e): ("fused %dx%d" % (v[1], v[2]) if v[0] == LL.LMB_SCHEDULE_FUSED else
-                                                           "cluster" if v[0] == LL.LMB_SCHEDULE_CLUSTER else "phases")
+                                                           "cluster" if v[0] == LL.LMB_SCHEDULE_CLUSTER else
+                                                           "grid %dx%d" % (v[1], v[2]) if v[0] == LL.LMB_SCHEDULE_GRID
+                                                           else "phases")
                                                   for e, v in sched.items()}},
         "speedup_vs_sequential": rep_per_s / seq_rep_per_s,
         "gpu_launches": int(launches),

@@ -45,12 +45,19 @@ extern "C" {
  * PHASES launches one kernel per sweep, the reaction and the overflow pass
  * (the reference's schedule, MpdRdmeSolver.cu:1011-1090); CLUSTER, for small
  * lattices, holds the whole lattice in the shared memory of one thread-block
- * cluster and runs every timestep of a run in one launch (classic overflow
- * handling only; lmb_lattice_set_schedule refuses a lattice that does not
- * fit with LMB_E_UNSUPPORTED).  All give the same lattice bit for bit. */
+ * cluster and runs every timestep of a run in one launch; GRID runs the
+ * FUSED tiles of a Ty x Tz plan (0, 0 = the least-halo plan that fits) all
+ * resident at once, one cooperative launch per run: each block keeps its
+ * region in shared memory from one timestep to the next and reloads only its
+ * halo rows, which the neighbouring blocks store, after a bounded grid
+ * barrier (a wait that gives up ends the run with LMB_E_TIMEOUT).  CLUSTER
+ * and GRID: classic overflow handling only; lmb_lattice_set_schedule refuses
+ * a lattice (or plan) that does not fit with LMB_E_UNSUPPORTED.  All give
+ * the same lattice bit for bit. */
 #define LMB_SCHEDULE_FUSED 0
 #define LMB_SCHEDULE_PHASES 1
 #define LMB_SCHEDULE_CLUSTER 2
+#define LMB_SCHEDULE_GRID 3
 
 /* Reaction types (CMESolver.h:79-112). */
 #define LMB_REACTION_ZEROTH 0
@@ -174,8 +181,9 @@ int lmb_lattice_set_row_major(lmb_lattice *lattice, const void *particles, const
                               uint32_t number_species, uint32_t number_site_types);
 int lmb_lattice_get_row_major(lmb_lattice *lattice, void *particles, uint8_t *sites);
 /* Timestep schedule of this lattice: LMB_SCHEDULE_FUSED with tile Ty x Tz
- * (0, 0 = default plan), LMB_SCHEDULE_PHASES or LMB_SCHEDULE_CLUSTER (Ty, Tz
- * unused).  The reference has fixed block sizes instead
+ * (0, 0 = default plan), LMB_SCHEDULE_GRID with tile Ty x Tz (0, 0 = the
+ * least-halo plan whose tiles fit on the device at once),
+ * LMB_SCHEDULE_PHASES or LMB_SCHEDULE_CLUSTER (Ty, Tz unused).  The reference has fixed block sizes instead
  * (options.cmake:89-95). */
 int lmb_lattice_set_schedule(lmb_lattice *lattice, int schedule, uint32_t Ty, uint32_t Tz);
 int lmb_lattice_get_schedule(lmb_lattice *lattice, int *schedule, uint32_t *Ty, uint32_t *Tz);

@@ -29,6 +29,7 @@ LMB_NOALLOC_MAX_SPECIES = 4095
 LMB_SCHEDULE_FUSED = 0
 LMB_SCHEDULE_PHASES = 1
 LMB_SCHEDULE_CLUSTER = 2
+LMB_SCHEDULE_GRID = 3
 LMB_CME_KERNEL_AUTO = 0
 LMB_CME_KERNEL_GENERIC = 1
 

@@ -115,6 +115,24 @@ static int cuda_status(cudaError_t e)
     return LMB_E_CUDA;
 }
 
+// Schedules that hold the lattice in shared memory and run every timestep of
+// a run in one launch.
+static bool resident_schedule(int schedule)
+{
+    return schedule == LMB_SCHEDULE_CLUSTER || schedule == LMB_SCHEDULE_GRID;
+}
+
+// The one launch of a run on a resident schedule, from the current buffer.
+static cudaError_t launch_resident(lmb_lattice *l, const lmb_model *m, cudaStream_t stream)
+{
+    uint32_t *a = l->buf[l->cur], *b = l->buf[l->cur ^ 1];
+    if (l->schedule == LMB_SCHEDULE_GRID)
+        return launch_fused_grid((int)l->bps, (int)l->slots, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap,
+                                 l->tile, m->nr > 0, stream);
+    return launch_cluster_run((int)l->bps, (int)l->slots, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap,
+                              stream);
+}
+
 extern "C" int lmb_abi_version(void) { return LMB_ABI_VERSION; }
 
 extern "C" const char *lmb_status_string(int s)
@@ -657,6 +675,19 @@ extern "C" int lmb_lattice_set_schedule(lmb_lattice *l, int schedule, uint32_t T
         l->schedule = schedule;
         return LMB_OK;
     }
+    if (schedule == LMB_SCHEDULE_GRID) {
+        // Every tile resident at once, checked with the largest staged tables (8 KiB).
+        CK(cudaSetDevice(l->ctx->device));
+        TileShape t;
+        const bool ok = (Ty == 0 && Tz == 0)
+                            ? fused_grid_default_shape(l->g, (int)l->bps, (int)l->slots, l->cap, 8 * 1024, t)
+                            : fused_make_shape(l->g, (int)l->bps, (int)l->slots, Ty, Tz, t) &&
+                                  fused_grid_fits(l->g, (int)l->bps, (int)l->slots, l->cap, 8 * 1024, t);
+        if (!ok) return LMB_E_UNSUPPORTED;
+        l->tile = t;
+        l->schedule = schedule;
+        return LMB_OK;
+    }
     if (schedule != LMB_SCHEDULE_FUSED) return LMB_E_ARG;
     TileShape t;
     bool ok = (Ty == 0 && Tz == 0) ? fused_default_shape(l->g, (int)l->bps, (int)l->slots, t)
@@ -671,8 +702,9 @@ extern "C" int lmb_lattice_get_schedule(lmb_lattice *l, int *schedule, uint32_t 
 {
     if (!l) return LMB_E_ARG;
     if (schedule) *schedule = l->schedule;
-    if (Ty) *Ty = l->schedule == LMB_SCHEDULE_FUSED ? l->tile.Ty : 0;
-    if (Tz) *Tz = l->schedule == LMB_SCHEDULE_FUSED ? l->tile.Tz : 0;
+    const bool tiled = l->schedule == LMB_SCHEDULE_FUSED || l->schedule == LMB_SCHEDULE_GRID;
+    if (Ty) *Ty = tiled ? l->tile.Ty : 0;
+    if (Tz) *Tz = tiled ? l->tile.Tz : 0;
     return LMB_OK;
 }
 
@@ -999,8 +1031,8 @@ static int run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_
         }
         CK(cudaMemsetAsync(l->counts_dev, 0, sizeof(unsigned long long) * (count_ns + 1), c->stream));
     }
-    // The cluster-resident schedule resolves overflows the classic way only.
-    if (l->schedule == LMB_SCHEDULE_CLUSTER && mode != LMB_OVERFLOW_CLASSIC) return LMB_E_UNSUPPORTED;
+    // The shared-memory-resident schedules resolve overflows the classic way only.
+    if (resident_schedule(l->schedule) && mode != LMB_OVERFLOW_CLASSIC) return LMB_E_UNSUPPORTED;
     CK(launch_begin_run(l->rs, seed, first, n, (uint32_t)mode, c->stream, in_kernel ? first + n - 1 : ~0u, count_ns,
                         l->counts_dev));
     if (device_check) {
@@ -1011,10 +1043,9 @@ static int run_async(lmb_lattice *l, const lmb_model *mc, uint32_t seed, uint32_
     l->pending_cur0 = l->cur;
     l->pending_check = device_check;
     uint32_t done = 0;
-    if (l->schedule == LMB_SCHEDULE_CLUSTER && n > 0) {
+    if (resident_schedule(l->schedule) && n > 0) {
         // Every timestep in one launch, ending in the buffer n's parity gives.
-        CK(launch_cluster_run((int)l->bps, (int)l->slots, l->buf[l->cur], l->buf[l->cur ^ 1], l->sites, l->g,
-                              m->dev, l->rs, l->list, l->cap, c->stream));
+        CK(launch_resident(l, m, c->stream));
         l->cur ^= (int)(n & 1u);
         done = n;
     }
@@ -1159,7 +1190,7 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
     for (auto &e : ev) CK(cudaEventCreate(&e));
     const int bps = (int)l->bps, S = (int)l->slots;
     const int cur0 = l->cur;
-    const bool cluster = l->schedule == LMB_SCHEDULE_CLUSTER;
+    const bool cluster = resident_schedule(l->schedule);
     const bool fused = l->schedule == LMB_SCHEDULE_FUSED || cluster;
     if (cluster && mode != LMB_OVERFLOW_CLASSIC) return LMB_E_UNSUPPORTED;
     for (uint32_t s = 0; s < n; s++) {
@@ -1170,7 +1201,7 @@ extern "C" int lmb_run_profiled(lmb_lattice *l, const lmb_model *mc, uint32_t se
             // fused-timestep entry, one launch per timestep.
             CK(cudaEventRecord(E[10], c->stream));
             if (s == 0) {
-                CK(launch_cluster_run(bps, S, a, b, l->sites, l->g, m->dev, l->rs, l->list, l->cap, c->stream));
+                CK(launch_resident(l, m, c->stream));
                 l->cur ^= (int)(n & 1u);
             }
             CK(cudaEventRecord(E[11], c->stream));
@@ -1274,6 +1305,9 @@ extern "C" int lmb_lattice_autotune(lmb_lattice *l, const lmb_model *m, uint32_t
             TileShape t;
             if (fused_make_shape(l->g, (int)l->bps, (int)l->slots, ty, tz, t)) cands.push_back({LMB_SCHEDULE_FUSED, ty, tz});
         }
+    // LMB_SCHEDULE_GRID is not a candidate: on one lattice it times as its
+    // fused plan does, and its cooperative launch cannot overlap another
+    // lattice's run on a second stream, as fused launches do.
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1288,7 +1322,7 @@ extern "C" int lmb_lattice_autotune(lmb_lattice *l, const lmb_model *m, uint32_t
             cudaMemcpyAsync(l->buf[l->cur], save, wbytes, cudaMemcpyDeviceToDevice, c->stream);
             cudaEventRecord(e0, c->stream);
             rc = lmb_run_async(l, m, seed, first, timesteps, LMB_OVERFLOW_CLASSIC);
-            if (rc != LMB_OK && cd.sched == LMB_SCHEDULE_CLUSTER && rc == LMB_E_CUDA) {
+            if (rc != LMB_OK && resident_schedule(cd.sched) && rc == LMB_E_CUDA) {
                 // A cluster the device would not launch: not a candidate.
                 cudaGetLastError();
                 rc = LMB_OK;

@@ -1136,4 +1136,250 @@ cudaError_t launch_cluster_run(int bps, int slots, uint32_t *buf0, uint32_t *buf
     return cudaErrorInvalidValue;
 }
 
+
+// ---------------------------------------------------------------------------
+// Grid-resident fused tiles: every tile of a fused plan resident at once
+// ---------------------------------------------------------------------------
+//
+// When the plan's tiles fit on the device together (a cooperative launch of
+// one block per tile), one launch runs every timestep of a run.  A block
+// keeps its region in shared memory from one timestep to the next: after
+// tile_timestep it stores its owned rows into the global buffer of that
+// timestep (buf1, buf0, buf1, ... : the buffers alternate as they do between
+// fused launches), and after a grid barrier it reloads only its halo rows
+// from there, which the neighbouring tiles stored.  The site types and the
+// staged model tables are loaded once per run.
+//
+// Overflows: a block that queued one sees the queue count non-zero after its
+// own timestep (its atomics precede that read), and raises the timestep's flag
+// (RunState::grid_full, by timestep index modulo 3) before the barrier; after
+// it every block reads the same flag.  When it is up, block 0 resolves the
+// queue in the timestep's buffer (which then holds the whole lattice), and
+// after a second barrier every block reloads its whole region.  Block 0 clears
+// the flag of timestep + 2 after the barrier of timestep: every block read
+// that flag (as timestep - 1's) before this barrier, and raises it only after
+// the next one, which block 0 reaches after the clearing store.
+//
+// Hazards on the buffers: a buffer is written at timestep k + 2 only after the
+// barrier of timestep k + 1, which every block reaches after its halo reads of
+// timestep k; the input (buf0) is first written at the second timestep, after
+// every block has loaded its region.  So a run gives, bit for bit, what the
+// same number of fused launches gives.
+//
+// The barrier (grid_barrier) is bounded: a wait that gives up sets
+// LMB_E_TIMEOUT and ends the block; the others give up at their next barrier.
+constexpr uint32_t GRID_SPIN_LIMIT = 1u << 22;
+
+// Grid barrier of a cooperative launch.  Each block adds one arrival to `bar`
+// (zeroed before the launch) and waits, in thread 0, until the count reaches
+// `target` = (barriers passed + 1) x blocks.  False when the wait gave up.
+__device__ __forceinline__ bool grid_barrier(unsigned long long *bar, unsigned long long target)
+{
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1ull);
+        uint32_t ok = 0;
+        for (uint32_t it = 0; it < GRID_SPIN_LIMIT; it++) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+            if (v >= target) {
+                ok = 1;
+                break;
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <int BPS, int S>
+__global__ void __launch_bounds__(FUSED_THREADS, 2)
+    fused_grid_kernel(uint32_t *__restrict__ buf0, uint32_t *__restrict__ buf1, const uint8_t *__restrict__ sites,
+                      Geometry g, const __grid_constant__ DevTables m, RunState *__restrict__ rs,
+                      OverflowEntry *__restrict__ list, uint32_t cap, const __grid_constant__ TileShape ts,
+                      int with_reaction)
+{
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ uint32_t s_cnt[4];
+    __shared__ uint32_t rowbase[FUSED_MAX_ROWS];
+    __shared__ uint16_t yrow[FUSED_MAX_ROWS], zrow[FUSED_MAX_ROWS];
+    __shared__ uint8_t rowflag[FUSED_MAX_ROWS];
+    __shared__ uint32_t s_go;
+    __shared__ DevTables s_mt;
+    const int32_t status = rs->status;
+    const uint32_t seed = rs->seed, first = rs->step, end = rs->end_step;
+    const uint32_t tid = threadIdx.x, nthr = blockDim.x, nblocks = gridDim.x;
+    const TileSmem t = tile_smem<BPS, S>(smem, ts, rowbase, yrow, zrow, rowflag, s_cnt);
+    {
+        const DevTables staged = m.stage_bytes ? stage_tables(m, t.tables, tid, nthr) : m;
+        if (tid == 0) s_mt = staged;
+    }
+    tile_rows(g, ts, blockIdx.x, t);
+    __syncthreads();
+    tile_load<BPS, S, true>(buf0, sites, g, ts, t, t.A, t.occA, false, true);
+    if (status != LMB_OK || first >= end) return;  // the same for every block
+
+    uint32_t *src_w = t.A, *dst_w = t.B, *src_o = t.occA, *dst_o = t.occB;
+    unsigned long long passed = 0;  // arrivals the barriers passed so far have counted
+    uint32_t k = 0;
+    for (uint32_t step = first; step < end; step++, k++) {
+        tile_timestep<BPS, S, true>(g, s_mt, rs, list, cap, ts, t, src_w, dst_w, src_o, dst_o, seed, step,
+                                    with_reaction);
+        uint32_t *out = (k & 1u) ? buf0 : buf1;
+        tile_store<BPS, S>(out, g, ts, t, src_w, src_o);
+        // tile_timestep ended with a block barrier: this block's overflows
+        // are in the queue count.
+        if (tid == 0 && __ldcg(&rs->ovf_count) != 0) atomicOr(&rs->grid_full[step % 3u], 1u);
+        passed += nblocks;
+        if (!grid_barrier(&rs->grid_bar, passed)) {
+            if (tid == 0) atomicCAS(&rs->status, (int32_t)LMB_OK, (int32_t)LMB_E_TIMEOUT);
+            return;
+        }
+        if (tid == 0) {
+            s_go = __ldcg(&rs->grid_full[step % 3u]);
+            if (blockIdx.x == 0) rs->grid_full[(step + 2u) % 3u] = 0;
+        }
+        __syncthreads();
+        if (s_go) {
+            // Overflows are queued: block 0 resolves them in `out`, as the
+            // last block of a fused launch does, then every block reloads.
+            if (blockIdx.x == 0) {
+                if (tid == 0) rs->step = step;
+                __syncthreads();
+                resolve_block_flat<BPS, S>(out, sites, g, rs, list, cap, (OverflowEntry *)smem, tid, nthr, nullptr);
+                __threadfence();
+            }
+            passed += nblocks;
+            if (!grid_barrier(&rs->grid_bar, passed)) {
+                if (tid == 0) atomicCAS(&rs->status, (int32_t)LMB_OK, (int32_t)LMB_E_TIMEOUT);
+                return;
+            }
+            if (*(volatile int32_t *)&rs->status != LMB_OK) return;  // the partial lattice is in `out`
+            // Block 0's sort area covered its whole dynamic shared memory:
+            // the staged tables (same place, same contents) and the site
+            // types come back with the region.
+            if (blockIdx.x == 0 && m.stage_bytes) stage_tables(m, t.tables, tid, nthr);
+            tile_load<BPS, S, true>(out, sites, g, ts, t, src_w, src_o, false, blockIdx.x == 0);
+        } else {
+            tile_load<BPS, S, true>(out, sites, g, ts, t, src_w, src_o, true, false);
+        }
+    }
+    if (blockIdx.x == 0 && tid == 0) set_step(rs, seed, end);
+}
+
+// Blocks of fused_grid_kernel with `smem` bytes an SM holds at once (0 when
+// the kernel's attributes cannot be set).
+template <int BPS, int S>
+static uint32_t grid_blocks_per_sm(size_t smem)
+{
+    if (cudaFuncSetAttribute(fused_grid_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_grid_kernel<BPS, S>, FUSED_THREADS, smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (uint32_t)per_sm;
+}
+
+#define GRID_DISPATCH(BPS_, S_, ...) \
+    if (bps == BPS_ && slots == S_) { \
+        __VA_ARGS__;                  \
+    }
+
+static uint32_t grid_capacity(int bps, int slots, size_t smem)
+{
+    int dev = 0, sms = 0, coop = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) {
+        cudaGetLastError();
+        return 0;
+    }
+    uint32_t per_sm = 0;
+    GRID_DISPATCH(1, 4, per_sm = grid_blocks_per_sm<1, 4>(smem))
+    GRID_DISPATCH(1, 8, per_sm = grid_blocks_per_sm<1, 8>(smem))
+    GRID_DISPATCH(1, 16, per_sm = grid_blocks_per_sm<1, 16>(smem))
+    GRID_DISPATCH(4, 4, per_sm = grid_blocks_per_sm<4, 4>(smem))
+    GRID_DISPATCH(4, 8, per_sm = grid_blocks_per_sm<4, 8>(smem))
+    GRID_DISPATCH(4, 16, per_sm = grid_blocks_per_sm<4, 16>(smem))
+    return per_sm * (uint32_t)sms;
+}
+
+bool fused_grid_fits(const Geometry &g, int bps, int slots, uint32_t cap, uint32_t stage_bytes, const TileShape &ts)
+{
+    const uint32_t W = bps == 1 ? slots / 4 : slots;
+    const size_t smem = fused_smem_bytes(ts, g.X, W, cap, stage_bytes);
+    if (smem > FUSED_MAX_SMEM) return false;
+    return ts.tiles_y * ts.tiles_z <= grid_capacity(bps, slots, smem);
+}
+
+bool fused_grid_default_shape(const Geometry &g, int bps, int slots, uint32_t cap, uint32_t stage_bytes,
+                              TileShape &ts)
+{
+    // The least halo overhead among the shapes whose tiles fit together.
+    const uint32_t cands[] = {1, 2, 4, 8, 16};
+    bool found = false;
+    double best = 1e30;
+    for (uint32_t Ty : cands)
+        for (uint32_t Tz : cands) {
+            TileShape t;
+            if (!fused_make_shape(g, bps, slots, Ty, Tz, t) || !fused_grid_fits(g, bps, slots, cap, stage_bytes, t))
+                continue;
+            const double halo = (double)(Ty + 2) * (Tz + 2) / ((double)Ty * Tz);
+            if (halo < best) {
+                best = halo;
+                ts = t;
+                found = true;
+            }
+        }
+    return found;
+}
+
+template <int BPS, int S>
+static cudaError_t fused_grid_launch_t(uint32_t *buf0, uint32_t *buf1, const uint8_t *sites, const Geometry &g,
+                                       const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
+                                       const TileShape &ts, int with_reaction, size_t smem, cudaStream_t stream)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ts.tiles_y * ts.tiles_z);
+    cfg.blockDim = dim3(FUSED_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // every block resident at once, or no launch
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    count_launch();
+    return cudaLaunchKernelEx(&cfg, fused_grid_kernel<BPS, S>, buf0, buf1, sites, g, m, rs, list, cap, ts,
+                              with_reaction);
+}
+
+cudaError_t launch_fused_grid(int bps, int slots, uint32_t *buf0, uint32_t *buf1, const uint8_t *sites,
+                              const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
+                              const TileShape &ts, int with_reaction, cudaStream_t stream)
+{
+    if (!fused_grid_fits(g, bps, slots, cap, m.stage_bytes, ts)) return cudaErrorInvalidConfiguration;
+    const uint32_t W = bps == 1 ? slots / 4 : slots;
+    const size_t smem = fused_smem_bytes(ts, g.X, W, cap, m.stage_bytes);
+    // The barrier count and the three overflow flags, contiguous in the run state.
+    cudaError_t e = cudaMemsetAsync(&rs->grid_bar, 0, sizeof(unsigned long long) + 3 * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    GRID_DISPATCH(1, 4, return fused_grid_launch_t<1, 4>(buf0, buf1, sites, g, m, rs, list, cap, ts, with_reaction, smem, stream))
+    GRID_DISPATCH(1, 8, return fused_grid_launch_t<1, 8>(buf0, buf1, sites, g, m, rs, list, cap, ts, with_reaction, smem, stream))
+    GRID_DISPATCH(1, 16, return fused_grid_launch_t<1, 16>(buf0, buf1, sites, g, m, rs, list, cap, ts, with_reaction, smem, stream))
+    GRID_DISPATCH(4, 4, return fused_grid_launch_t<4, 4>(buf0, buf1, sites, g, m, rs, list, cap, ts, with_reaction, smem, stream))
+    GRID_DISPATCH(4, 8, return fused_grid_launch_t<4, 8>(buf0, buf1, sites, g, m, rs, list, cap, ts, with_reaction, smem, stream))
+    GRID_DISPATCH(4, 16, return fused_grid_launch_t<4, 16>(buf0, buf1, sites, g, m, rs, list, cap, ts, with_reaction, smem, stream))
+    return cudaErrorInvalidValue;
+}
+
 }  // namespace lmb

@@ -68,4 +68,22 @@ cudaError_t launch_cluster_run(int bytes_per_slot, int slots, uint32_t *buf0, ui
                                const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
                                cudaStream_t stream);
 
+// Grid-resident fused tiles (lmb_fused.cu): the tiles of a fused plan held
+// in shared memory by a cooperative launch of one block per tile, every
+// timestep of a run in one launch; halo rows exchanged through the two
+// buffers (which alternate as between fused launches), a bounded grid barrier
+// per timestep (LMB_E_TIMEOUT in the run state when a wait gives up).  The
+// run starts from buf0 and ends in buf0 or buf1 by the parity of its timestep
+// count (of the failing timestep + 1 when it fails).  fused_grid_fits: the
+// plan's tiles fit on the current device at once (it sets the kernel's
+// shared-memory attribute); fused_grid_default_shape: the least-halo shape
+// that does.
+bool fused_grid_fits(const Geometry &g, int bytes_per_slot, int slots, uint32_t cap, uint32_t stage_bytes,
+                     const TileShape &ts);
+bool fused_grid_default_shape(const Geometry &g, int bytes_per_slot, int slots, uint32_t cap, uint32_t stage_bytes,
+                              TileShape &ts);
+cudaError_t launch_fused_grid(int bytes_per_slot, int slots, uint32_t *buf0, uint32_t *buf1, const uint8_t *sites,
+                              const Geometry &g, const DevTables &m, RunState *rs, OverflowEntry *list, uint32_t cap,
+                              const TileShape &ts, int with_reaction, cudaStream_t stream);
+
 }  // namespace lmb

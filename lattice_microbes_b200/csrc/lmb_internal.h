@@ -100,6 +100,11 @@ struct RunState {
     uint32_t count_step;
     uint32_t count_ns;
     unsigned long long *counts;
+    // Grid-resident schedule, zeroed before each of its launches: the
+    // arrivals at the grid barrier so far, and the "an overflow was queued"
+    // flags of the timesteps, by timestep index modulo 3.
+    unsigned long long grid_bar;
+    uint32_t grid_full[3];
 };
 
 

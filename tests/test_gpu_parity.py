@@ -38,6 +38,8 @@ def _gpu_run(ctx, tables_or_spec, lattice, sites, seed, step0, nsteps, mode=0, f
         lat.set_schedule(L.LMB_SCHEDULE_PHASES)
     elif schedule == "cluster":
         lat.set_schedule(L.LMB_SCHEDULE_CLUSTER)
+    elif schedule == "grid":
+        lat.set_schedule(L.LMB_SCHEDULE_GRID, *tile)
     else:
         lat.set_schedule(L.LMB_SCHEDULE_FUSED, *tile)
     lat.set_native(lattice, sites)
@@ -324,7 +326,68 @@ def test_cluster_schedule_bimolecular_vs_oracle(ctx):
     assert np.array_equal(out, ref)
 
 
-@pytest.mark.parametrize("schedule", ["phases", "fused", "cluster"])
+@pytest.mark.parametrize("shape,slots,bps,per_slot,nsteps,tile", [
+    ((32, 32, 32), 8, 1, 0.01, 40, (0, 0)),    # the default plan: least halo among shapes that fit at once
+    ((16, 16, 16), 4, 1, 0.2, 40, (1, 1)),     # 256 tiles of one row
+    ((24, 20, 48), 16, 1, 0.05, 30, (4, 2)),   # rows not 16-byte aligned
+    ((32, 16, 32), 4, 4, 0.15, 30, (2, 4)),    # IntLattice
+    ((32, 8, 16), 8, 1, 0.5, 20, (2, 2)),      # dense: overflows resolved in global memory most timesteps
+    ((32, 8, 12), 8, 1, 0.9, 10, (4, 2)),      # denser still: the run may fail as the oracle's does
+    ((64, 64, 128), 8, 1, 0.01, 12, (4, 8)),   # 256 tiles, two per SM
+])
+def test_grid_schedule_vs_oracle(ctx, shape, slots, bps, per_slot, nsteps, tile):
+    """The grid-resident schedule (every tile of a fused plan held in shared
+    memory by one cooperative launch, halo rows exchanged through global
+    memory, every timestep of the run in one launch) against the oracle: the
+    same status, statistics and lattice, including overflow resolutions and
+    runs that stop at a failed resolution."""
+    X, Y, Z = shape
+    spec = configs.random_problem(83, X=X, Y=Y, Z=Z, slots=slots, bytes_per_slot=bps, density=per_slot * slots,
+                                  nst=3)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 37, 5, nsteps)
+    out, rc, st = _gpu_run(ctx, t, spec.lattice, spec.sites, 37, 5, nsteps, schedule="grid", tile=tile,
+                           chunks=[nsteps // 2, nsteps - nsteps // 2])
+    assert rc == rc_ref
+    if rc == 0:
+        assert sum(x.overflows for x in st) == st_ref.overflows
+        assert sum(x.reactions for x in st) == st_ref.reactions
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("tile", [(4, 8), (8, 4), (2, 16)])
+def test_grid_schedule_rodcell_vs_oracle(ctx, tile):
+    """The 64x64x128 rod cell (membrane, cytoplasm and nucleoid site types,
+    membrane-only reactions) on the grid-resident schedule, 24 timesteps in
+    two runs, against the oracle."""
+    spec = configs.config1(seed=2)
+    t = oracle_tables(spec)
+    ref, rc_ref, st_ref = oracle_run(t, spec.lattice, spec.sites, 31, 0, 24)
+    out, rc, st = _gpu_run(ctx, spec, spec.lattice, spec.sites, 31, 0, 24, from_spec=True, schedule="grid",
+                           tile=tile, chunks=[11, 13])
+    assert rc == rc_ref == 0
+    assert sum(x.reactions for x in st) == st_ref.reactions
+    assert np.array_equal(out, ref)
+
+
+def test_grid_schedule_refuses_what_does_not_fit(ctx):
+    """A lattice none of whose tile plans fit on the device at once is
+    refused with LMB_E_UNSUPPORTED, and the lattice keeps its schedule."""
+    from lattice_microbes_b200 import _lib as L
+    from lattice_microbes_b200.solver import Lattice
+    lat = Lattice(ctx, 256, 256, 64, 16, 4)
+    before = lat.schedule()
+    with pytest.raises(L.LmbError) as err:
+        lat.set_schedule(L.LMB_SCHEDULE_GRID)
+    assert err.value.status == L.LMB_E_UNSUPPORTED
+    with pytest.raises(L.LmbError) as err:
+        lat.set_schedule(L.LMB_SCHEDULE_GRID, 1, 1)
+    assert err.value.status == L.LMB_E_UNSUPPORTED
+    assert lat.schedule() == before
+    lat.close()
+
+
+@pytest.mark.parametrize("schedule", ["phases", "fused", "cluster", "grid"])
 def test_run_native_async_refuses_bad_contents(ctx, schedule):
     """New contents given to lmb_run_native_async are checked on the device
     ahead of the timesteps: a species id above the model's fails the solve
@@ -335,7 +398,8 @@ def test_run_native_async_refuses_bad_contents(ctx, schedule):
     from lattice_microbes_b200.solver import Lattice, Model
     spec = configs.random_problem(91, X=32, Y=16, Z=16, slots=8, bytes_per_slot=1, density=0.1, nst=3)
     t = oracle_tables(spec)
-    sched = {"phases": L.LMB_SCHEDULE_PHASES, "fused": L.LMB_SCHEDULE_FUSED, "cluster": L.LMB_SCHEDULE_CLUSTER}
+    sched = {"phases": L.LMB_SCHEDULE_PHASES, "fused": L.LMB_SCHEDULE_FUSED, "cluster": L.LMB_SCHEDULE_CLUSTER,
+             "grid": L.LMB_SCHEDULE_GRID}
     model = Model.from_tables(ctx, t)
     lat = Lattice(ctx, t.X, t.Y, t.Z, t.slots, t.bytes_per_slot)
     lat.set_schedule(sched[schedule])
@@ -618,7 +682,7 @@ def test_plane_bounds_across_runs_and_edits(ctx, slots, bps):
     assert np.array_equal(out, ref)
 
 
-@pytest.mark.parametrize("schedule", SCHEDULES + ["cluster"])
+@pytest.mark.parametrize("schedule", SCHEDULES + ["cluster", "grid"])
 @pytest.mark.parametrize("case", ["sparse", "storm", "relaxed", "zero_steps"])
 def test_run_counts_equal_separate_counts(ctx, schedule, case):
     """lmb_run_counts_async takes the species totals inside the run (the fused
@@ -641,11 +705,13 @@ def test_run_counts_equal_separate_counts(ctx, schedule, case):
         lat.set_schedule(L.LMB_SCHEDULE_PHASES)
     elif schedule == "cluster":
         lat.set_schedule(L.LMB_SCHEDULE_CLUSTER)
+    elif schedule == "grid":
+        lat.set_schedule(L.LMB_SCHEDULE_GRID)
     else:
         lat.set_schedule(L.LMB_SCHEDULE_FUSED)
     lat.set_native(spec.lattice, spec.sites)
-    if schedule == "cluster" and mode == L.LMB_OVERFLOW_RELAXED:
-        # The cluster-resident schedule resolves overflows the classic way only.
+    if schedule in ("cluster", "grid") and mode == L.LMB_OVERFLOW_RELAXED:
+        # The shared-memory-resident schedules resolve overflows the classic way only.
         with pytest.raises(L.LmbError) as err:
             lat.run_counts(model, 17, 0, n, spec.ns, mode, check=False)
         assert err.value.status == L.LMB_E_UNSUPPORTED
