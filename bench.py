@@ -99,6 +99,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference kernels on the GPU (e.g. under a profiler)")
+    ap.add_argument("--e2e-depth", type=int, default=3,
+                    help="solves in flight in the end-to-end measurement (lattices it rotates over)")
     ap.add_argument("--schedule", choices=["auto", "fused", "phases", "cluster", "grid"], default="auto")
     ap.add_argument("--workload", choices=["crowded", "rodcell", "bimolecular", "batch", "cme", "serve", "trajectory",
                                            "pair"],
@@ -521,37 +523,44 @@ def run_ours(a):
     # ---- end to end through the public API with host buffers ----
     # Every step is one solve: its input lattice and site types copied from
     # pinned host memory, T timesteps, the final lattice copied back into
-    # pinned host memory (lmb_run_native_async).  The solves alternate
-    # between two lattices on two contexts (streams), each step's solve
-    # queued while the one before runs, so that one solve's copies overlap
-    # the other's timesteps; the clock runs from the first call to the last
-    # solve's end (wall clock).
+    # pinned host memory (lmb_run_native_async).  The solves rotate over
+    # `depth` lattices on as many contexts (streams), each step's solve
+    # queued while the ones before run, so that the copies of some solves
+    # overlap the timesteps of others (a lattice's own upload waits for its
+    # previous download on its stream); the clock runs from the first call
+    # to the last solve's end (wall clock).
+    depth = max(1, a.e2e_depth)
     words = spec.words * N
     h_lat = torch.from_numpy(spec.lattice.copy()).pin_memory()
     h_sites = torch.from_numpy(spec.sites.copy()).pin_memory()
-    h_out = [torch.empty(words, dtype=torch.int32).pin_memory() for _ in range(2)]
-    ctx2 = Context(device)
-    lat2 = Lattice(ctx2, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
-    lat2.set_schedule(*sched)
-    lat2.set_native(spec.lattice, spec.sites)
-    pair = [lat, lat2]
-    for k in range(2):  # graphs captured and buffers touched before the clock starts
-        pair[k].run_native_async(model, seed, 0, T, h_lat.data_ptr(), h_sites.data_ptr(), h_out[k].data_ptr())
-        pair[k].wait()
+    h_out = [torch.empty(words, dtype=torch.int32).pin_memory() for _ in range(depth)]
+    extra = []
+    ring = [lat]
+    for _ in range(depth - 1):
+        c_ = Context(device)
+        l_ = Lattice(c_, spec.X, spec.Y, spec.Z, spec.slots, spec.bytes_per_slot)
+        l_.set_schedule(*sched)
+        l_.set_native(spec.lattice, spec.sites)
+        extra.append((c_, l_))
+        ring.append(l_)
+    for k in range(depth):  # graphs captured and buffers touched before the clock starts
+        ring[k].run_native_async(model, seed, 0, T, h_lat.data_ptr(), h_sites.data_ptr(), h_out[k].data_ptr())
+        ring[k].wait()
     torch.cuda.synchronize(device)
     ranks.barrier()
     t0 = time.perf_counter()
     for k in range(a.steps):
-        if k >= 2:
-            pair[k % 2].wait()
-        pair[k % 2].run_native_async(model, seed, 0, T, h_lat.data_ptr(), h_sites.data_ptr(),
-                                     h_out[k % 2].data_ptr())
-    for k in range(min(2, a.steps)):
-        pair[(a.steps - 1 - k) % 2].wait()
+        if k >= depth:
+            ring[k % depth].wait()
+        ring[k % depth].run_native_async(model, seed, 0, T, h_lat.data_ptr(), h_sites.data_ptr(),
+                                         h_out[k % depth].data_ptr())
+    for k in range(min(depth, a.steps)):
+        ring[(a.steps - 1 - k) % depth].wait()
     e2e_total = ranks.max((time.perf_counter() - t0) * 1e3, device)
     e2e_value = aggregate_rate(N * T * a.steps, e2e_total, world)
-    lat2.close()
-    ctx2.close()
+    for c_, l_ in extra:
+        l_.close()
+        c_.close()
 
     if rank == 0:
         line = {
@@ -611,8 +620,9 @@ def run_ours(a):
                 "d2h_bytes_per_step": int(words * 4),
                 "what": "one solve per step through lmb_run_native_async (input lattice and site types from "
                         "pinned host memory, %d timesteps, final lattice to pinned host memory), solves "
-                        "alternating between two lattices on two streams so that copies overlap timesteps; "
-                        "wall clock" % T,
+                        "rotating over %d lattices on as many streams so that copies overlap timesteps; "
+                        "wall clock" % (T, depth),
+                "solves_in_flight": depth,
             },
             "gpu_launches": int(launches),
             "clocks": clock_info,
