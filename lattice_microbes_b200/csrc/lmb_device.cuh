@@ -25,6 +25,48 @@ __device__ __forceinline__ void chain_enter()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// Grid barrier of a cooperative launch (all blocks resident at once).  Each
+// block adds one arrival to `bar` (zeroed before the launch) and waits, in
+// thread 0, until the count reaches `target` = (barriers passed + 1) x
+// blocks.  The wait is bounded: it gives up after GRID_WAIT_NS of
+// %globaltimer time (or GRID_SPIN_LIMIT polls, whichever comes first) and
+// returns false, so a block that never arrives ends the run with an error
+// status instead of holding the GPU.
+constexpr unsigned long long GRID_WAIT_NS = 1000000000ull;  // 1 s
+constexpr uint32_t GRID_SPIN_LIMIT = 1u << 24;
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_barrier(unsigned long long *bar, unsigned long long target)
+{
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1ull);
+        const unsigned long long t0 = globaltimer_ns();
+        uint32_t ok = 0;
+        for (uint32_t it = 0; it < GRID_SPIN_LIMIT; it++) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+            if (v >= target) {
+                ok = 1;
+                break;
+            }
+            if ((it & 63u) == 63u && globaltimer_ns() - t0 > GRID_WAIT_NS) break;
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // Model-table read.  The tables live in global memory, or in shared memory
 // when a kernel stages them there, so the load is a generic one.
 template <typename T>

@@ -1166,36 +1166,9 @@ cudaError_t launch_cluster_run(int bps, int slots, uint32_t *buf0, uint32_t *buf
 // every block has loaded its region.  So a run gives, bit for bit, what the
 // same number of fused launches gives.
 //
-// The barrier (grid_barrier) is bounded: a wait that gives up sets
-// LMB_E_TIMEOUT and ends the block; the others give up at their next barrier.
-constexpr uint32_t GRID_SPIN_LIMIT = 1u << 22;
-
-// Grid barrier of a cooperative launch.  Each block adds one arrival to `bar`
-// (zeroed before the launch) and waits, in thread 0, until the count reaches
-// `target` = (barriers passed + 1) x blocks.  False when the wait gave up.
-__device__ __forceinline__ bool grid_barrier(unsigned long long *bar, unsigned long long target)
-{
-    __shared__ uint32_t s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(bar, 1ull);
-        uint32_t ok = 0;
-        for (uint32_t it = 0; it < GRID_SPIN_LIMIT; it++) {
-            unsigned long long v;
-            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
-            if (v >= target) {
-                ok = 1;
-                break;
-            }
-        }
-        __threadfence();
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
+// The barrier (grid_barrier, lmb_device.cuh) is bounded: a wait that gives up
+// sets LMB_E_TIMEOUT and ends the block; the others give up at their next
+// barrier.
 template <int BPS, int S>
 __global__ void __launch_bounds__(FUSED_THREADS, 2)
     fused_grid_kernel(uint32_t *__restrict__ buf0, uint32_t *__restrict__ buf1, const uint8_t *__restrict__ sites,
