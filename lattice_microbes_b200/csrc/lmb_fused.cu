@@ -1249,10 +1249,21 @@ __global__ void __launch_bounds__(FUSED_THREADS, 2)
 template <int BPS, int S>
 static uint32_t grid_blocks_per_sm(size_t smem)
 {
-    if (cudaFuncSetAttribute(fused_grid_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
+    // The limit only grows (per device), as for the fused kernel, so that a
+    // smaller plan checked later never lowers it under a larger one's launch.
+    static size_t granted[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
         return 0;
+    }
+    if (smem > granted[dev]) {
+        if (cudaFuncSetAttribute(fused_grid_kernel<BPS, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        granted[dev] = smem;
     }
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_grid_kernel<BPS, S>, FUSED_THREADS, smem) !=
