@@ -36,6 +36,22 @@ def test_library_exports_every_declared_symbol():
     assert not [n for n in declared if n not in L.PROTOTYPES], "binding out of date"
 
 
+def test_binding_constants_equal_the_header():
+    """Every integer LMB_* constant the Python binding defines has the value
+    include/lmb.h gives it, and the header's schedules, status codes and
+    overflow modes are all bound."""
+    from lattice_microbes_b200 import _lib as L
+    text = open(os.path.join(ROOT, "include", "lmb.h")).read()
+    header = {n: int(v) for n, v in re.findall(r"#define\s+(LMB_\w+)\s+\(?(-?\d+)\)?", text)}
+    assert len(header) >= 20
+    for name, value in header.items():
+        if hasattr(L, name):
+            assert getattr(L, name) == value, name
+    for prefix in ("LMB_SCHEDULE_", "LMB_E_", "LMB_OVERFLOW_"):
+        unbound = [n for n in header if n.startswith(prefix) and not hasattr(L, n)]
+        assert not unbound, unbound
+
+
 def test_abi_version_and_status_strings():
     from lattice_microbes_b200 import _lib as L
     assert L.lib().lmb_abi_version() == 1
