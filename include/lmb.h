@@ -46,7 +46,8 @@ extern "C" {
  * (the reference's schedule, MpdRdmeSolver.cu:1011-1090); CLUSTER, for small
  * lattices, holds the whole lattice in the shared memory of one thread-block
  * cluster and runs every timestep of a run in one launch; GRID runs the
- * FUSED tiles of a Ty x Tz plan (0, 0 = the least-halo plan that fits) all
+ * FUSED tiles of a Ty x Tz plan (0, 0 = the plan with the most tiles, then
+ * the least halo, among those that fit) all
  * resident at once, one cooperative launch per run: each block keeps its
  * region in shared memory from one timestep to the next and reloads only its
  * halo rows, which the neighbouring blocks store, after a bounded grid
@@ -182,7 +183,8 @@ int lmb_lattice_set_row_major(lmb_lattice *lattice, const void *particles, const
 int lmb_lattice_get_row_major(lmb_lattice *lattice, void *particles, uint8_t *sites);
 /* Timestep schedule of this lattice: LMB_SCHEDULE_FUSED with tile Ty x Tz
  * (0, 0 = default plan), LMB_SCHEDULE_GRID with tile Ty x Tz (0, 0 = the
- * least-halo plan whose tiles fit on the device at once),
+ * plan with the most tiles, then the least halo, whose tiles fit on the
+ * device at once),
  * LMB_SCHEDULE_PHASES or LMB_SCHEDULE_CLUSTER (Ty, Tz unused).  The reference has fixed block sizes instead
  * (options.cmake:89-95). */
 int lmb_lattice_set_schedule(lmb_lattice *lattice, int schedule, uint32_t Ty, uint32_t Tz);

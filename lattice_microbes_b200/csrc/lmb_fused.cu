@@ -1308,18 +1308,24 @@ bool fused_grid_fits(const Geometry &g, int bps, int slots, uint32_t cap, uint32
 bool fused_grid_default_shape(const Geometry &g, int bps, int slots, uint32_t cap, uint32_t stage_bytes,
                               TileShape &ts)
 {
-    // The least halo overhead among the shapes whose tiles fit together.
+    // The most tiles among the shapes whose tiles fit together (a timestep
+    // is the slowest tile's chain, shorter for smaller tiles), then the least
+    // halo overhead.  On the rod cell this picks 4 x 8 (256 tiles), the
+    // fastest plan measured; 8 x 8 (128 tiles, the least halo) is 7 % slower.
     const uint32_t cands[] = {1, 2, 4, 8, 16};
     bool found = false;
-    double best = 1e30;
+    uint32_t best_tiles = 0;
+    double best_halo = 1e30;
     for (uint32_t Ty : cands)
         for (uint32_t Tz : cands) {
             TileShape t;
             if (!fused_make_shape(g, bps, slots, Ty, Tz, t) || !fused_grid_fits(g, bps, slots, cap, stage_bytes, t))
                 continue;
+            const uint32_t tiles = t.tiles_y * t.tiles_z;
             const double halo = (double)(Ty + 2) * (Tz + 2) / ((double)Ty * Tz);
-            if (halo < best) {
-                best = halo;
+            if (tiles > best_tiles || (tiles == best_tiles && halo < best_halo)) {
+                best_tiles = tiles;
+                best_halo = halo;
                 ts = t;
                 found = true;
             }

@@ -76,8 +76,8 @@ cudaError_t launch_cluster_run(int bytes_per_slot, int slots, uint32_t *buf0, ui
 // run starts from buf0 and ends in buf0 or buf1 by the parity of its timestep
 // count (of the failing timestep + 1 when it fails).  fused_grid_fits: the
 // plan's tiles fit on the current device at once (it sets the kernel's
-// shared-memory attribute); fused_grid_default_shape: the least-halo shape
-// that does.
+// shared-memory attribute); fused_grid_default_shape: among the shapes that
+// do, the one with the most tiles, then the least halo.
 bool fused_grid_fits(const Geometry &g, int bytes_per_slot, int slots, uint32_t cap, uint32_t stage_bytes,
                      const TileShape &ts);
 bool fused_grid_default_shape(const Geometry &g, int bytes_per_slot, int slots, uint32_t cap, uint32_t stage_bytes,

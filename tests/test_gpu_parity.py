@@ -327,7 +327,7 @@ def test_cluster_schedule_bimolecular_vs_oracle(ctx):
 
 
 @pytest.mark.parametrize("shape,slots,bps,per_slot,nsteps,tile", [
-    ((32, 32, 32), 8, 1, 0.01, 40, (0, 0)),    # the default plan: least halo among shapes that fit at once
+    ((32, 32, 32), 8, 1, 0.01, 40, (0, 0)),    # the default plan: the most tiles that fit at once
     ((16, 16, 16), 4, 1, 0.2, 40, (1, 1)),     # 256 tiles of one row
     ((24, 20, 48), 16, 1, 0.05, 30, (4, 2)),   # rows not 16-byte aligned
     ((32, 16, 32), 4, 4, 0.15, 30, (2, 4)),    # IntLattice
