@@ -319,12 +319,12 @@ __device__ __forceinline__ SiteWords<BPS, S> sweep_site(const SiteWords<BPS, S> 
 // Per-reaction propensity from FP32 counts (byte_reaction_dev.cu:62-102,
 // MPD_GLOBAL_R_MATRIX branch: the self reaction is rate*n*(n-1)).
 // hi: slots at and above it are empty (an unrolled loop stops there).
+// The same from a reaction's table entries (D1, D2, order, rate), for a
+// reaction allowed on the site's type.
 template <int BPS, int S>
-__device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_t t, const SiteWords<BPS, S> &s,
-                                                     uint32_t rx, int hi)
+__device__ __forceinline__ float propensity_of(const SiteWords<BPS, S> &s, int hi, uint32_t d1, uint32_t d2,
+                                               uint32_t order, float rate)
 {
-    if (!tload(m.RL + (size_t)rx * m.nst + t)) return 0.0f;
-    const uint32_t d1 = tload(m.D1 + rx), d2 = tload(m.D2 + rx);
     float n1 = 0.0f, n2 = 0.0f;
 #pragma unroll
     for (int k = 0; k < S; k++) {
@@ -335,14 +335,21 @@ __device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_
             n2 = __fadd_rn(n2, p == d2 ? 1.0f : 0.0f);
         }
     }
-    const float rate = tload(m.rate + rx);
-    switch (tload(m.order + rx)) {
+    switch (order) {
     case 1: return rate;
     case 2: return __fmul_rn(rate, n1);
     case 3: return __fmul_rn(__fmul_rn(rate, n1), n2);
     case 4: return __fmul_rn(__fmul_rn(rate, n1), __fsub_rn(n1, 1.0f));
     default: return 0.0f;
     }
+}
+
+template <int BPS, int S>
+__device__ __forceinline__ float reaction_propensity(const DevTables &m, uint32_t t, const SiteWords<BPS, S> &s,
+                                                     uint32_t rx, int hi)
+{
+    if (!tload(m.RL + (size_t)rx * m.nst + t)) return 0.0f;
+    return propensity_of<BPS, S>(s, hi, tload(m.D1 + rx), tload(m.D2 + rx), tload(m.order + rx), tload(m.rate + rx));
 }
 
 // The first two exits of react_site, for a site of type t holding n
@@ -520,14 +527,46 @@ __device__ __forceinline__ bool react_site(SiteWords<BPS, S> &s, uint32_t t, uin
             visit(rx);
         }
     } else if (bitmap) {
+        // Candidates in ascending order, RXB at a time: every table entry of
+        // the batch is loaded before any propensity is formed (one round trip
+        // per batch instead of two per candidate), then the batch is visited
+        // in order with the same arithmetic as visit().
+        constexpr int RXB = 4;
+        uint32_t rxs[RXB];
+        int nb = 0;
+        auto flush = [&]() {
+            uint32_t rl[RXB], d1[RXB], d2[RXB], ord[RXB];
+            float rate[RXB];
+#pragma unroll
+            for (int j = 0; j < RXB; j++) {
+                const uint32_t rx = j < nb ? rxs[j] : rxs[0];
+                rl[j] = tload(m.RL + (size_t)rx * m.nst + t);
+                d1[j] = tload(m.D1 + rx);
+                d2[j] = tload(m.D2 + rx);
+                ord[j] = tload(m.order + rx);
+                rate[j] = tload(m.rate + rx);
+            }
+#pragma unroll
+            for (int j = 0; j < RXB; j++) {
+                if (j >= nb) break;
+                const float prop = rl[j] ? propensity_of<BPS, S>(s, hi, d1[j], d2[j], ord[j], rate[j]) : 0.0f;
+                if (prop > 0.0f) {
+                    if (rp > 0.0f) idx = rxs[j];
+                    rp = __fsub_rn(rp, prop);
+                }
+            }
+            nb = 0;
+        };
         for (uint32_t w = 0; w < nbw; w++) {
             uint32_t bits = bm[w];
             while (bits) {
                 const uint32_t k = __ffs(bits) - 1;
                 bits &= bits - 1;
-                visit(w * 32u + k);
+                rxs[nb++] = w * 32u + k;
+                if (nb == RXB) flush();
             }
         }
+        if (nb > 0) flush();
     } else {
         // Insertion sort of the few entries; repeats skipped.
         for (int a = 1; a < nc; a++) {
