@@ -189,9 +189,12 @@ int lmb_lattice_get_row_major(lmb_lattice *lattice, void *particles, uint8_t *si
  * (options.cmake:89-95). */
 int lmb_lattice_set_schedule(lmb_lattice *lattice, int schedule, uint32_t Ty, uint32_t Tz);
 int lmb_lattice_get_schedule(lmb_lattice *lattice, int *schedule, uint32_t *Ty, uint32_t *Tz);
-/* Autotuner: times every schedule and tile shape that fits for `timesteps`
- * on a saved copy of the lattice state, restores the state and keeps the
- * fastest. */
+/* Autotuner: times the per-phase schedule, the cluster-resident one where it
+ * fits and every fused tile shape that fits for `timesteps` on a saved copy
+ * of the lattice state, restores the state and keeps the fastest.  The
+ * grid-resident schedule is chosen only by lmb_lattice_set_schedule: its
+ * cooperative launch does not overlap other lattices' runs on other streams,
+ * which fused launches do. */
 int lmb_lattice_autotune(lmb_lattice *lattice, const lmb_model *model, uint32_t seed, uint32_t first_timestep,
                          uint32_t timesteps, int *schedule, uint32_t *Ty, uint32_t *Tz, float *best_ms);
 /* Device pointers of the current particle buffer and of the site types. */
